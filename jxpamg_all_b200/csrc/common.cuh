@@ -1,0 +1,96 @@
+// Shared definitions for the B200 CPR-GMRES library: status codes, CUDA
+// error plumbing, device buffers and small launch helpers.
+//
+// Status codes follow the reference (jxfpamg-0220/include/jxf_util.h:152-159):
+// 0 success, 1 generic, 2 memory, 4 argument, 256 convergence; this library
+// adds JXCPR_ERROR_DEVICE for a failed CUDA call and JXCPR_ERROR_NUMERIC for a
+// NaN/Inf seen on the device.  No entry point aborts the process.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <cstddef>
+#include <string>
+
+#define JXCPR_SUCCESS 0
+#define JXCPR_ERROR_GENERIC 1
+#define JXCPR_ERROR_MEMORY 2
+#define JXCPR_ERROR_ARG 4
+#define JXCPR_ERROR_CONV 256
+#define JXCPR_ERROR_DEVICE 512
+#define JXCPR_ERROR_NUMERIC 1024
+
+namespace jxcpr {
+
+// Last error message (thread-local) for diagnostics through the C ABI.
+void set_error(const char *fmt, ...);
+const char *last_error();
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+struct CudaError {
+    cudaError_t code;
+    const char *what;
+};
+
+#define JX_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e__ = (call);                                                      \
+        if (e__ != cudaSuccess) {                                                      \
+            ::jxcpr::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,              \
+                               cudaGetErrorString(e__));                               \
+            throw ::jxcpr::CudaError{e__, #call};                                      \
+        }                                                                              \
+    } while (0)
+
+#define JX_LAUNCH_CHECK() JX_CUDA(cudaGetLastError())
+
+// Owning device buffer (cudaMalloc'd, 256-byte aligned, padded by 64 bytes so
+// that 16-byte-rounded bulk copies of the tail stay inside the allocation).
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        size_t bytes = count * sizeof(T) + 64;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            set_error("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+            throw CudaError{e, "cudaMalloc"};
+        }
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void zero(cudaStream_t s) { if (n) JX_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void upload(const T *h, size_t count, cudaStream_t s) {
+        if (count) JX_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void download(T *h, size_t count, cudaStream_t s) const {
+        if (count) JX_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+    T *get() const { return p; }
+};
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace jxcpr

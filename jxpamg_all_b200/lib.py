@@ -1,0 +1,48 @@
+"""ctypes binding of libjxcpr_b200.so (the product library).
+
+There is no CPU fallback: if the library is missing or CUDA is unavailable
+the calls raise.  The binding mirrors include/jxcpr_b200.h one to one.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libjxcpr_b200.so")
+
+c_int, c_double, c_void_p, c_longlong, c_char_p = (ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                                   ctypes.c_longlong, ctypes.c_char_p)
+
+_lib = None
+
+
+class JxcprError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"jxcpr status {status}: {msg}")
+        self.status = status
+
+
+def _declare(lib):
+    f = lib.jxcpr_last_error
+    f.restype = c_char_p
+    lib.jxcpr_bsr_matvec_dev.argtypes = [c_int, c_int, c_longlong, c_void_p, c_void_p, c_void_p, c_double,
+                                         c_void_p, c_double, c_void_p, c_int, c_void_p]
+    lib.jxcpr_bsr_matvec_dev_f32.argtypes = lib.jxcpr_bsr_matvec_dev.argtypes
+    lib.jxcpr_dot_dev.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
+
+
+def load():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built; run `python -m jxpamg_all_b200.build`")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise JxcprError(status, load().jxcpr_last_error().decode(errors="replace"))
