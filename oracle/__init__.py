@@ -110,3 +110,142 @@ def ref_bsr_decouple(ia, ja, a, bs, rhs, dtype_code):
     a2, r2 = _f64(a).copy(), _f64(rhs).copy()
     ref().ref_bsr_decouple(c_int(nb), c_int(bs), _p(ia), _p(ja), _p(a2), _p(r2), c_int(dtype_code), c_int(1))
     return a2, r2
+
+
+# ---- AMG / CPR / GMRES handles ----------------------------------------------------
+class _CprBase:
+    """Common accessors for a CPR handle (restatement or reference)."""
+
+    _prefix = ""
+
+    def _fn(self, name):
+        return getattr(self._lib, self._prefix + name)
+
+    def num_levels(self):
+        return int(self._fn("cpr_num_levels")(c_void_p(self.h)))
+
+    def level_matrix(self, lev, what):
+        """(ia, ja, a) of A_l (what=0) or P_l (what=1), or None."""
+        sizes = np.zeros(3, np.int32)
+        st = self._fn("cpr_level_sizes")(c_void_p(self.h), c_int(lev), c_int(what), _p(sizes))
+        if st < 0:
+            return None
+        n, m, nnz = (int(v) for v in sizes)
+        ia = np.zeros(n + 1, np.int32)
+        ja = np.zeros(max(nnz, 1), np.int32)
+        a = np.zeros(max(nnz, 1))
+        self._fn("cpr_level_matrix")(c_void_p(self.h), c_int(lev), c_int(what), _p(ia), _p(ja), _p(a))
+        return ia, ja[:nnz], a[:nnz], m
+
+    def level_cf(self, lev, n):
+        cf = np.zeros(n, np.int32)
+        st = self._fn("cpr_level_cf")(c_void_p(self.h), c_int(lev), _p(cf))
+        return None if st < 0 else cf
+
+
+class OracleCPR(_CprBase):
+    """CPR setup of the restatement (AMG hierarchy built at construction)."""
+
+    _prefix = "orc_"
+
+    def __init__(self, ia, ja, a, bs, stage2_maxit=3):
+        self._lib = orc()
+        self._lib.orc_cpr_create.restype = c_void_p
+        self.nb, self.bs = len(ia) - 1, bs
+        self._keep = (_i32(ia), _i32(ja), _f64(a))
+        self.h = self._lib.orc_cpr_create(c_int(self.nb), c_int(bs), *(_p(v) for v in self._keep),
+                                          c_int(stage2_maxit))
+
+    def apply(self, r):
+        z = np.zeros(self.nb * self.bs)
+        self._lib.orc_cpr_apply_h(c_void_p(self.h), _p(_f64(r)), _p(z))
+        return z
+
+    def vcycle(self, rp, xp=None):
+        xp = np.zeros(self.nb) if xp is None else _f64(xp).copy()
+        self._lib.orc_cpr_amg_vcycle(c_void_p(self.h), _p(_f64(rp)), _p(xp))
+        return xp
+
+    def __del__(self):
+        try:
+            self._lib.orc_cpr_destroy(c_void_p(self.h))
+        except Exception:
+            pass
+
+
+class RefCPR(_CprBase):
+    """CPR setup of the reference library (JXF_CPRCreate/SetParameter/Setup)."""
+
+    _prefix = "ref_"
+
+    def __init__(self, ia, ja, a, bs, stage2_maxit=3, stage2_type=2):
+        self._lib = ref()
+        self.nb, self.bs = len(ia) - 1, bs
+        self._keep = (_i32(ia), _i32(ja), _f64(a))
+        self.h = self._lib.ref_cpr_create(c_int(self.nb), c_int(bs), *(_p(v) for v in self._keep), c_int(1),
+                                          c_int(stage2_maxit), c_int(stage2_type), c_int(1))
+        if not self.h:
+            raise RuntimeError("reference CPR setup failed")
+
+    def apply(self, r):
+        z = np.zeros(self.nb * self.bs)
+        self._lib.ref_cpr_apply(c_void_p(self.h), _p(_f64(r)), _p(z), c_int(1))
+        return z
+
+    def vcycle(self, rp, xp=None):
+        xp = np.zeros(self.nb) if xp is None else _f64(xp).copy()
+        self._lib.ref_cpr_amg_solve(c_void_p(self.h), _p(_f64(rp)), _p(xp), c_int(1))
+        return xp
+
+
+def gmres(ia, ja, a, bs, b, x0=None, k_dim=30, tol=1e-6, max_iter=200, cpr=None):
+    """Restated GMRES; returns dict(x, iters, rel, converged, norms)."""
+    nb = len(ia) - 1
+    n = nb * bs
+    x = np.zeros(n) if x0 is None else _f64(x0).copy()
+    rel = np.zeros(1)
+    conv = np.zeros(1, np.int32)
+    norms = np.zeros(max_iter + 1)
+    keep = (_i32(ia), _i32(ja), _f64(a), _f64(b))
+    it = orc().orc_gmres_solve(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), c_int(k_dim),
+                               c_double(tol), c_int(max_iter), c_void_p(cpr.h if cpr else 0), _p(rel), _p(conv),
+                               _p(norms))
+    return dict(x=x, iters=int(it), rel=float(rel[0]), converged=bool(conv[0]), norms=norms[:it + 1])
+
+
+def ref_gmres(ia, ja, a, bs, b, x0=None, k_dim=30, tol=1e-6, max_iter=200, decouple=0, precond=1,
+              stage2_maxit=3, stage2_type=2):
+    """The reference driver sequence (decouple -> CPR setup -> GMRES solve)."""
+    nb = len(ia) - 1
+    n = nb * bs
+    x = np.zeros(n) if x0 is None else _f64(x0).copy()
+    info = np.zeros(2, np.int32)
+    rel = np.zeros(2)
+    norms = np.zeros(max_iter + 1)
+    times = np.zeros(5)
+    keep = (_i32(ia), _i32(ja), _f64(a), _f64(b))
+    ref().ref_cpr_gmres_solve(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), c_int(decouple),
+                              c_int(precond), c_int(k_dim), c_double(tol), c_int(max_iter), c_int(stage2_maxit),
+                              c_int(stage2_type), _p(info), _p(rel), _p(norms), _p(times), c_int(1))
+    it = int(info[0])
+    return dict(x=x, iters=it, rel=float(rel[0]), true_rel=float(rel[1]), converged=bool(info[1]),
+                norms=norms[:it + 1], times=times)
+
+
+def hgs_relax(ia, ja, a, bs, x, b, w=0.7, omega=0.9, direction=1, sweeps=1):
+    nb = len(ia) - 1
+    x = _f64(x).copy()
+    keep = (_i32(ia), _i32(ja), _f64(a))
+    for _ in range(sweeps):
+        orc().orc_hgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), c_double(w),
+                            c_double(omega), c_int(direction))
+    return x
+
+
+def ref_hgs_relax(ia, ja, a, bs, x, b, w=0.7, omega=0.9, direction=1, sweeps=1):
+    nb = len(ia) - 1
+    x = _f64(x).copy()
+    keep = (_i32(ia), _i32(ja), _f64(a))
+    ref().ref_hgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), c_double(w),
+                        c_double(omega), c_int(direction), c_int(sweeps))
+    return x

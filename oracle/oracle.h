@@ -15,4 +15,53 @@ void orc_prolong(int nb, int bs, int p, const double *xp, double *x);
 void orc_bsr_submatrix(int nb, int bs, const int *ia, const int *ja, const double *a, int p, int *cia, int *cja,
                        double *ca);
 
+
+/* ---- AMG / CPR / GMRES restatement (orc_amg.c, orc_cpr.c) ---- */
+#define ORC_MAX_LEVELS 26
+
+typedef struct {
+    int n, m;     /* rows, cols */
+    int *ia, *ja; /* 0-based CSR, diagonal first where present */
+    double *a;
+} orc_csr;
+
+typedef struct {
+    int num_levels;
+    int owns_A0;
+    orc_csr A[ORC_MAX_LEVELS];
+    orc_csr P[ORC_MAX_LEVELS];
+    int *CF[ORC_MAX_LEVELS];
+} orc_amg;
+
+typedef struct {
+    int nb, bs, stage2_maxit;
+    const int *ia, *ja;
+    const double *a;
+    orc_csr Ap;
+    orc_amg amg;
+} orc_cpr;
+
+void orc_csr_free(orc_csr *A);
+void orc_strength(const orc_csr *A, double theta, double max_row_sum, orc_csr *S);
+void orc_rs_first_pass(const orc_csr *S, int *CF);
+double orc_park_miller(int *seed);
+void orc_pmis(const orc_csr *S, int *CF);
+void orc_hmis(const orc_csr *S, int *CF);
+void orc_extpi_interp(const orc_csr *A, const orc_csr *S, const int *CF, orc_csr *P);
+void orc_rap(const orc_csr *A, const orc_csr *P, orc_csr *Ac);
+void orc_amg_setup(const orc_csr *A0, int max_levels, int coarse_threshold, orc_amg *H);
+void orc_amg_free(orc_amg *H);
+void orc_csr_matvec(const orc_csr *A, double alpha, const double *x, double beta, double *y);
+void orc_csr_matvec_t(const orc_csr *A, double alpha, const double *x, double beta, double *y);
+void orc_relax6(const orc_csr *A, const double *f, double *u);
+int orc_gselim(const orc_csr *A, const double *f, double *u);
+void orc_amg_vcycle(const orc_amg *H, const double *f0, double *u0);
+void orc_hgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                   double w, double omega, int direction);
+void orc_cpr_setup(orc_cpr *C, int nb, int bs, const int *ia, const int *ja, const double *a, int stage2_maxit);
+void orc_cpr_apply(const orc_cpr *C, const double *r, double *z);
+void orc_cpr_free(orc_cpr *C);
+int orc_gmres(int nb, int bs, const int *ia, const int *ja, const double *a, const double *b, double *x, int k_dim,
+              double tol, int max_iter, const orc_cpr *precond, double *rel, int *converged, double *norms);
+
 #endif

@@ -293,7 +293,7 @@ int ref_cpr_gmres_solve(int nb, int bs, const int *ia, const int *ja, const doub
     JXF_GMRESSetMaxIter(gm, max_iter);
     JXF_GMRESSetTol(gm, tol);
     JXF_GMRESSetLogging(gm, 1);
-    JXF_GMRESSetPrintLevel(gm, 0);
+    JXF_GMRESSetPrintLevel(gm, 1); /* norms[] are recorded only when printing */
     if (cpr)
         JXF_GMRESSetPrecond(gm, (JXF_PtrToSolverFcn)JXF_CPRPrecond, (JXF_PtrToSolverFcn)JXF_CPRSetup, (JXF_Solver)cpr);
     JXF_GMRESSetup(gm, (JXF_Matrix)Ap, (JXF_Vector)pb, (JXF_Vector)px);

@@ -1,6 +1,10 @@
 import os
 import sys
 
+# The reference library's results depend on its OpenMP thread count; pin it to 1
+# before any library is loaded.
+os.environ.setdefault("OMP_NUM_THREADS", "1")
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

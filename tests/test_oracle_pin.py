@@ -46,3 +46,34 @@ def test_abf_consistent_rhs_keeps_solution(systems):
     a2, r2 = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
     assert np.array_equal(a1, a2)
     assert not np.allclose(r1, r2)
+
+
+@pytest.mark.parametrize("name", ["small", "tiny3", "c0"])
+@pytest.mark.parametrize("w,omega,direction", [(0.7, 0.9, 1), (1.0, 1.0, 1), (0.7, 0.9, -1)])
+def test_hgs_relax_pin(systems, name, w, omega, direction):
+    s = systems(name)
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
+    x0 = np.random.default_rng(1).standard_normal(s.n)
+    got = oracle.hgs_relax(s.ia, s.ja, a, s.block_size, x0, b, w, omega, direction, 3)
+    want = oracle.ref_hgs_relax(s.ia, s.ja, a, s.block_size, x0, b, w, omega, direction, 3)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("name", ["tiny", "small", "tiny3"])
+def test_cpr_and_gmres_pin_live(systems, name):
+    """Restatement vs the live reference: hierarchy, one CPR application, full solve."""
+    s = systems(name)
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
+    R = oracle.RefCPR(s.ia, s.ja, a, s.block_size)
+    O = oracle.OracleCPR(s.ia, s.ja, a, s.block_size)
+    assert R.num_levels() == O.num_levels()
+    for lev in range(R.num_levels()):
+        ar, ao = R.level_matrix(lev, 0), O.level_matrix(lev, 0)
+        for u, v in zip(ar[:3], ao[:3]):
+            assert np.array_equal(u, v)
+    r = np.random.default_rng(7).standard_normal(s.n)
+    assert np.array_equal(R.apply(r), O.apply(r))
+    ref = oracle.ref_gmres(s.ia, s.ja, s.a, s.block_size, s.b, decouple=1, tol=1e-6, max_iter=200)
+    orc = oracle.gmres(s.ia, s.ja, a, s.block_size, b, tol=1e-6, max_iter=200, cpr=O)
+    assert ref["iters"] == orc["iters"]
+    assert np.array_equal(ref["x"], orc["x"])
