@@ -69,6 +69,56 @@ JXCPR_API int jxcpr_kernel_error_flag(void);
  */
 JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, double *out_host, void *stream);
 
+/* ---- solver object ---------------------------------------------------------
+ * CPR-GMRES on one GPU: jxcpr_solver_setup copies a BSR matrix (host or
+ * device arrays), applies the configured decoupling (jxf_BSRMatrixDecouple,
+ * jxfpamg-0220/csrc/cpr/jxf_bsr_decoup.c:1273) and builds the CPR
+ * preconditioner (JXF_CPRSetup, jxfpamg-0220/csrc/cpr/jxf_cpr.c:268-422);
+ * jxcpr_solver_solve decouples b and runs restarted GMRES
+ * (jxf_GMRESSolve, jxfpamg-0220/csrc/krylov/pgmres.c:950-1713) with CPR
+ * (JXF_CPRPrecond, jxf_cpr.c:424-610) as right preconditioner.  It returns 0
+ * when the relative residual reached tol, JXCPR_ERROR_CONV (256) otherwise.
+ *
+ * Options (jxcpr_solver_set_int / _set_real; unknown keys return 4, as
+ * JXF_CPRSetParameter does, jxf_cpr.c:226-262):
+ *   int : k_dim (30), max_iter (100), min_iter (0), is_check_restarted (1),
+ *         pressure_index (0), stage1_maxit (1), stage2_maxit (3),
+ *         stage1_solver_type (1 AMG; 0 none), stage2_solver_type (2 HGS),
+ *         decouple (0 none, 1 ABF, 5 True-IMPES), consistent_rhs (0: the
+ *         reference's right-hand-side arithmetic, 1: solution-preserving),
+ *         smoother_order (0 exact sequential order, 1 multicolour),
+ *         coarse_exact (1 substitution in the reference's order, 0 inverse),
+ *         use_tma_spmv (1), print_level, logging, block_size (ignored)
+ *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),
+ *         convfac_threshold (1e4), stage2_relax_weight (0.7), stage2_omega (0.9)
+ */
+typedef struct jxcpr_solver jxcpr_solver;
+
+JXCPR_API int jxcpr_solver_create(jxcpr_solver **solver);
+JXCPR_API int jxcpr_solver_destroy(jxcpr_solver *solver);
+JXCPR_API int jxcpr_solver_set_int(jxcpr_solver *solver, const char *key, int value);
+JXCPR_API int jxcpr_solver_set_real(jxcpr_solver *solver, const char *key, double value);
+/* device != 0: ia/ja/a are device pointers. */
+JXCPR_API int jxcpr_solver_setup(jxcpr_solver *solver, int nb, int bs, long long nnzb, const int *ia,
+                                 const int *ja, const double *a, int device);
+/* b, x: nb*bs entries (host or device); x holds the initial guess on entry. */
+JXCPR_API int jxcpr_solver_solve(jxcpr_solver *solver, const double *b, double *x, int device, int *iterations,
+                                 double *rel_residual);
+/* Residual history of the last solve; returns its length (iterations + 1). */
+JXCPR_API int jxcpr_solver_get_norms(jxcpr_solver *solver, double *norms, int capacity);
+/* stats[0..3]: setup ms, solve ms, CPR stage-1 setup s, number of AMG levels. */
+JXCPR_API int jxcpr_solver_stats(jxcpr_solver *solver, double *stats);
+/* AMG hierarchy inspection: what = 0 A_l, 1 P_l, 2 R_l = P_l^T; sizes = {rows, cols, nnz}. */
+JXCPR_API int jxcpr_solver_num_levels(jxcpr_solver *solver);
+JXCPR_API int jxcpr_solver_level_sizes(jxcpr_solver *solver, int level, int what, int *sizes);
+JXCPR_API int jxcpr_solver_level_matrix(jxcpr_solver *solver, int level, int what, int *ia, int *ja, double *a);
+JXCPR_API int jxcpr_solver_level_cf(jxcpr_solver *solver, int level, int *cf);
+/* Decoupled block values after setup (host copy). */
+JXCPR_API int jxcpr_solver_decoupled_values(jxcpr_solver *solver, double *a);
+/* One CPR application z = M^{-1} r / one AMG V-cycle on the pressure system (xp in/out). */
+JXCPR_API int jxcpr_solver_cpr_apply(jxcpr_solver *solver, const double *r, double *z, int device);
+JXCPR_API int jxcpr_solver_vcycle(jxcpr_solver *solver, const double *rp, double *xp, int device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,315 @@
+// Pressure AMG: hierarchy construction and the V(1,1) cycle of CPR stage 1.
+//
+// Setup follows jxf_PAMGSetup (jxfpamg-0220/csrc/amg/par_amg_setup.c:525-1240):
+// per level strength -> HMIS -> ext+i -> Galerkin product, stopping after the
+// level whose coarse size is <= coarse_threshold (1000) or at max_levels-1.
+//
+// The cycle follows jxf_PAMGCycle (amg/par_cycle.c:20-969) with
+// jxf_PAMGRelaxIF (par_relax_if.c:22-76) as CPR configures it: on every level
+// but the coarsest, two symmetric Gauss-Seidel applications before and two
+// after the coarse correction (relax_order 1 visits "C then F" and "F then C",
+// and jxf_PAMGRelax resets the point selection to "all points", par_relax.c:48);
+// residual r = f - A u, restriction f_c = P^T r, prolongation u += P u_c; on the
+// coarsest level the dense Gaussian elimination of jxf_gselim
+// (operation/matops/par_gs.c:20-74), here factored once at setup.
+#include <algorithm>
+#include <vector>
+
+#include "amg.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace jxcpr {
+
+// ---------------------------------------------------------------------------
+// coarsest level: dense LU without pivoting in jxf_gselim's order
+// ---------------------------------------------------------------------------
+__global__ void dense_assemble_kernel(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                                      const double *__restrict__ a, double *__restrict__ M) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = ia[i]; k < ia[i + 1]; ++k) M[(long long)i * n + ja[k]] = a[k];
+}
+
+// One elimination step k on the trailing block; also records the multipliers.
+__global__ void lu_step_kernel(int n, int k, double *__restrict__ M, double *__restrict__ Lt) {
+    const int j = k + 1 + blockIdx.y;            // row
+    const int m = k + 1 + blockIdx.x * blockDim.x + threadIdx.x;  // column
+    if (j >= n) return;
+    const double akk = M[(long long)k * n + k];
+    const double ajk = M[(long long)j * n + k];
+    const bool active = (akk != 0.0) && (ajk != 0.0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) Lt[(long long)k * n + j] = active ? ajk / akk : 0.0;
+    if (!active || m >= n) return;
+    const double factor = ajk / akk;
+    M[(long long)j * n + m] -= factor * M[(long long)k * n + m];
+}
+
+__global__ void transpose_upper_kernel(int n, const double *__restrict__ M, double *__restrict__ Ut) {
+    const int j = blockIdx.y;  // row of U
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;  // column of U
+    if (j >= n || k >= n) return;
+    Ut[(long long)k * n + j] = (j <= k) ? M[(long long)j * n + k] : 0.0;
+}
+
+// Forward and back substitution with the stored factors, column oriented, in
+// jxf_gselim's order (bit-identical to re-running the elimination).
+__global__ void __launch_bounds__(1024) lu_solve_kernel(int n, const double *__restrict__ Lt,
+                                                        const double *__restrict__ Ut, const double *__restrict__ f,
+                                                        double *__restrict__ u) {
+    extern __shared__ double xs[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = f[i];
+    __syncthreads();
+    if (n == 1) {
+        if (threadIdx.x == 0 && Ut[0] != 0.0) u[0] = xs[0] / Ut[0];
+        else if (threadIdx.x == 0) u[0] = xs[0];
+        return;
+    }
+    for (int k = 0; k < n - 1; ++k) {
+        const double xk = xs[k];
+        const double *col = Lt + (long long)k * n;
+        for (int j = k + 1 + threadIdx.x; j < n; j += blockDim.x) {
+            const double l = col[j];
+            if (l != 0.0) xs[j] -= l * xk;
+        }
+        __syncthreads();
+    }
+    for (int k = n - 1; k > 0; --k) {
+        if (threadIdx.x == 0) xs[k] /= Ut[(long long)k * n + k];
+        __syncthreads();
+        const double xk = xs[k];
+        const double *col = Ut + (long long)k * n;
+        for (int j = threadIdx.x; j < k; j += blockDim.x) {
+            const double v = col[j];
+            if (v != 0.0) xs[j] -= xk * v;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) xs[0] /= Ut[0];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = xs[i];
+}
+
+// Explicit inverse column by column (setup of the fast coarse solve).
+__global__ void lu_inverse_kernel(int n, const double *__restrict__ Lt, const double *__restrict__ Ut,
+                                  double *__restrict__ inv_t, double *__restrict__ work) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;  // unit vector e_c
+    if (c >= n) return;
+    double *x = work + (long long)c * n;
+    for (int i = 0; i < n; ++i) x[i] = (i == c) ? 1.0 : 0.0;
+    for (int k = 0; k < n - 1; ++k) {
+        const double xk = x[k];
+        for (int j = k + 1; j < n; ++j) {
+            const double l = Lt[(long long)k * n + j];
+            if (l != 0.0) x[j] -= l * xk;
+        }
+    }
+    for (int k = n - 1; k > 0; --k) {
+        x[k] /= Ut[(long long)k * n + k];
+        const double xk = x[k];
+        for (int j = 0; j < k; ++j) {
+            const double v = Ut[(long long)k * n + j];
+            if (v != 0.0) x[j] -= xk * v;
+        }
+    }
+    x[0] /= Ut[0];
+    for (int i = 0; i < n; ++i) inv_t[(long long)c * n + i] = x[i];  // column c of A^{-1}
+}
+
+__global__ void transpose_sq_kernel(int n, const double *__restrict__ in, double *__restrict__ out) {
+    const int r = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n && c < n) out[(long long)c * n + r] = in[(long long)r * n + c];
+}
+
+// u = Ainv f, one warp per row.
+__global__ void dense_gemv_kernel(int n, const double *__restrict__ Ainv, const double *__restrict__ f,
+                                  double *__restrict__ u) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0.0;
+    for (int c = lane; c < n; c += 32) s += Ainv[(long long)row * n + c] * f[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) u[row] = s;
+}
+
+void coarse_setup(Amg &H, cudaStream_t s) {
+    AmgLevel &L = *H.levels.back();
+    const int n = L.A.nrows;
+    H.nc = n;
+    if (n == 0) return;
+    if (n > 8192) {
+        set_error("coarsest level has %d rows (dense solve limited to 8192); coarsening stalled", n);
+        throw CudaError{cudaErrorInvalidValue, "coarse size"};
+    }
+    DevBuf<double> M((size_t)n * n);
+    M.zero(s);
+    dense_assemble_kernel<<<div_up(n, 128), 128, 0, s>>>(n, L.A.ia.get(), L.A.ja.get(), L.A.a.get(), M.get());
+    JX_LAUNCH_CHECK();
+    H.Lt.alloc((size_t)n * n);
+    H.Lt.zero(s);
+    for (int k = 0; k < n - 1; ++k) {
+        dim3 grid(div_up(std::max(1, n - k - 1), 256), n - k - 1);
+        lu_step_kernel<<<grid, 256, 0, s>>>(n, k, M.get(), H.Lt.get());
+        JX_LAUNCH_CHECK();
+    }
+    H.Ufac.alloc((size_t)n * n);
+    transpose_upper_kernel<<<dim3(div_up(n, 256), n), 256, 0, s>>>(n, M.get(), H.Ufac.get());
+    JX_LAUNCH_CHECK();
+    if (!H.prm.coarse_exact) {
+        DevBuf<double> inv_t((size_t)n * n), work((size_t)n * n);
+        lu_inverse_kernel<<<div_up(n, 64), 64, 0, s>>>(n, H.Lt.get(), H.Ufac.get(), inv_t.get(), work.get());
+        JX_LAUNCH_CHECK();
+        H.Ainv.alloc((size_t)n * n);
+        transpose_sq_kernel<<<dim3(div_up(n, 256), n), 256, 0, s>>>(n, inv_t.get(), H.Ainv.get());
+        JX_LAUNCH_CHECK();
+    }
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s) {
+    const int n = H.nc;
+    if (n == 0) return;
+    if (H.prm.coarse_exact) {
+        const size_t smem = sizeof(double) * (size_t)n;
+        if (smem > 48 * 1024) {
+            JX_CUDA(cudaFuncSetAttribute(lu_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        lu_solve_kernel<<<1, 1024, smem, s>>>(n, H.Lt.get(), H.Ufac.get(), f, u);
+    } else {
+        dense_gemv_kernel<<<div_up((long long)n * 32, 256), 256, 0, s>>>(n, H.Ainv.get(), f, u);
+    }
+    JX_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// hierarchy
+// ---------------------------------------------------------------------------
+static void level_schedules(AmgLevel &L, int order, cudaStream_t s) {
+    const int n = L.A.nrows;
+    std::vector<int> ia(n + 1), ja(L.A.nnz > 0 ? L.A.nnz : 1);
+    L.A.ia.download(ia.data(), n + 1, s);
+    L.A.ja.download(ja.data(), L.A.nnz, s);
+    JX_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> perm, gptr, rank;
+    build_schedule_host(n, ia.data(), ja.data(), order, true, perm, gptr, rank);
+    upload_schedule(perm, gptr, rank, L.fwd, s);
+    build_schedule_host(n, ia.data(), ja.data(), order, false, perm, gptr, rank);
+    upload_schedule(perm, gptr, rank, L.bwd, s);
+}
+
+void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
+    H.levels.clear();
+    H.levels.emplace_back(new AmgLevel());
+    H.levels[0]->A = std::move(A0);
+    int level = 0;
+    while (true) {
+        AmgLevel &L = *H.levels[level];
+        const int n = L.A.nrows;
+        DevPattern S;
+        amg_strength(L.A.view(), H.prm.strong_threshold, H.prm.max_row_sum, S, s);
+        std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);
+        S.ia.download(sia.data(), n + 1, s);
+        S.ja.download(sja.data(), S.nnz, s);
+        JX_CUDA(cudaStreamSynchronize(s));
+        L.cf.assign(n, 0);
+        rs_first_pass_host(n, sia.data(), sja.data(), L.cf.data());
+        DevBuf<int> cf(n > 0 ? n : 1);
+        cf.upload(L.cf.data(), n, s);
+        amg_pmis(S, cf.get(), s);
+        cf.download(L.cf.data(), n, s);
+        const int nc = amg_extpi_interp(L.A.view(), S, cf.get(), L.P, s);
+        csr_transpose(L.P.view(), L.R, s);
+        std::unique_ptr<AmgLevel> next(new AmgLevel());
+        amg_rap(L.A.view(), L.P, L.R, next->A, s);
+        H.levels.push_back(std::move(next));
+        ++level;
+        if (level == H.prm.max_levels - 1 || nc <= H.prm.coarse_threshold) break;
+    }
+    for (auto &Lp : H.levels) {
+        AmgLevel &L = *Lp;
+        const int n = L.A.nrows;
+        L.f.alloc(n > 0 ? n : 1);
+        L.u.alloc(n > 0 ? n : 1);
+        L.lanes = lanes_for(n > 0 ? (double)L.A.nnz / n : 1.0);
+        if (&L == H.levels.back().get()) continue;
+        level_schedules(L, H.prm.order, s);
+        if (H.prm.order == ORDER_EXACT) {
+            L.smoother = SMOOTH_EXACT_GS;
+        } else if (L.fwd.ngroups <= H.prm.max_colors) {
+            L.smoother = SMOOTH_COLOR_GS;
+        } else {
+            L.smoother = SMOOTH_L1_JACOBI;
+            L.dinv.alloc(n > 0 ? n : 1);
+            l1_diag(L.A.view(), L.dinv.get(), s);
+        }
+    }
+    const int n0 = H.levels[0]->A.nrows;
+    H.work.alloc((size_t)(n0 > 0 ? n0 : 1) * 2);
+    H.err.alloc(1);
+    H.err.zero(s);
+    coarse_setup(H, s);
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+// One "symmetric Gauss-Seidel application" of the level's smoother.
+static void sgs(Amg &H, AmgLevel &L, const double *f, double *u, double *vt, cudaStream_t s) {
+    switch (L.smoother) {
+        case SMOOTH_EXACT_GS:
+            gs_sweep(L.A.view(), L.fwd, f, u, L.fwd.rank.get(), vt, H.err.get(), s);
+            gs_sweep(L.A.view(), L.bwd, f, u, L.bwd.rank.get(), vt, H.err.get(), s);
+            break;
+        case SMOOTH_COLOR_GS:
+            gs_sweep_colors(L.A.view(), L.fwd, L.lanes, f, u, s);
+            gs_sweep_colors(L.A.view(), L.bwd, L.lanes, f, u, s);
+            break;
+        default:
+            jacobi_l1_sweep(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
+            jacobi_l1_sweep(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
+            break;
+    }
+}
+
+void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s) {
+    const int L = H.num_levels();
+    double *vt = H.work.get();
+    double *res = H.work.get() + H.levels[0]->A.nrows;
+    auto F = [&](int l) -> const double * { return l == 0 ? f0 : H.levels[l]->f.get(); };
+    auto U = [&](int l) -> double * { return l == 0 ? u0 : H.levels[l]->u.get(); };
+    if (L == 1) {
+        // a single level cannot happen with coarse_threshold >= 1 unless n <= threshold; solve directly
+        coarse_solve(H, f0, u0, s);
+        return;
+    }
+    for (int l = 0; l < L - 1; ++l) {
+        AmgLevel &Lv = *H.levels[l];
+        sgs(H, Lv, F(l), U(l), vt, s);
+        sgs(H, Lv, F(l), U(l), vt, s);
+        const int n = Lv.A.nrows;
+        JX_CUDA(cudaMemsetAsync(U(l + 1), 0, sizeof(double) * H.levels[l + 1]->A.nrows, s));
+        if (H.prm.order == ORDER_EXACT) {
+            JX_CUDA(cudaMemcpyAsync(res, F(l), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            csr_spmv(Lv.A.view(), -1.0, U(l), 1.0, res, s);
+            csr_spmv(Lv.R.view(), 1.0, res, 0.0, H.levels[l + 1]->f.get(), s);
+        } else {
+            residual_vec(Lv.A.view(), Lv.lanes, F(l), U(l), res, s);
+            const int nr = Lv.R.nrows;
+            spmv_vec(Lv.R.view(), lanes_for(nr > 0 ? (double)Lv.R.nnz / nr : 1.0), 1.0, res, 0.0,
+                     H.levels[l + 1]->f.get(), s);
+        }
+    }
+    coarse_solve(H, F(L - 1), U(L - 1), s);
+    for (int l = L - 2; l >= 0; --l) {
+        AmgLevel &Lv = *H.levels[l];
+        if (H.prm.order == ORDER_EXACT)
+            csr_spmv(Lv.P.view(), 1.0, U(l + 1), 1.0, U(l), s);
+        else
+            spmv_vec(Lv.P.view(), lanes_for(Lv.P.nrows > 0 ? (double)Lv.P.nnz / Lv.P.nrows : 1.0), 1.0, U(l + 1), 1.0,
+                     U(l), s);
+        sgs(H, Lv, F(l), U(l), vt, s);
+        sgs(H, Lv, F(l), U(l), vt, s);
+    }
+}
+
+}  // namespace jxcpr

@@ -1,0 +1,123 @@
+// AMG hierarchy, smoother schedules and the setup / cycle entry points.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace jxcpr {
+
+// Sparsity pattern only (strength matrix).
+struct DevPattern {
+    int n = 0;
+    long long nnz = 0;
+    DevBuf<int> ia, ja;
+};
+
+// Rows grouped so that rows of one group can be relaxed concurrently and the
+// groups, taken in order, reproduce a Gauss-Seidel sweep.
+struct Schedule {
+    int ngroups = 0;
+    int max_group = 0;
+    DevBuf<int> perm;       // rows, group by group
+    DevBuf<int> group_ptr;  // ngroups + 1 offsets into perm
+    DevBuf<int> rank;       // per row: neighbours of lower rank are read updated
+    std::vector<int> h_group_ptr;
+};
+
+enum SmootherOrder {
+    // Level schedule of the natural ordering: identical results to the
+    // reference's sequential sweeps.
+    ORDER_EXACT = 0,
+    // Greedy multicolour ordering: Gauss-Seidel in colour order, far fewer
+    // groups (a different but equally valid smoother).
+    ORDER_MULTICOLOR = 1,
+};
+
+enum LevelSmoother {
+    SMOOTH_EXACT_GS = 0,  // sequential-order Gauss-Seidel (level schedule, bit-exact)
+    SMOOTH_COLOR_GS = 1,  // multicolour Gauss-Seidel, one launch per colour
+    SMOOTH_L1_JACOBI = 2, // l1-Jacobi (dense coarse levels in multicolour mode)
+};
+
+struct AmgLevel {
+    int smoother = SMOOTH_EXACT_GS;
+    int lanes = 1;           // lanes per row of the vectorised CSR kernels
+    DevBuf<double> dinv;     // l1-Jacobi inverse weights
+    DeviceCsr A;          // level operator (diagonal first in every row)
+    DeviceCsr P;          // interpolation to this level from level+1 (n x nc)
+    DeviceCsr R;          // P^T, rows listing fine points ascending
+    std::vector<int> cf;  // host copy of the C/F splitting (tests)
+    Schedule fwd, bwd;    // Gauss-Seidel schedules
+    DevBuf<double> f, u;  // right-hand side and iterate of this level
+};
+
+struct AmgParams {
+    int max_levels = 25;
+    int coarse_threshold = 1000;
+    double strong_threshold = 0.25;
+    double max_row_sum = 0.9;
+    int order = ORDER_EXACT;
+    int coarse_exact = 1;  // 1: substitution in the reference's order; 0: explicit inverse (GEMV)
+    int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
+};
+
+struct Amg {
+    AmgParams prm;
+    std::vector<std::unique_ptr<AmgLevel>> levels;
+    // coarsest level dense factors (row-major n x n), L stored transposed
+    int nc = 0;
+    DevBuf<double> Ufac, Lt, Ainv;
+    DevBuf<double> work;  // residual of the finest level
+    DevBuf<int> err;      // device error flag of the smoothers
+    int num_levels() const { return (int)levels.size(); }
+};
+
+// amg_setup.cu
+void amg_strength(const CsrView<double> &A, double theta, double max_row_sum, DevPattern &S, cudaStream_t s);
+void amg_pmis(const DevPattern &S, int *cf_dev, cudaStream_t s);
+int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *cf_dev, DeviceCsr &P,
+                     cudaStream_t s);
+void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, DeviceCsr &Ac, cudaStream_t s,
+             long long table_budget_entries = (1LL << 27));
+
+// setup_host.cu (sequential graph passes)
+void rs_first_pass_host(int n, const int *sia, const int *sja, int *cf);
+void build_schedule_host(int n, const int *ia, const int *ja, int order, bool forward, std::vector<int> &perm,
+                         std::vector<int> &group_ptr, std::vector<int> &rank);
+void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr, const std::vector<int> &rank,
+                     Schedule &S, cudaStream_t s);
+
+// amg.cu
+void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s);
+void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s);  // one V(1,1), u0 in/out
+void coarse_setup(Amg &H, cudaStream_t s);
+void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s);
+
+// smoother_fast.cu
+int lanes_for(double mean_row);
+void l1_diag(const CsrView<double> &A, double *dinv, cudaStream_t s);
+void gs_sweep_colors(const CsrView<double> &A, const Schedule &sch, int V, const double *f, double *u,
+                     cudaStream_t s);
+void jacobi_l1_sweep(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u,
+                     double *tmp, cudaStream_t s);
+void residual_vec(const CsrView<double> &A, int V, const double *f, const double *u, double *r, cudaStream_t s);
+void spmv_vec(const CsrView<double> &A, int V, double alpha, const double *x, double beta, double *y,
+              cudaStream_t s);
+
+// smoother.cu
+void hgs_sweep_groups(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
+                      double *vt, double w, double omega, cudaStream_t s);
+// One Gauss-Seidel sweep of A u = f along `sch` (relax_weight = omega = 1,
+// rows with a zero diagonal skipped): jxf_PAMGRelax6's forward or backward
+// pass.
+void gs_sweep(const CsrView<double> &A, const Schedule &sch, const double *f, double *u, const int *rank,
+              double *vt, int *err, cudaStream_t s);
+// Stage-2 block hybrid Gauss-Seidel (jxf_ParBSRHGSRelax) along `sch`; vt is
+// scratch (nb*bs) that receives the iterate at sweep start.
+void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
+               double *vt, double w, double omega, int *err, cudaStream_t s);
+
+}  // namespace jxcpr

@@ -1,0 +1,616 @@
+// Setup of the pressure AMG hierarchy as CPR configures it
+// (jxfpamg-0220/csrc/cpr/jxf_cpr.c:319-377): classical strength, HMIS
+// coarsening, extended+i interpolation, Galerkin coarse operator.
+//
+// Every numeric and ordering decision follows the reference so that the CF
+// splitting, the interpolation pattern and values and the coarse operators
+// are bit-identical (checked against the oracle and the golden fixtures):
+//
+// * strength      -- jxf_PAMGCreateS, amg/par_strength.c:20-415; one thread
+//                    per row, S keeps A's column order without the diagonal.
+// * HMIS          -- amg/par_coarsen_hmis.c:20-37: the Ruge-Stueben first
+//                    pass (par_coarsen_ruge.c:249-420) is a sequential greedy
+//                    on a bucket list and runs on the host (rs_first_pass in
+//                    setup_host.cpp); the PMIS completion
+//                    (par_coarsen_pmis.c:27-719) runs here.  Its result does
+//                    not depend on the order points are visited, so a
+//                    parallel sweep per round reproduces it; the random
+//                    tie-breaks are the reference's Park-Miller sequence from
+//                    seed 2747 (par_indepset.c:19-55), computed per point by
+//                    jumping ahead a^(i+1) mod (2^31-1).
+// * ext+i         -- jxf_PAMGBuildExtPIInterp, amg/par_interp_6.c:19-790; one
+//                    thread per fine row runs the reference's row procedure,
+//                    with the row's interpolation set kept in a scratch list
+//                    (discovery order) instead of the global marker array.
+// * Galerkin      -- jxf_PAMGBuildCoarseOperatorKT,
+//                    operation/matops/par_rap.c:185: one thread per coarse
+//                    row walks R row -> A row -> P row, diagonal first, new
+//                    columns appended in discovery order, products (r*a)*p
+//                    accumulated in traversal order, with a per-row open-
+//                    addressing table mapping column -> slot.
+#include <algorithm>
+#include <vector>
+
+#include "amg.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace jxcpr {
+
+// ---------------------------------------------------------------------------
+// Strength of connection
+// ---------------------------------------------------------------------------
+__global__ void strength_mark_kernel(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                                     const double *__restrict__ a, double theta, double max_row_sum,
+                                     unsigned char *__restrict__ mark, int *__restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d = ia[i], e = ia[i + 1];
+    if (d == e) {  // empty row: no connections (the reference assumes a stored diagonal)
+        cnt[i] = 0;
+        return;
+    }
+    const double diag = a[d];
+    double row_scale = 0.0, row_sum = diag;
+    if (diag < 0) {
+        for (int k = d + 1; k < e; ++k) {
+            const double v = a[k];
+            row_scale = row_scale < v ? v : row_scale;
+            row_sum += v;
+        }
+    } else {
+        for (int k = d + 1; k < e; ++k) {
+            const double v = a[k];
+            row_scale = row_scale < v ? row_scale : v;
+            row_sum += v;
+        }
+    }
+    row_sum = fabs(row_sum / diag);
+    int c = 0;
+    mark[d] = 0;
+    if ((row_sum > max_row_sum) && (max_row_sum < 1.0)) {
+        for (int k = d + 1; k < e; ++k) mark[k] = 0;
+    } else if (diag < 0) {
+        for (int k = d + 1; k < e; ++k) {
+            const unsigned char m = !(a[k] <= theta * row_scale);
+            mark[k] = m;
+            c += m;
+        }
+    } else {
+        for (int k = d + 1; k < e; ++k) {
+            const unsigned char m = !(a[k] >= theta * row_scale);
+            mark[k] = m;
+            c += m;
+        }
+    }
+    cnt[i] = c;
+}
+
+__global__ void strength_fill_kernel(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                                     const unsigned char *__restrict__ mark, const int *__restrict__ sia,
+                                     int *__restrict__ sja) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = sia[i];
+    for (int k = ia[i]; k < ia[i + 1]; ++k)
+        if (mark[k]) sja[p++] = ja[k];
+}
+
+void amg_strength(const CsrView<double> &A, double theta, double max_row_sum, DevPattern &S, cudaStream_t s) {
+    const int n = A.nrows;
+    DevBuf<unsigned char> mark(A.nnz > 0 ? A.nnz : 1);
+    DevBuf<int> cnt(n + 1);
+    cnt.zero(s);
+    strength_mark_kernel<<<div_up(n, 256), 256, 0, s>>>(n, A.ia, A.ja, A.a, theta, max_row_sum, mark.get(),
+                                                        cnt.get());
+    JX_LAUNCH_CHECK();
+    S.n = n;
+    S.ia.alloc(n + 1);
+    exclusive_scan_int(cnt.get(), S.ia.get(), n + 1, s);
+    int nnz = 0;
+    JX_CUDA(cudaMemcpyAsync(&nnz, S.ia.get() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    S.nnz = nnz;
+    S.ja.alloc(nnz > 0 ? nnz : 1);
+    strength_fill_kernel<<<div_up(n, 256), 256, 0, s>>>(n, A.ia, A.ja, mark.get(), S.ia.get(), S.ja.get());
+    JX_LAUNCH_CHECK();
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// PMIS completion of HMIS
+// ---------------------------------------------------------------------------
+#define CF_C 1
+#define CF_F (-1)
+#define CF_Z (-2)
+#define CF_SF (-3)
+
+__global__ void col_count_kernel(long long nnz, const int *__restrict__ ja, int *__restrict__ cnt) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nnz) atomicAdd(cnt + ja[k], 1);
+}
+
+// Park-Miller: seed_{i+1} = 16807 * seed_i mod (2^31 - 1); the i-th draw after
+// seeding with s0 is s0 * 16807^(i+1) mod m, divided by m.
+__device__ __forceinline__ unsigned long long pm_pow(unsigned long long e) {
+    const unsigned long long m = 2147483647ULL;
+    unsigned long long r = 1, b = 16807ULL;
+    while (e) {
+        if (e & 1ULL) r = (r * b) % m;
+        b = (b * b) % m;
+        e >>= 1;
+    }
+    return r;
+}
+
+__global__ void pmis_init_kernel(int n, const int *__restrict__ sia, const int *__restrict__ colcnt,
+                                 double *__restrict__ measure, int *__restrict__ cf,
+                                 unsigned char *__restrict__ in_graph) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long m = 2147483647ULL;
+    const unsigned long long seed = (2747ULL * pm_pow((unsigned long long)i + 1ULL)) % m;
+    double meas = (double)colcnt[i];
+    meas += (double)(int)seed / 2147483647.0;
+    int c = cf[i];
+    unsigned char g = 0;
+    if (c == -1) c = 0;
+    if (c == CF_Z) {
+        if (meas >= 1.0 || (sia[i + 1] - sia[i]) > 0) {
+            c = 0;
+            g = 1;
+        } else {
+            c = CF_F;
+        }
+    } else if (c == CF_SF) {
+        meas = 0.0;
+    } else {
+        g = 1;
+    }
+    cf[i] = c;
+    measure[i] = meas;
+    in_graph[i] = g;
+}
+
+__global__ void pmis_is_init_kernel(int n, const double *__restrict__ measure, const unsigned char *__restrict__ g,
+                                    int *__restrict__ cf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && g[i] && measure[i] > 1) cf[i] = 1;
+}
+
+__global__ void pmis_is_remove_kernel(int n, const int *__restrict__ sia, const int *__restrict__ sja,
+                                      const double *__restrict__ measure, const unsigned char *__restrict__ g,
+                                      int *__restrict__ cf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !g[i]) return;
+    const double mi = measure[i];
+    if (!(mi > 1)) return;
+    for (int k = sia[i]; k < sia[i + 1]; ++k) {
+        int j = sja[k];
+        if (j < 0) j = -j - 1;
+        const double mj = measure[j];
+        if (mj > 1) {
+            if (mi > mj) cf[j] = 0;
+            else if (mj > mi) cf[i] = 0;
+        }
+    }
+}
+
+__global__ void pmis_set_cf_kernel(int n, const int *__restrict__ sia, int *__restrict__ sja,
+                                   const double *__restrict__ measure, const unsigned char *__restrict__ g,
+                                   int *__restrict__ cf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !g[i]) return;
+    const int kb = sia[i], ke = sia[i + 1];
+    int c = cf[i];
+    bool remove = false;
+    if (measure[i] < 1.0) {
+        c = CF_F;
+        remove = true;
+    }
+    if (c > 0) {
+        c = CF_C;
+        remove = true;
+    } else {
+        for (int k = kb; k < ke; ++k) {
+            int j = sja[k];
+            if (j < 0) j = -j - 1;
+            if (j != i && cf[j] > 0) c = CF_F;  // a neighbour's own entry is never i (S has no diagonal)
+        }
+        if (c == CF_F) remove = true;
+    }
+    cf[i] = c;
+    if (remove)
+        for (int k = kb; k < ke; ++k)
+            if (sja[k] > -1) sja[k] = -sja[k] - 1;
+}
+
+__global__ void pmis_remove_edges_kernel(int n, const int *__restrict__ sia, int *__restrict__ sja,
+                                         const unsigned char *__restrict__ g, const int *__restrict__ cf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !g[i] || cf[i] != 0) return;
+    for (int k = sia[i]; k < sia[i + 1]; ++k) {
+        int j = sja[k];
+        if (j < 0) j = -j - 1;
+        if (cf[j] != 0 && sja[k] > -1) sja[k] = -sja[k] - 1;
+    }
+}
+
+__global__ void pmis_update_graph_kernel(int n, double *__restrict__ measure, unsigned char *__restrict__ g,
+                                         const int *__restrict__ cf, int *__restrict__ remaining) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !g[i]) return;
+    if (cf[i] != 0) {
+        measure[i] = 0.0;
+        g[i] = 0;
+    } else {
+        atomicAdd(remaining, 1);
+    }
+}
+
+__global__ void count_flag_kernel(int n, const unsigned char *__restrict__ g, int *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && g[i]) atomicAdd(out, 1);
+}
+
+void amg_pmis(const DevPattern &S, int *cf_dev, cudaStream_t s) {
+    const int n = S.n;
+    DevBuf<int> sja(S.nnz > 0 ? S.nnz : 1), colcnt(n), counter(1);
+    DevBuf<double> measure(n);
+    DevBuf<unsigned char> g(n);
+    if (S.nnz) JX_CUDA(cudaMemcpyAsync(sja.get(), S.ja.get(), sizeof(int) * S.nnz, cudaMemcpyDeviceToDevice, s));
+    colcnt.zero(s);
+    if (S.nnz) {
+        col_count_kernel<<<div_up(S.nnz, 256), 256, 0, s>>>(S.nnz, S.ja.get(), colcnt.get());
+        JX_LAUNCH_CHECK();
+    }
+    const int grid = div_up(n, 256);
+    pmis_init_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), colcnt.get(), measure.get(), cf_dev, g.get());
+    JX_LAUNCH_CHECK();
+    counter.zero(s);
+    count_flag_kernel<<<grid, 256, 0, s>>>(n, g.get(), counter.get());
+    JX_LAUNCH_CHECK();
+    int remaining = 0;
+    JX_CUDA(cudaMemcpyAsync(&remaining, counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    int iter = 0;
+    while (remaining > 0) {
+        if (iter > 20000) {
+            set_error("pmis: no progress");
+            throw CudaError{cudaErrorUnknown, "pmis"};
+        }
+        if (iter) {
+            pmis_is_init_kernel<<<grid, 256, 0, s>>>(n, measure.get(), g.get(), cf_dev);
+            JX_LAUNCH_CHECK();
+            pmis_is_remove_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), sja.get(), measure.get(), g.get(), cf_dev);
+            JX_LAUNCH_CHECK();
+        }
+        ++iter;
+        pmis_set_cf_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), sja.get(), measure.get(), g.get(), cf_dev);
+        JX_LAUNCH_CHECK();
+        pmis_remove_edges_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), sja.get(), g.get(), cf_dev);
+        JX_LAUNCH_CHECK();
+        counter.zero(s);
+        pmis_update_graph_kernel<<<grid, 256, 0, s>>>(n, measure.get(), g.get(), cf_dev, counter.get());
+        JX_LAUNCH_CHECK();
+        JX_CUDA(cudaMemcpyAsync(&remaining, counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Extended+i interpolation
+// ---------------------------------------------------------------------------
+__global__ void c_flag_kernel(int n, const int *__restrict__ cf, int *__restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = cf[i] >= 0 ? 1 : 0;
+}
+
+// Upper bound of the interpolation set size of each fine row.
+__global__ void interp_bound_kernel(int n, const int *__restrict__ sia, const int *__restrict__ sja,
+                                    const int *__restrict__ cf, long long *__restrict__ bound) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long b = 0;
+    const int ci = cf[i];
+    if (ci >= 0) {
+        b = 1;
+    } else if (ci != CF_SF) {
+        for (int k = sia[i]; k < sia[i + 1]; ++k) {
+            const int i1 = sja[k];
+            const int c1 = cf[i1];
+            if (c1 >= 0) b += 1;
+            else if (c1 != CF_SF) b += sia[i1 + 1] - sia[i1];
+        }
+    }
+    bound[i] = b;
+}
+
+__device__ __forceinline__ int find_in(const int *list, int len, int v) {
+    for (int t = 0; t < len; ++t)
+        if (list[t] == v) return t;
+    return -1;
+}
+
+// Discovery-ordered interpolation set of each F row (fine indices, deduped).
+__global__ void interp_list_kernel(int n, const int *__restrict__ sia, const int *__restrict__ sja,
+                                   const int *__restrict__ cf, const long long *__restrict__ boff,
+                                   int *__restrict__ scratch, int *__restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ci = cf[i];
+    if (ci >= 0) {
+        cnt[i] = 1;
+        return;
+    }
+    if (ci == CF_SF) {
+        cnt[i] = 0;
+        return;
+    }
+    int *list = scratch + boff[i];
+    int len = 0;
+    for (int k = sia[i]; k < sia[i + 1]; ++k) {
+        const int i1 = sja[k];
+        const int c1 = cf[i1];
+        if (c1 >= 0) {
+            if (find_in(list, len, i1) < 0) list[len++] = i1;
+        } else if (c1 != CF_SF) {
+            for (int q = sia[i1]; q < sia[i1 + 1]; ++q) {
+                const int k1 = sja[q];
+                if (cf[k1] >= 0 && find_in(list, len, k1) < 0) list[len++] = k1;
+            }
+        }
+    }
+    cnt[i] = len;
+}
+
+__device__ __forceinline__ bool is_strong_f(const int *__restrict__ sia, const int *__restrict__ sja,
+                                            const int *__restrict__ cf, int i, int i1) {
+    const int c1 = cf[i1];
+    if (c1 >= 0 || c1 == CF_SF) return false;
+    for (int k = sia[i]; k < sia[i + 1]; ++k)
+        if (sja[k] == i1) return true;
+    return false;
+}
+
+__global__ void interp_fill_kernel(int n, const int *__restrict__ aia, const int *__restrict__ aja,
+                                   const double *__restrict__ aa, const int *__restrict__ sia,
+                                   const int *__restrict__ sja, const int *__restrict__ cf,
+                                   const int *__restrict__ f2c, const long long *__restrict__ boff,
+                                   const int *__restrict__ scratch, const int *__restrict__ pia,
+                                   int *__restrict__ pja, double *__restrict__ pa) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ci = cf[i];
+    const int jb = pia[i];
+    if (ci >= 0) {
+        pja[jb] = f2c[i];
+        pa[jb] = 1.0;
+        return;
+    }
+    if (ci == CF_SF) return;
+    const int *list = scratch + boff[i];
+    const int len = pia[i + 1] - jb;
+    for (int t = 0; t < len; ++t) {
+        pja[jb + t] = f2c[list[t]];
+        pa[jb + t] = 0.0;
+    }
+    if (aia[i] == aia[i + 1]) return;  // empty row
+    double diagonal = aa[aia[i]];
+    for (int k = aia[i] + 1; k < aia[i + 1]; ++k) {
+        const int i1 = aja[k];
+        const int slot = find_in(list, len, i1);
+        if (slot >= 0) {
+            pa[jb + slot] += aa[k];
+        } else if (is_strong_f(sia, sja, cf, i, i1)) {
+            double sum = 0.0;
+            int sgn = 1;
+            if (aia[i1] < aia[i1 + 1] && aa[aia[i1]] < 0) sgn = -1;
+            for (int q = aia[i1] + 1; q < aia[i1 + 1]; ++q) {
+                const int i2 = aja[q];
+                if ((find_in(list, len, i2) >= 0 || i2 == i) && (sgn * aa[q]) < 0) sum += aa[q];
+            }
+            if (sum != 0) {
+                const double distribute = aa[k] / sum;
+                for (int q = aia[i1] + 1; q < aia[i1 + 1]; ++q) {
+                    const int i2 = aja[q];
+                    const int s2 = find_in(list, len, i2);
+                    if (s2 >= 0 && (sgn * aa[q]) < 0) pa[jb + s2] += distribute * aa[q];
+                    if (i2 == i && (sgn * aa[q]) < 0) diagonal += distribute * aa[q];
+                }
+            } else {
+                diagonal += aa[k];
+            }
+        } else if (cf[i1] != CF_SF) {
+            diagonal += aa[k];
+        }
+    }
+    for (int t = 0; t < len; ++t) pa[jb + t] /= -diagonal;
+}
+
+int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *cf_dev, DeviceCsr &P,
+                     cudaStream_t s) {
+    const int n = A.nrows;
+    const int grid = div_up(n, 256);
+    DevBuf<int> flag(n + 1), f2c(n + 1), cnt(n + 1);
+    c_flag_kernel<<<grid, 256, 0, s>>>(n, cf_dev, flag.get());
+    JX_LAUNCH_CHECK();
+    exclusive_scan_int(flag.get(), f2c.get(), n + 1, s);
+    int nc = 0;
+    JX_CUDA(cudaMemcpyAsync(&nc, f2c.get() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DevBuf<long long> bound(n + 1), boff(n + 1);
+    bound.zero(s);
+    interp_bound_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), S.ja.get(), cf_dev, bound.get());
+    JX_LAUNCH_CHECK();
+    exclusive_scan_ll(bound.get(), boff.get(), n + 1, s);
+    long long total = 0;
+    JX_CUDA(cudaMemcpyAsync(&total, boff.get() + n, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    DevBuf<int> scratch(total > 0 ? total : 1);
+    cnt.zero(s);
+    interp_list_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), S.ja.get(), cf_dev, boff.get(), scratch.get(),
+                                            cnt.get());
+    JX_LAUNCH_CHECK();
+    DevBuf<int> pia(n + 1);
+    exclusive_scan_int(cnt.get(), pia.get(), n + 1, s);
+    int nnz = 0;
+    JX_CUDA(cudaMemcpyAsync(&nnz, pia.get() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    P.nrows = n;
+    P.ncols = nc;
+    P.nnz = nnz;
+    P.ia = std::move(pia);
+    P.ja.alloc(nnz > 0 ? nnz : 1);
+    P.a.alloc(nnz > 0 ? nnz : 1);
+    interp_fill_kernel<<<grid, 256, 0, s>>>(n, A.ia, A.ja, A.a, S.ia.get(), S.ja.get(), cf_dev, f2c.get(),
+                                            boff.get(), scratch.get(), P.ia.get(), P.ja.get(), P.a.get());
+    JX_LAUNCH_CHECK();
+    JX_CUDA(cudaStreamSynchronize(s));
+    return nc;
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin coarse operator A_c = R A P (R = P^T, stable transpose)
+// ---------------------------------------------------------------------------
+__global__ void rap_bound_kernel(int nc, const int *__restrict__ ria, const int *__restrict__ rja,
+                                 const int *__restrict__ aia, const int *__restrict__ aja,
+                                 const int *__restrict__ pia, long long *__restrict__ tsize) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc) return;
+    long long b = 1;
+    for (int r = ria[I]; r < ria[I + 1]; ++r) {
+        const int i = rja[r];
+        for (int k = aia[i]; k < aia[i + 1]; ++k) {
+            const int j = aja[k];
+            b += pia[j + 1] - pia[j];
+        }
+    }
+    // open-addressing table of at least 2x the bound, power of two
+    long long t = 16;
+    while (t < 2 * b) t <<= 1;
+    tsize[I] = t;
+}
+
+__device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 2654435761u; }
+
+// Returns the slot of column J (inserting it with slot `next` if absent).
+__device__ __forceinline__ int table_slot(int *keys, int *vals, long long tsz, int J, int &next, bool &fresh) {
+    unsigned h = hash_col(J) & (unsigned)(tsz - 1);
+    while (true) {
+        const int k = keys[h];
+        if (k == J) {
+            fresh = false;
+            return vals[h];
+        }
+        if (k < 0) {
+            keys[h] = J;
+            vals[h] = next;
+            fresh = true;
+            return next++;
+        }
+        h = (h + 1) & (unsigned)(tsz - 1);
+    }
+}
+
+template <bool FILL>
+__global__ void rap_row_kernel(int I0, int I1, const int *__restrict__ ria, const int *__restrict__ rja,
+                               const double *__restrict__ ra, const int *__restrict__ aia,
+                               const int *__restrict__ aja, const double *__restrict__ aa,
+                               const int *__restrict__ pia, const int *__restrict__ pja,
+                               const double *__restrict__ pa, const long long *__restrict__ toff,
+                               long long tbase, int *__restrict__ tkeys, int *__restrict__ tvals,
+                               int *__restrict__ cnt, const int *__restrict__ cia, int *__restrict__ cja,
+                               double *__restrict__ ca) {
+    const int I = I0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= I1) return;
+    const long long off = toff[I] - tbase;
+    const long long tsz = toff[I + 1] - toff[I];
+    int *keys = tkeys + off;
+    int *vals = tvals + off;
+    for (long long t = 0; t < tsz; ++t) keys[t] = -1;
+    int next = 0;
+    bool fresh;
+    const int base = FILL ? cia[I] : 0;
+    table_slot(keys, vals, tsz, I, next, fresh);  // diagonal first
+    if (FILL) {
+        cja[base] = I;
+        ca[base] = 0.0;
+    }
+    for (int r = ria[I]; r < ria[I + 1]; ++r) {
+        const int i = rja[r];
+        const double pr = FILL ? ra[r] : 0.0;
+        for (int k = aia[i]; k < aia[i + 1]; ++k) {
+            const int j = aja[k];
+            const double pav = FILL ? pr * aa[k] : 0.0;
+            for (int q = pia[j]; q < pia[j + 1]; ++q) {
+                const int J = pja[q];
+                const int slot = table_slot(keys, vals, tsz, J, next, fresh);
+                if (FILL) {
+                    if (fresh) {
+                        cja[base + slot] = J;
+                        ca[base + slot] = pav * pa[q];
+                    } else {
+                        ca[base + slot] += pav * pa[q];
+                    }
+                }
+            }
+        }
+    }
+    if (!FILL) cnt[I] = next;
+}
+
+void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, DeviceCsr &Ac, cudaStream_t s,
+             long long table_budget_entries) {
+    const int nc = P.ncols;
+    DevBuf<long long> tsize(nc + 1), toff(nc + 1);
+    tsize.zero(s);
+    rap_bound_kernel<<<div_up(nc, 256), 256, 0, s>>>(nc, R.ia.get(), R.ja.get(), A.ia, A.ja, P.ia.get(),
+                                                     tsize.get());
+    JX_LAUNCH_CHECK();
+    exclusive_scan_ll(tsize.get(), toff.get(), nc + 1, s);
+    std::vector<long long> h_off(nc + 1);
+    JX_CUDA(cudaMemcpyAsync(h_off.data(), toff.get(), sizeof(long long) * (nc + 1), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    // chunks of coarse rows whose tables fit the budget
+    std::vector<int> cuts{0};
+    while (cuts.back() < nc) {
+        const int a0 = cuts.back();
+        int b = (int)(std::upper_bound(h_off.begin() + a0 + 1, h_off.end(), h_off[a0] + table_budget_entries) -
+                      h_off.begin()) - 1;
+        if (b <= a0) b = a0 + 1;
+        if (b > nc) b = nc;
+        cuts.push_back(b);
+    }
+    long long max_chunk = 1;
+    for (size_t c = 1; c < cuts.size(); ++c) max_chunk = std::max(max_chunk, h_off[cuts[c]] - h_off[cuts[c - 1]]);
+    DevBuf<int> tkeys(max_chunk), tvals(max_chunk), cnt(nc + 1);
+    cnt.zero(s);
+    for (size_t c = 1; c < cuts.size(); ++c) {
+        const int I0 = cuts[c - 1], I1 = cuts[c];
+        rap_row_kernel<false><<<div_up(I1 - I0, 128), 128, 0, s>>>(
+            I0, I1, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
+            toff.get(), h_off[I0], tkeys.get(), tvals.get(), cnt.get(), nullptr, nullptr, nullptr);
+        JX_LAUNCH_CHECK();
+    }
+    DevBuf<int> cia(nc + 1);
+    exclusive_scan_int(cnt.get(), cia.get(), nc + 1, s);
+    int nnz = 0;
+    JX_CUDA(cudaMemcpyAsync(&nnz, cia.get() + nc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    Ac.nrows = nc;
+    Ac.ncols = nc;
+    Ac.nnz = nnz;
+    Ac.ia = std::move(cia);
+    Ac.ja.alloc(nnz > 0 ? nnz : 1);
+    Ac.a.alloc(nnz > 0 ? nnz : 1);
+    for (size_t c = 1; c < cuts.size(); ++c) {
+        const int I0 = cuts[c - 1], I1 = cuts[c];
+        rap_row_kernel<true><<<div_up(I1 - I0, 128), 128, 0, s>>>(
+            I0, I1, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
+            toff.get(), h_off[I0], tkeys.get(), tvals.get(), nullptr, Ac.ia.get(), Ac.ja.get(), Ac.a.get());
+        JX_LAUNCH_CHECK();
+    }
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace jxcpr

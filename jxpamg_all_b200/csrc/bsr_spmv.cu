@@ -89,42 +89,11 @@ __device__ __forceinline__ X row_init(const X *y, long long idx, int init_mode, 
 }
 
 
-// Accumulates one output component of a block row.  Rows with at most MAXK
-// blocks (every row of a 7-point stencil) first fetch all column indices,
-// then issue all x gathers, then accumulate in stored order: the gathers are
-// in flight together instead of one L2 round trip per block.  The summation
-// order is unchanged, so the result stays bit-identical.
+// Accumulates one output component of a block row in stored block order.
 template <int BS, typename V, typename X, bool SMEM>
 __device__ __forceinline__ X row_accumulate(X acc, long long kb, long long ke, long long kbase,
                                             const V *__restrict__ vals, const int *__restrict__ cols,
                                             const X *__restrict__ x, int comp) {
-    constexpr int MAXK = 8;
-    const int nk = (int)(ke - kb);
-    if (nk <= MAXK) {
-        int cc[MAXK];
-        V av[MAXK][BS];
-        X xv[MAXK][BS];
-#pragma unroll
-        for (int q = 0; q < MAXK; ++q) {
-            if (q < nk) {
-                const long long k = kb + q - kbase;
-                cc[q] = SMEM ? cols[k] : __ldg(cols + k);
-#pragma unroll
-                for (int j = 0; j < BS; ++j)
-                    av[q][j] = SMEM ? vals[k * (BS * BS) + comp * BS + j] : __ldg(vals + k * (BS * BS) + comp * BS + j);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < MAXK; ++q)
-            if (q < nk) gather_x<BS, X>(x, cc[q], xv[q]);
-#pragma unroll
-        for (int q = 0; q < MAXK; ++q)
-            if (q < nk) {
-#pragma unroll
-                for (int j = 0; j < BS; ++j) acc = acc + (X)av[q][j] * xv[q][j];
-            }
-        return acc;
-    }
     for (long long k = kb; k < ke; ++k) {
         const long long kk = k - kbase;
         const int c = SMEM ? cols[kk] : __ldg(cols + kk);

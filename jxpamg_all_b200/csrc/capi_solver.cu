@@ -1,0 +1,239 @@
+// C ABI of the solver object: setup / solve with host or device arrays,
+// string-keyed options (the reference's JXF_CPRSetParameter style), and
+// inspection of the AMG hierarchy for parity tests.
+#include <string.h>
+
+#include <new>
+
+#include "jxcpr_b200.h"
+#include "solver.cuh"
+
+using namespace jxcpr;
+
+struct jxcpr_solver {
+    Solver s;
+};
+
+namespace {
+template <typename F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const CudaError &) {
+        return JXCPR_ERROR_DEVICE;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return JXCPR_ERROR_MEMORY;
+    } catch (...) {
+        set_error("unexpected exception");
+        return JXCPR_ERROR_GENERIC;
+    }
+}
+
+int set_int_param(SolverParams &p, const char *key, int v) {
+    struct {
+        const char *k;
+        int *f;
+    } tab[] = {{"k_dim", &p.k_dim},
+               {"max_iter", &p.max_iter},
+               {"min_iter", &p.min_iter},
+               {"is_check_restarted", &p.is_check_restarted},
+               {"print_level", &p.print_level},
+               {"logging", &p.logging},
+               {"pressure_index", &p.pressure_index},
+               {"stage1_maxit", &p.stage1_maxit},
+               {"stage2_maxit", &p.stage2_maxit},
+               {"stage1_solver_type", &p.stage1_solver_type},
+               {"stage2_solver_type", &p.stage2_solver_type},
+               {"decouple", &p.decouple},
+               {"consistent_rhs", &p.consistent_rhs},
+               {"smoother_order", &p.smoother_order},
+               {"coarse_exact", &p.coarse_exact},
+               {"max_colors", &p.max_colors},
+               {"use_tma_spmv", &p.use_tma_spmv}};
+    if (!key) return JXCPR_ERROR_ARG;
+    if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
+    for (auto &e : tab)
+        if (!strcmp(key, e.k)) {
+            *e.f = v;
+            return JXCPR_SUCCESS;
+        }
+    set_error("unknown integer parameter '%s'", key);
+    return JXCPR_ERROR_ARG;
+}
+
+int set_real_param(SolverParams &p, const char *key, double v) {
+    struct {
+        const char *k;
+        double *f;
+    } tab[] = {{"tol", &p.tol},
+               {"a_tol", &p.a_tol},
+               {"threshold", &p.threshold},
+               {"convfac_threshold", &p.convfac_threshold},
+               {"stage2_relax_weight", &p.stage2_relax_weight},
+               {"stage2_omega", &p.stage2_omega}};
+    if (!key) return JXCPR_ERROR_ARG;
+    for (auto &e : tab)
+        if (!strcmp(key, e.k)) {
+            *e.f = v;
+            return JXCPR_SUCCESS;
+        }
+    set_error("unknown real parameter '%s'", key);
+    return JXCPR_ERROR_ARG;
+}
+}  // namespace
+
+extern "C" {
+
+int jxcpr_solver_create(jxcpr_solver **h) {
+    if (!h) return JXCPR_ERROR_ARG;
+    *h = new (std::nothrow) jxcpr_solver();
+    return *h ? JXCPR_SUCCESS : JXCPR_ERROR_MEMORY;
+}
+
+int jxcpr_solver_destroy(jxcpr_solver *h) {
+    if (!h) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        cudaStream_t st = h->s.owns_stream ? h->s.stream : nullptr;
+        delete h;
+        if (st) cudaStreamDestroy(st);
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_set_int(jxcpr_solver *h, const char *key, int value) {
+    if (!h) return JXCPR_ERROR_ARG;
+    return set_int_param(h->s.prm, key, value);
+}
+
+int jxcpr_solver_set_real(jxcpr_solver *h, const char *key, double value) {
+    if (!h) return JXCPR_ERROR_ARG;
+    return set_real_param(h->s.prm, key, value);
+}
+
+int jxcpr_solver_setup(jxcpr_solver *h, int nb, int bs, long long nnzb, const int *ia, const int *ja,
+                       const double *a, int device) {
+    if (!h || nb < 0 || nnzb < 0 || (bs != 2 && bs != 3) || !ia || (nnzb && (!ja || !a))) {
+        set_error("solver_setup: bad arguments");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        h->s.setup(nb, bs, nnzb, ia, ja, a, device);
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_solve(jxcpr_solver *h, const double *b, double *x, int device, int *iterations,
+                       double *rel_residual) {
+    if (!h || !b || !x || !h->s.cpr.ready) {
+        set_error("solver_solve: bad arguments or no setup");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        GmresResult r = h->s.solve(b, x, device);
+        if (iterations) *iterations = r.iterations;
+        if (rel_residual) *rel_residual = r.rel_residual;
+        if (r.status) return r.status;
+        return r.converged ? JXCPR_SUCCESS : JXCPR_ERROR_CONV;
+    });
+}
+
+int jxcpr_solver_get_norms(jxcpr_solver *h, double *norms, int capacity) {
+    if (!h || !norms) return -1;
+    const int n = (int)h->s.last.norms.size();
+    for (int i = 0; i < n && i < capacity; ++i) norms[i] = h->s.last.norms[i];
+    return n;
+}
+
+int jxcpr_solver_stats(jxcpr_solver *h, double *stats) {
+    if (!h || !stats) return JXCPR_ERROR_ARG;
+    stats[0] = h->s.setup_ms;
+    stats[1] = h->s.solve_ms;
+    stats[2] = h->s.cpr.stats[0];
+    stats[3] = (double)h->s.cpr.amg.num_levels();
+    return JXCPR_SUCCESS;
+}
+
+int jxcpr_solver_num_levels(jxcpr_solver *h) { return h ? h->s.cpr.amg.num_levels() : -1; }
+
+int jxcpr_solver_level_sizes(jxcpr_solver *h, int lev, int what, int *sizes) {
+    if (!h || !sizes || lev < 0 || lev >= h->s.cpr.amg.num_levels()) return -1;
+    const AmgLevel &L = *h->s.cpr.amg.levels[lev];
+    const DeviceCsr &M = what == 0 ? L.A : (what == 1 ? L.P : L.R);
+    if (what != 0 && lev == h->s.cpr.amg.num_levels() - 1) return -1;
+    sizes[0] = M.nrows;
+    sizes[1] = M.ncols;
+    sizes[2] = (int)M.nnz;
+    return 0;
+}
+
+int jxcpr_solver_level_matrix(jxcpr_solver *h, int lev, int what, int *ia, int *ja, double *a) {
+    int sz[3];
+    if (jxcpr_solver_level_sizes(h, lev, what, sz) < 0) return -1;
+    return guarded([&] {
+        const AmgLevel &L = *h->s.cpr.amg.levels[lev];
+        const DeviceCsr &M = what == 0 ? L.A : (what == 1 ? L.P : L.R);
+        JX_CUDA(cudaMemcpy(ia, M.ia.get(), sizeof(int) * (sz[0] + 1), cudaMemcpyDeviceToHost));
+        JX_CUDA(cudaMemcpy(ja, M.ja.get(), sizeof(int) * sz[2], cudaMemcpyDeviceToHost));
+        JX_CUDA(cudaMemcpy(a, M.a.get(), sizeof(double) * sz[2], cudaMemcpyDeviceToHost));
+        return 0;
+    });
+}
+
+int jxcpr_solver_level_cf(jxcpr_solver *h, int lev, int *cf) {
+    if (!h || !cf || lev < 0 || lev >= h->s.cpr.amg.num_levels() - 1) return -1;
+    const std::vector<int> &v = h->s.cpr.amg.levels[lev]->cf;
+    memcpy(cf, v.data(), sizeof(int) * v.size());
+    return 0;
+}
+
+int jxcpr_solver_decoupled_values(jxcpr_solver *h, double *a_host) {
+    if (!h || !a_host) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        const DeviceBsr &A = h->s.A;
+        JX_CUDA(cudaMemcpy(a_host, A.a.get(), sizeof(double) * A.nnzb * A.bs * A.bs, cudaMemcpyDeviceToHost));
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_cpr_apply(jxcpr_solver *h, const double *r, double *z, int device) {
+    if (!h || !r || !z || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        Solver &S = h->s;
+        const long long n = (long long)S.A.nb * S.A.bs;
+        cudaStream_t st = S.stream;
+        const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        JX_CUDA(cudaMemcpyAsync(S.b.get(), r, sizeof(double) * n, in, st));
+        JX_CUDA(cudaMemsetAsync(S.x.get(), 0, sizeof(double) * n, st));
+        S.cpr.apply(S.b.get(), S.x.get(), st);
+        const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        JX_CUDA(cudaMemcpyAsync(z, S.x.get(), sizeof(double) * n, out, st));
+        JX_CUDA(cudaStreamSynchronize(st));
+        int f = 0;
+        JX_CUDA(cudaMemcpy(&f, S.cpr.amg.err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+        if (f) {
+            set_error("smoother wait timed out");
+            return JXCPR_ERROR_DEVICE;
+        }
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int device) {
+    if (!h || !rp || !xp || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        Solver &S = h->s;
+        const int nb = S.A.nb;
+        cudaStream_t st = S.stream;
+        const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        JX_CUDA(cudaMemcpyAsync(S.cpr.rp.get(), rp, sizeof(double) * nb, in, st));
+        JX_CUDA(cudaMemcpyAsync(S.cpr.xp.get(), xp, sizeof(double) * nb, in, st));
+        amg_vcycle(S.cpr.amg, S.cpr.rp.get(), S.cpr.xp.get(), st);
+        const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        JX_CUDA(cudaMemcpyAsync(xp, S.cpr.xp.get(), sizeof(double) * nb, out, st));
+        JX_CUDA(cudaStreamSynchronize(st));
+        return JXCPR_SUCCESS;
+    });
+}
+
+}  // extern "C"

@@ -30,6 +30,61 @@ struct CsrView {
     const V *a = nullptr;
 };
 
+// Owning device CSR / BSR containers.
+struct DeviceCsr {
+    int nrows = 0, ncols = 0;
+    long long nnz = 0;
+    DevBuf<int> ia, ja;
+    DevBuf<double> a;
+    void alloc(int n, int m, long long z) {
+        nrows = n;
+        ncols = m;
+        nnz = z;
+        ia.alloc((size_t)n + 1);
+        ja.alloc((size_t)(z > 0 ? z : 1));
+        a.alloc((size_t)(z > 0 ? z : 1));
+    }
+    CsrView<double> view() const { return CsrView<double>{nrows, ncols, nnz, ia.get(), ja.get(), a.get()}; }
+};
+
+struct DeviceBsr {
+    int nb = 0, bs = 0;
+    long long nnzb = 0;
+    DevBuf<int> ia, ja;
+    DevBuf<double> a;
+    void alloc(int n, int b, long long z) {
+        nb = n;
+        bs = b;
+        nnzb = z;
+        ia.alloc((size_t)n + 1);
+        ja.alloc((size_t)(z > 0 ? z : 1));
+        a.alloc((size_t)(z > 0 ? z : 1) * b * b);
+    }
+    BsrView<double> view() const { return BsrView<double>{nb, bs, nnzb, ia.get(), ja.get(), a.get()}; }
+};
+
+// ---- scan.cu ---------------------------------------------------------------
+// out[0] = 0, out[i] = in[0] + ... + in[i-1]  (n entries; int32 / int64)
+void exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
+void exclusive_scan_ll(const long long *in, long long *out, int n, cudaStream_t s);
+
+// ---- csr_ops.cu ------------------------------------------------------------
+void csr_spmv(const CsrView<double> &A, double alpha, const double *x, double beta, double *y, cudaStream_t s);
+void csr_transpose(const CsrView<double> &A, DeviceCsr &T, cudaStream_t s);
+void pattern_transpose(int n, int m, long long nnz, const int *ia, const int *ja, int *tia, int *tja, int *tperm,
+                       cudaStream_t s);
+void bsr_pressure_csr(const BsrView<double> &A, int p, DeviceCsr &Ap, cudaStream_t s);
+void restrict_pressure(int nb, int bs, int p, const double *r, double *rp, cudaStream_t s);
+void prolong_pressure(int nb, int bs, int p, const double *xp, double *x, cudaStream_t s);
+
+// ---- decouple.cu -----------------------------------------------------------
+// Matrix part of jxf_BSRMatrixDecouple (type 1 ABF, 5 True-IMPES); `coef`
+// (nb * decouple_coef_size) receives what the right-hand side update needs.
+int decouple_coef_size(int bs, int type);
+void bsr_decouple_matrix(DeviceBsr &A, int type, double *coef, cudaStream_t s);
+void bsr_decouple_rhs(int nb, int bs, int type, const double *coef, double *rhs, int consistent_rhs,
+                      cudaStream_t s);
+
 // ---- bsr_spmv.cu ---------------------------------------------------------
 // y = alpha*A*x + beta*y with the reference's rounding sequence.  `staged`
 // selects the TMA-staged persistent kernel (requires `err`, a device int set

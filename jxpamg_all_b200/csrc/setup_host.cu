@@ -1,0 +1,224 @@
+// The two inherently sequential graph passes of the setup, run on the host:
+//
+// * rs_first_pass_host -- the Ruge-Stueben first coloring pass used by HMIS
+//   (jxfpamg-0220/csrc/amg/par_coarsen_ruge.c:249-420 with the bucket lists
+//   of amg/amg_linklist.c).  It is a greedy that always takes the head of the
+//   highest non-empty measure bucket, so its result depends on the exact
+//   insertion order; it is reproduced here with O(1) bucket operations:
+//   buckets indexed by measure, points appended at the tail, the highest
+//   non-empty bucket tracked.
+// * build_schedule_host -- grouping of rows for the Gauss-Seidel sweeps on
+//   the device: either the level schedule of the natural ordering (row i
+//   waits for every j < i of its row in a forward sweep, j > i backward) or a
+//   greedy multicolouring.
+//
+// Both read the pattern once (O(nnz)); everything numeric stays on the GPU.
+#include <algorithm>
+#include <vector>
+
+#include "amg.cuh"
+
+namespace jxcpr {
+
+namespace {
+struct Buckets {
+    std::vector<int> next, prev, head, tail;
+    int maxm = 0;
+    Buckets(int n, int cap) : next(n, -1), prev(n, -1), head(cap, -1), tail(cap, -1) {}
+    void enter(int m, int i) {
+        next[i] = -1;
+        prev[i] = tail[m];
+        if (tail[m] >= 0) next[tail[m]] = i; else head[m] = i;
+        tail[m] = i;
+        if (m > maxm) maxm = m;
+    }
+    void remove(int m, int i) {
+        if (prev[i] >= 0) next[prev[i]] = next[i]; else head[m] = next[i];
+        if (next[i] >= 0) prev[next[i]] = prev[i]; else tail[m] = prev[i];
+        while (maxm > 0 && head[maxm] < 0) --maxm;
+    }
+};
+}  // namespace
+
+void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF) {
+    const int C_PT = 1, F_PT = -1, Z_PT = -2, SF_PT = -3, UNDEC = 0;
+    const int nnz = Si[n];
+    std::vector<int> STi(n + 1, 0), STj(nnz > 0 ? nnz : 1);
+    for (int k = 0; k < nnz; ++k) STi[Sj[k] + 1]++;
+    for (int i = 0; i < n; ++i) STi[i + 1] += STi[i];
+    {
+        std::vector<int> pos(STi.begin(), STi.end() - 1);
+        for (int i = 0; i < n; ++i)
+            for (int k = Si[i]; k < Si[i + 1]; ++k) STj[pos[Sj[k]]++] = i;
+    }
+    std::vector<int> measure(n);
+    int maxmeasure = 0;
+    for (int i = 0; i < n; ++i) {
+        measure[i] = STi[i + 1] - STi[i];
+        maxmeasure = std::max(maxmeasure, measure[i]);
+    }
+    Buckets B(n, maxmeasure + n + 2);
+    int num_left = 0;
+    for (int j = 0; j < n; ++j) {
+        if (Si[j + 1] - Si[j] == 0) {
+            CF[j] = SF_PT;
+            measure[j] = 0;
+        } else {
+            CF[j] = UNDEC;
+            ++num_left;
+        }
+    }
+    for (int j = 0; j < n; ++j) {
+        const int m = measure[j];
+        if (CF[j] == SF_PT) continue;
+        if (m > 0) {
+            B.enter(m, j);
+        } else {
+            CF[j] = Z_PT;
+            for (int k = Si[j]; k < Si[j + 1]; ++k) {
+                const int nb = Sj[k];
+                if (CF[nb] != SF_PT) {
+                    if (nb < j) {
+                        int nm = measure[nb];
+                        if (nm > 0) B.remove(nm, nb);
+                        nm = ++measure[nb];
+                        B.enter(nm, nb);
+                    } else {
+                        ++measure[nb];
+                    }
+                }
+            }
+            --num_left;
+        }
+    }
+    while (num_left > 0) {
+        const int index = B.head[B.maxm];
+        CF[index] = C_PT;
+        const int m = measure[index];
+        measure[index] = 0;
+        --num_left;
+        B.remove(m, index);
+        for (int k = STi[index]; k < STi[index + 1]; ++k) {
+            const int nb = STj[k];
+            if (CF[nb] == UNDEC) {
+                CF[nb] = F_PT;
+                B.remove(measure[nb], nb);
+                --num_left;
+                for (int q = Si[nb]; q < Si[nb + 1]; ++q) {
+                    const int n2 = Sj[q];
+                    if (CF[n2] == UNDEC) {
+                        B.remove(measure[n2], n2);
+                        B.enter(++measure[n2], n2);
+                    }
+                }
+            }
+        }
+        for (int k = Si[index]; k < Si[index + 1]; ++k) {
+            const int nb = Sj[k];
+            if (CF[nb] == UNDEC) {
+                int mm = measure[nb];
+                B.remove(mm, nb);
+                measure[nb] = --mm;
+                if (mm > 0) {
+                    B.enter(mm, nb);
+                } else {
+                    CF[nb] = F_PT;
+                    --num_left;
+                    for (int q = Si[nb]; q < Si[nb + 1]; ++q) {
+                        const int n2 = Sj[q];
+                        if (CF[n2] == UNDEC) {
+                            B.remove(measure[n2], n2);
+                            B.enter(++measure[n2], n2);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+void build_schedule_host(int n, const int *ia, const int *ja, int order, bool forward, std::vector<int> &perm,
+                         std::vector<int> &group_ptr, std::vector<int> &rank) {
+    std::vector<int> grp(n, 0);
+    int ng = 0;
+    if (order == ORDER_EXACT) {
+        if (forward) {
+            for (int i = 0; i < n; ++i) {
+                int g = 0;
+                for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                    const int j = ja[k];
+                    if (j < i) g = std::max(g, grp[j] + 1);
+                }
+                grp[i] = g;
+                ng = std::max(ng, g + 1);
+            }
+        } else {
+            for (int i = n - 1; i >= 0; --i) {
+                int g = 0;
+                for (int k = ia[i]; k < ia[i + 1]; ++k) {
+                    const int j = ja[k];
+                    if (j > i) g = std::max(g, grp[j] + 1);
+                }
+                grp[i] = g;
+                ng = std::max(ng, g + 1);
+            }
+        }
+    } else {
+        // greedy colouring of the symmetrised pattern, natural order
+        std::vector<int> ti(n + 1, 0), tj(ia[n] > 0 ? ia[n] : 1);
+        for (int k = 0; k < ia[n]; ++k) ti[ja[k] + 1]++;
+        for (int i = 0; i < n; ++i) ti[i + 1] += ti[i];
+        {
+            std::vector<int> pos(ti.begin(), ti.end() - 1);
+            for (int i = 0; i < n; ++i)
+                for (int k = ia[i]; k < ia[i + 1]; ++k) tj[pos[ja[k]]++] = i;
+        }
+        std::vector<int> color(n, -1), mark(64, -1);
+        for (int i = 0; i < n; ++i) {
+            auto note = [&](int j) {
+                if (j != i && color[j] >= 0) {
+                    if (color[j] >= (int)mark.size()) mark.resize(2 * color[j] + 2, -1);
+                    mark[color[j]] = i;
+                }
+            };
+            for (int k = ia[i]; k < ia[i + 1]; ++k) note(ja[k]);
+            for (int k = ti[i]; k < ti[i + 1]; ++k) note(tj[k]);
+            int c = 0;
+            while (c < (int)mark.size() && mark[c] == i) ++c;
+            color[i] = c;
+            ng = std::max(ng, c + 1);
+        }
+        for (int i = 0; i < n; ++i) grp[i] = forward ? color[i] : (ng - 1 - color[i]);
+    }
+    if (n == 0) ng = 0;
+    group_ptr.assign(ng + 1, 0);
+    for (int i = 0; i < n; ++i) group_ptr[grp[i] + 1]++;
+    for (int g = 0; g < ng; ++g) group_ptr[g + 1] += group_ptr[g];
+    perm.assign(n > 0 ? n : 1, 0);
+    std::vector<int> pos(group_ptr.begin(), group_ptr.end());
+    for (int i = 0; i < n; ++i) perm[pos[grp[i]]++] = i;
+    // rank: the position of a row in the sequential order the sweep emulates
+    rank.assign(n > 0 ? n : 1, 0);
+    if (order == ORDER_EXACT) {
+        for (int i = 0; i < n; ++i) rank[i] = forward ? i : (n - 1 - i);
+    } else {
+        for (int i = 0; i < n; ++i) rank[i] = grp[i];
+    }
+}
+
+void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr, const std::vector<int> &rank,
+                     Schedule &S, cudaStream_t s) {
+    S.ngroups = (int)gptr.size() - 1;
+    S.h_group_ptr = gptr;
+    S.max_group = 0;
+    for (int g = 0; g < S.ngroups; ++g) S.max_group = std::max(S.max_group, gptr[g + 1] - gptr[g]);
+    S.perm.alloc(perm.size());
+    S.perm.upload(perm.data(), perm.size(), s);
+    S.group_ptr.alloc(gptr.size());
+    S.group_ptr.upload(gptr.data(), gptr.size(), s);
+    S.rank.alloc(rank.size());
+    S.rank.upload(rank.data(), rank.size(), s);
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace jxcpr

@@ -1,0 +1,363 @@
+// CPR preconditioner (jxfpamg-0220/csrc/cpr/jxf_cpr.c:268-610) and restarted
+// GMRES (jxfpamg-0220/csrc/krylov/pgmres.c:950-1713) driving the device kernels.
+//
+// GMRES runs its vector work on the device; the Hessenberg / Givens scalars
+// (k <= 30 of them) are updated on the host in the reference's exact scalar
+// order, so the only difference from the reference's iteration is the
+// summation order inside the device dot products.  Modified Gram-Schmidt is
+// fused: the update w -= h_{j-1} p_{j-1} and the next product <p_j, w> share
+// one pass over w.
+#include <math.h>
+
+#include <algorithm>
+#include <chrono>
+
+#include "solver.cuh"
+
+namespace jxcpr {
+
+// ---------------------------------------------------------------------------
+// CPR
+// ---------------------------------------------------------------------------
+void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
+    A = A_;
+    Timer t;
+    t.start(s);
+    amg.prm.order = prm.smoother_order;
+    amg.prm.coarse_exact = prm.coarse_exact;
+    amg.prm.max_colors = prm.max_colors;
+    DeviceCsr Ap;
+    bsr_pressure_csr(A, prm.pressure_index, Ap, s);
+    amg_setup(amg, std::move(Ap), s);
+    rp.alloc(A.nb > 0 ? A.nb : 1);
+    xp.alloc(A.nb > 0 ? A.nb : 1);
+    vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+    stats[0] = t.stop_ms(s) * 1e-3;
+    stats[2] = 0.0;  // stage 2 (HGS) needs no setup beyond the level-0 schedule
+    ready = true;
+}
+
+void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
+    const int nb = A.nb, bs = A.bs;
+    restrict_pressure(nb, bs, prm.pressure_index, r, rp.get(), s);
+    JX_CUDA(cudaMemsetAsync(xp.get(), 0, sizeof(double) * nb, s));
+    for (int it = 0; it < prm.stage1_maxit; ++it) amg_vcycle(amg, rp.get(), xp.get(), s);
+    prolong_pressure(nb, bs, prm.pressure_index, xp.get(), z, s);
+    const AmgLevel &L0 = *amg.levels[0];
+    if (prm.stage2_solver_type == 2) {
+        for (int it = 0; it < prm.stage2_maxit; ++it) {
+            if (prm.smoother_order == ORDER_EXACT)
+                hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
+                          amg.err.get(), s);
+            else
+                hgs_sweep_groups(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight,
+                                 prm.stage2_omega, s);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused MGS pass: w += (-h_prev) * p_prev (if p_prev), then partial <p_j, w>
+// ---------------------------------------------------------------------------
+static constexpr int kMgsThreads = 512;
+
+// pj == nullptr with self_dot: <w, w> after the update (the normalisation pass).
+__global__ void __launch_bounds__(kMgsThreads) mgs_pass_kernel(long long n, double *__restrict__ w,
+                                                               const double *__restrict__ p_prev,
+                                                               const double *__restrict__ h_prev,
+                                                               const double *__restrict__ pj, int self_dot,
+                                                               double *__restrict__ partials) {
+    __shared__ double ws[kMgsThreads / 32];
+    const double a = p_prev ? -(*h_prev) : 0.0;
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * kMgsThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kMgsThreads) {
+        double wv = w[i];
+        if (p_prev) {
+            wv = wv + a * p_prev[i];
+            w[i] = wv;
+        }
+        if (self_dot) acc += wv * wv;
+        else if (pj) acc += wv * pj[i];
+    }
+    if (!pj && !self_dot) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < kMgsThreads / 32 ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) partials[blockIdx.x] = r;
+    }
+}
+
+__global__ void sum_partials_kernel(int np, const double *__restrict__ partials, double *__restrict__ out) {
+    __shared__ double ws[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < (int)(blockDim.x / 32) ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) *out = r;
+    }
+}
+
+void Gmres::setup(int n_, cudaStream_t s) {
+    n = n_;
+    p.clear();
+    for (int i = 0; i <= prm.k_dim; ++i) p.emplace_back((size_t)(n > 0 ? n : 1));
+    r.alloc(n > 0 ? n : 1);
+    w.alloc(n > 0 ? n : 1);
+    partials.alloc(reduce_partials() + 8);
+    scal.alloc(prm.k_dim + 8);
+    (void)s;
+}
+
+namespace {
+struct DevOps {
+    cudaStream_t s;
+    long long n;
+    double *partials, *scal;
+    int np;
+    // <x, y> into scal[slot] (device) -- reference order y*x irrelevant (commutative products)
+    void dot_to(const double *x, const double *y, int slot) {
+        dot_dev(n, x, y, partials, scal + slot, s);
+    }
+    double fetch(int slot) {
+        double v = 0.0;
+        JX_CUDA(cudaMemcpyAsync(&v, scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+        return v;
+    }
+};
+}  // namespace
+
+GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s) {
+    GmresResult res;
+    const int k_dim = prm.k_dim;
+    const long long nl = n;
+    DevOps ops{s, nl, partials.get(), scal.get(), reduce_partials()};
+    std::vector<double> rs(k_dim + 1, 0.0), c(k_dim, 0.0), sn(k_dim, 0.0);
+    std::vector<std::vector<double>> hh(k_dim + 1, std::vector<double>(k_dim, 0.0));
+    const double epsmac = 1.e-16;
+    auto spmv = [&](double alpha, const double *xx, double beta, double *yy) {
+        bsr_spmv<double, double>(A, alpha, xx, beta, yy, kerr, s, prm.use_tma_spmv != 0 && kerr != nullptr);
+    };
+    auto precond = [&](const double *in, double *out) {
+        if (M) M->apply(in, out, s);
+        else copy_dev(nl, in, out, s);
+    };
+    const int np = ops.np;
+
+    copy_dev(nl, b, p[0].get(), s);
+    spmv(-1.0, x, 1.0, p[0].get());
+    ops.dot_to(b, b, 0);
+    const double b_norm = sqrt(ops.fetch(0));
+    if (b_norm != 0.0 && !(b_norm / b_norm == b_norm / b_norm)) {
+        set_error("gmres: NaN/Inf in b");
+        res.status = JXCPR_ERROR_GENERIC;
+        return res;
+    }
+    ops.dot_to(p[0].get(), p[0].get(), 0);
+    double r_norm = sqrt(ops.fetch(0));
+    if (r_norm != 0.0 && !(r_norm / r_norm == r_norm / r_norm)) {
+        set_error("gmres: NaN/Inf in A or x0");
+        res.status = JXCPR_ERROR_GENERIC;
+        return res;
+    }
+    const double r_norm_0 = r_norm;
+    double normdown = r_norm, conv_factor = 0.0;
+    res.norms.assign(prm.max_iter + 1, 0.0);
+    res.norms[0] = r_norm;
+    const double den_norm = b_norm > 0.0 ? b_norm : r_norm;
+    const double epsilon = std::max(prm.a_tol, prm.tol * den_norm);
+    int iter = 0, i = 0;
+    int converged = 0;
+    while (iter < prm.max_iter) {
+        rs[0] = r_norm;
+        if (r_norm == 0.0) {
+            res.iterations = iter;
+            res.converged = 1;
+            res.rel_residual = 0.0;
+            res.norms.resize(iter + 1);
+            return res;
+        }
+        if (r_norm <= epsilon && iter >= prm.min_iter) {
+            copy_dev(nl, b, r.get(), s);
+            spmv(-1.0, x, 1.0, r.get());
+            ops.dot_to(r.get(), r.get(), 0);
+            r_norm = sqrt(ops.fetch(0));
+            if (r_norm <= epsilon) {
+                converged = 1;
+                break;
+            }
+            if (prm.is_check_restarted == 0) break;
+        }
+        scale_dev(nl, 1.0 / r_norm, p[0].get(), s);
+        i = 0;
+        while (i < k_dim && iter < prm.max_iter) {
+            ++i;
+            ++iter;
+            JX_CUDA(cudaMemsetAsync(r.get(), 0, sizeof(double) * nl, s));
+            precond(p[i - 1].get(), r.get());
+            spmv(1.0, r.get(), 0.0, p[i].get());
+            // modified Gram-Schmidt, fused passes
+            for (int j = 0; j <= i; ++j) {
+                const double *pprev = j > 0 ? p[j - 1].get() : nullptr;
+                const double *hprev = j > 0 ? ops.scal + (j - 1) : nullptr;
+                const double *pj = j < i ? p[j].get() : nullptr;  // j == i: norm pass
+                mgs_pass_kernel<<<np, kMgsThreads, 0, s>>>(nl, p[i].get(), pprev, hprev, pj, j == i ? 1 : 0,
+                                                           ops.partials);
+                JX_LAUNCH_CHECK();
+                sum_partials_kernel<<<1, 512, 0, s>>>(np, ops.partials, ops.scal + j);
+                JX_LAUNCH_CHECK();
+            }
+            std::vector<double> hv(i + 1);
+            JX_CUDA(cudaMemcpyAsync(hv.data(), ops.scal, sizeof(double) * (i + 1), cudaMemcpyDeviceToHost, s));
+            JX_CUDA(cudaStreamSynchronize(s));
+            for (int j = 0; j < i; ++j) hh[j][i - 1] = hv[j];
+            double t = sqrt(hv[i]);
+            hh[i][i - 1] = t;
+            if (t != 0.0) {
+                t = 1.0 / t;
+                scale_dev(nl, t, p[i].get(), s);
+            }
+            for (int j = 1; j < i; ++j) {
+                t = hh[j - 1][i - 1];
+                hh[j - 1][i - 1] = sn[j - 1] * hh[j][i - 1] + c[j - 1] * t;
+                hh[j][i - 1] = -sn[j - 1] * t + c[j - 1] * hh[j][i - 1];
+            }
+            t = hh[i][i - 1] * hh[i][i - 1];
+            t += hh[i - 1][i - 1] * hh[i - 1][i - 1];
+            double gamma = sqrt(t);
+            if (gamma == 0.0) gamma = epsmac;
+            c[i - 1] = hh[i - 1][i - 1] / gamma;
+            sn[i - 1] = hh[i][i - 1] / gamma;
+            rs[i] = -hh[i][i - 1] * rs[i - 1];
+            rs[i] /= gamma;
+            rs[i - 1] = c[i - 1] * rs[i - 1];
+            hh[i - 1][i - 1] = sn[i - 1] * hh[i][i - 1] + c[i - 1] * hh[i - 1][i - 1];
+            r_norm = fabs(rs[i]);
+            conv_factor = r_norm / normdown;
+            normdown = r_norm;
+            res.norms[iter] = r_norm;
+            if (iter > 1 && conv_factor > prm.convfac_threshold) break;
+            if (r_norm <= epsilon && iter >= prm.min_iter) break;
+        }
+        // solution update: back-solve H y = rs, w = sum y_j p_j, x += M^{-1} w
+        rs[i - 1] = rs[i - 1] / hh[i - 1][i - 1];
+        for (int k = i - 2; k >= 0; --k) {
+            double t = 0.0;
+            for (int j = k + 1; j < i; ++j) t -= hh[k][j] * rs[j];
+            t += rs[k];
+            rs[k] = t / hh[k][k];
+        }
+        copy_dev(nl, p[i - 1].get(), w.get(), s);
+        scale_dev(nl, rs[i - 1], w.get(), s);
+        for (int j = i - 2; j >= 0; --j) axpy_dev(nl, rs[j], p[j].get(), w.get(), s);
+        JX_CUDA(cudaMemsetAsync(r.get(), 0, sizeof(double) * nl, s));
+        precond(w.get(), r.get());
+        axpy_dev(nl, 1.0, r.get(), x, s);
+        if (r_norm <= epsilon && iter >= prm.min_iter) {
+            copy_dev(nl, b, r.get(), s);
+            spmv(-1.0, x, 1.0, r.get());
+            ops.dot_to(r.get(), r.get(), 0);
+            r_norm = sqrt(ops.fetch(0));
+            if (r_norm <= epsilon) {
+                converged = 1;
+                break;
+            }
+            if (prm.is_check_restarted == 1) {
+                copy_dev(nl, r.get(), p[0].get(), s);
+                i = 0;
+            } else {
+                break;
+            }
+        }
+        if (iter > 1 && conv_factor > prm.convfac_threshold) break;
+        for (int j = i; j > 0; --j) {
+            rs[j - 1] = -sn[j - 1] * rs[j];
+            rs[j] = c[j - 1] * rs[j];
+        }
+        if (i) axpy_dev(nl, rs[i] - 1.0, p[i].get(), p[i].get(), s);
+        for (int j = i - 1; j > 0; --j) axpy_dev(nl, rs[j], p[j].get(), p[i].get(), s);
+        if (i) {
+            axpy_dev(nl, rs[0] - 1.0, p[0].get(), p[0].get(), s);
+            axpy_dev(nl, 1.0, p[i].get(), p[0].get(), s);
+        }
+    }
+    res.iterations = iter;
+    res.converged = converged;
+    res.rel_residual = b_norm > 0.0 ? r_norm / b_norm : r_norm / r_norm_0;
+    res.norms.resize(iter + 1);
+    JX_CUDA(cudaStreamSynchronize(s));
+    return res;
+}
+
+// ---------------------------------------------------------------------------
+// Solver
+// ---------------------------------------------------------------------------
+void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device) {
+    if (!stream) {
+        JX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        owns_stream = true;
+    }
+    cudaStream_t s = stream;
+    auto t0 = std::chrono::steady_clock::now();
+    A.alloc(nb, bs, nnzb);
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    JX_CUDA(cudaMemcpyAsync(A.ia.get(), ia, sizeof(int) * (nb + 1), kind, s));
+    JX_CUDA(cudaMemcpyAsync(A.ja.get(), ja, sizeof(int) * nnzb, kind, s));
+    JX_CUDA(cudaMemcpyAsync(A.a.get(), a, sizeof(double) * nnzb * bs * bs, kind, s));
+    const int csz = decouple_coef_size(bs, prm.decouple);
+    dcoef.alloc((size_t)(nb > 0 ? nb : 1) * (csz > 0 ? csz : 1));
+    if (prm.decouple) bsr_decouple_matrix(A, prm.decouple, dcoef.get(), s);
+    kerr.alloc(1);
+    kerr.zero(s);
+    cpr.prm = prm;
+    cpr.setup(A.view(), s);
+    gmres.prm = prm;
+    gmres.kerr = kerr.get();
+    gmres.setup(nb * bs, s);
+    b.alloc((size_t)(nb > 0 ? nb : 1) * bs);
+    x.alloc((size_t)(nb > 0 ? nb : 1) * bs);
+    JX_CUDA(cudaStreamSynchronize(s));
+    setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
+    cudaStream_t s = stream;
+    const long long n = (long long)A.nb * A.bs;
+    auto t0 = std::chrono::steady_clock::now();
+    const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    JX_CUDA(cudaMemcpyAsync(b.get(), b_in, sizeof(double) * n, in, s));
+    JX_CUDA(cudaMemcpyAsync(x.get(), x_io, sizeof(double) * n, in, s));
+    if (prm.decouple) bsr_decouple_rhs(A.nb, A.bs, prm.decouple, dcoef.get(), b.get(), prm.consistent_rhs, s);
+    gmres.prm = prm;
+    cpr.prm.stage2_maxit = prm.stage2_maxit;
+    cpr.prm.stage1_maxit = prm.stage1_maxit;
+    last = gmres.solve(A.view(), prm.stage1_solver_type ? &cpr : nullptr, b.get(), x.get(), s);
+    const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    JX_CUDA(cudaMemcpyAsync(x_io, x.get(), sizeof(double) * n, out, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    int kflag = 0, aflag = 0;
+    JX_CUDA(cudaMemcpy(&kflag, kerr.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    JX_CUDA(cudaMemcpy(&aflag, cpr.amg.err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (kflag || aflag) {
+        set_error("device wait timed out (spmv flag %d, smoother flag %d)", kflag, aflag);
+        last.status = JXCPR_ERROR_DEVICE;
+        kerr.zero(s);
+        cpr.amg.err.zero(s);
+    }
+    solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return last;
+}
+
+}  // namespace jxcpr

@@ -1,0 +1,116 @@
+// CPR preconditioner and restarted GMRES on one GPU.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "amg.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace jxcpr {
+
+struct SolverParams {
+    // GMRES (jxfpamg-0220/csrc/krylov/pgmres.c:431-470 defaults; the CPR
+    // driver sets k_dim 30, is_check_restarted 1, src/test_bsr_cprgmres.c:351-367)
+    int k_dim = 30;
+    int max_iter = 100;
+    int min_iter = 0;
+    double tol = 1e-6;
+    double a_tol = 0.0;
+    int is_check_restarted = 1;
+    double convfac_threshold = 1e4;
+    int print_level = 0;
+    int logging = 1;
+    // CPR (jxfpamg-0220/csrc/cpr/jxf_cpr.c:151-182, 226-262)
+    int pressure_index = 0;
+    int stage1_maxit = 1;
+    int stage2_maxit = 3;
+    int stage1_solver_type = 1;  // 1: AMG
+    int stage2_solver_type = 2;  // 2: block hybrid Gauss-Seidel (HGS)
+    double threshold = 1e-15;    // accepted and ignored, as in the reference
+    double stage2_relax_weight = 0.7;
+    double stage2_omega = 0.9;
+    // decoupling applied by the solver object (0 none, 1 ABF, 5 True-IMPES)
+    int decouple = 0;
+    int consistent_rhs = 0;
+    // device execution choices
+    int smoother_order = ORDER_EXACT;
+    int coarse_exact = 1;
+    int max_colors = 8;
+    int use_tma_spmv = 0;
+};
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~Timer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    float stop_ms(cudaStream_t s) {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+};
+
+// CPR two-stage preconditioner: restrict -> AMG V-cycle -> prolong -> stage 2.
+struct CprPrecond {
+    SolverParams prm;
+    BsrView<double> A;  // decoupled system matrix (owned by the solver)
+    Amg amg;
+    DevBuf<double> rp, xp, vt;
+    double stats[4] = {0, 0, 0, 0};  // stage1 setup, stage1 solve, stage2 setup, stage2 solve (seconds)
+    bool ready = false;
+    void setup(const BsrView<double> &A_, cudaStream_t s);
+    void apply(const double *r, double *z, cudaStream_t s);
+    int *err() { return amg.err.get(); }
+};
+
+struct GmresResult {
+    int iterations = 0;
+    int converged = 0;
+    double rel_residual = 0.0;
+    std::vector<double> norms;
+    int status = 0;
+};
+
+// Restarted right-preconditioned GMRES(k) with modified Gram-Schmidt and
+// Givens rotations (jxfpamg-0220/csrc/krylov/pgmres.c:950-1713).
+struct Gmres {
+    SolverParams prm;
+    int n = 0;
+    std::vector<DevBuf<double>> p;
+    DevBuf<double> r, w, partials, scal;  // scal: device scalars (dots)
+    int *kerr = nullptr;
+    void setup(int n_, cudaStream_t s);
+    GmresResult solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s);
+};
+
+// Full solver object: owns the device matrix, decoupling coefficients, CPR, GMRES.
+struct Solver {
+    SolverParams prm;
+    DeviceBsr A;
+    DevBuf<double> dcoef;  // decoupling weights per block row
+    CprPrecond cpr;
+    Gmres gmres;
+    DevBuf<double> b, x;
+    DevBuf<int> kerr;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    double setup_ms = 0.0, solve_ms = 0.0;
+    GmresResult last;
+    // A on the host or the device (device = 1), copied into the solver.
+    void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);
+    // b, x host or device; x holds the initial guess on entry.
+    GmresResult solve(const double *b_in, double *x_io, int device);
+};
+
+}  // namespace jxcpr

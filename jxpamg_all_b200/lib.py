@@ -46,3 +46,30 @@ def load():
 def check(status: int) -> None:
     if status != 0:
         raise JxcprError(status, load().jxcpr_last_error().decode(errors="replace"))
+
+
+def _declare_solver(lib):
+    P = c_void_p
+    lib.jxcpr_solver_create.argtypes = [ctypes.POINTER(c_void_p)]
+    lib.jxcpr_solver_destroy.argtypes = [P]
+    lib.jxcpr_solver_set_int.argtypes = [P, c_char_p, c_int]
+    lib.jxcpr_solver_set_real.argtypes = [P, c_char_p, c_double]
+    lib.jxcpr_solver_setup.argtypes = [P, c_int, c_int, c_longlong, P, P, P, c_int]
+    lib.jxcpr_solver_solve.argtypes = [P, P, P, c_int, P, P]
+    lib.jxcpr_solver_get_norms.argtypes = [P, P, c_int]
+    lib.jxcpr_solver_stats.argtypes = [P, P]
+    lib.jxcpr_solver_num_levels.argtypes = [P]
+    lib.jxcpr_solver_level_sizes.argtypes = [P, c_int, c_int, P]
+    lib.jxcpr_solver_level_matrix.argtypes = [P, c_int, c_int, P, P, P]
+    lib.jxcpr_solver_level_cf.argtypes = [P, c_int, P]
+    lib.jxcpr_solver_decoupled_values.argtypes = [P, P]
+    lib.jxcpr_solver_cpr_apply.argtypes = [P, P, P, c_int]
+    lib.jxcpr_solver_vcycle.argtypes = [P, P, P, c_int]
+
+
+_orig_declare = _declare
+
+
+def _declare(lib):  # noqa: F811
+    _orig_declare(lib)
+    _declare_solver(lib)

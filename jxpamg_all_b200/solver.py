@@ -1,0 +1,135 @@
+"""Python front end of the device CPR-GMRES solver object (libjxcpr_b200.so).
+
+Mirrors the reference's setup/solve sequence (decouple -> CPR setup -> GMRES
+solve, src/test_bsr_cprgmres.c:123-429) with its option names; host numpy
+arrays or device pointers (ints) are accepted.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import lib as _lib
+
+STATUS_CONV = 256
+
+
+def _ptr(a):
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class CprGmres:
+    """CPR-GMRES solver on the GPU.
+
+    Integer options: k_dim, max_iter, min_iter, is_check_restarted,
+    pressure_index, stage1_maxit, stage2_maxit, stage1_solver_type,
+    stage2_solver_type, decouple, consistent_rhs, smoother_order, coarse_exact,
+    use_tma_spmv.  Real options: tol, a_tol, threshold, convfac_threshold,
+    stage2_relax_weight, stage2_omega.
+    """
+
+    def __init__(self, **options):
+        self._so = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self._so.jxcpr_solver_create(ctypes.byref(h)))
+        self.h = h
+        self.nb = self.bs = 0
+        self.set(**options)
+
+    def set(self, **options):
+        for k, v in options.items():
+            if isinstance(v, float):
+                st = self._so.jxcpr_solver_set_real(self.h, k.encode(), float(v))
+            else:
+                st = self._so.jxcpr_solver_set_int(self.h, k.encode(), int(v))
+            _lib.check(st)
+        return self
+
+    def setup(self, ia, ja, a, bs, nb=None, nnzb=None, device=False):
+        if device:
+            self.nb, self.bs = int(nb), int(bs)
+            _lib.check(self._so.jxcpr_solver_setup(self.h, self.nb, self.bs, int(nnzb), _ptr(ia), _ptr(ja),
+                                                   _ptr(a), 1))
+        else:
+            self._keep = (np.ascontiguousarray(ia, np.int32), np.ascontiguousarray(ja, np.int32),
+                          np.ascontiguousarray(a, np.float64))
+            self.nb, self.bs = len(ia) - 1, int(bs)
+            _lib.check(self._so.jxcpr_solver_setup(self.h, self.nb, self.bs, len(ja), *(_ptr(v) for v in self._keep),
+                                                   0))
+        return self
+
+    def solve(self, b, x0=None, device=False):
+        """Returns (x, iterations, relative residual, converged)."""
+        it = np.zeros(1, np.int32)
+        rel = np.zeros(1)
+        if device:
+            st = self._so.jxcpr_solver_solve(self.h, _ptr(b), _ptr(x0), 1, _ptr(it), _ptr(rel))
+            x = x0
+        else:
+            x = np.zeros(self.nb * self.bs) if x0 is None else np.array(x0, dtype=np.float64)
+            bb = np.ascontiguousarray(b, np.float64)
+            st = self._so.jxcpr_solver_solve(self.h, _ptr(bb), _ptr(x), 0, _ptr(it), _ptr(rel))
+        if st not in (0, STATUS_CONV):
+            _lib.check(st)
+        return x, int(it[0]), float(rel[0]), st == 0
+
+    def norms(self):
+        buf = np.zeros(100000)
+        n = self._so.jxcpr_solver_get_norms(self.h, _ptr(buf), len(buf))
+        return buf[:n].copy()
+
+    def stats(self):
+        s = np.zeros(4)
+        _lib.check(self._so.jxcpr_solver_stats(self.h, _ptr(s)))
+        return dict(setup_ms=s[0], solve_ms=s[1], cpr_stage1_setup_s=s[2], levels=int(s[3]))
+
+    # ---- inspection -----------------------------------------------------------
+    def num_levels(self):
+        return int(self._so.jxcpr_solver_num_levels(self.h))
+
+    def level_matrix(self, lev, what=0):
+        sz = np.zeros(3, np.int32)
+        if self._so.jxcpr_solver_level_sizes(self.h, lev, what, _ptr(sz)) < 0:
+            return None
+        n, m, nnz = (int(v) for v in sz)
+        ia = np.zeros(n + 1, np.int32)
+        ja = np.zeros(max(nnz, 1), np.int32)
+        a = np.zeros(max(nnz, 1))
+        if self._so.jxcpr_solver_level_matrix(self.h, lev, what, _ptr(ia), _ptr(ja), _ptr(a)) < 0:
+            raise RuntimeError("level_matrix failed")
+        return ia, ja[:nnz], a[:nnz], m
+
+    def level_cf(self, lev, n):
+        cf = np.zeros(n, np.int32)
+        if self._so.jxcpr_solver_level_cf(self.h, lev, _ptr(cf)) < 0:
+            return None
+        return cf
+
+    def decoupled_values(self, nnzb):
+        a = np.zeros(nnzb * self.bs * self.bs)
+        _lib.check(self._so.jxcpr_solver_decoupled_values(self.h, _ptr(a)))
+        return a
+
+    def cpr_apply(self, r):
+        z = np.zeros(self.nb * self.bs)
+        _lib.check(self._so.jxcpr_solver_cpr_apply(self.h, _ptr(np.ascontiguousarray(r, np.float64)), _ptr(z), 0))
+        return z
+
+    def vcycle(self, rp, xp=None):
+        xp = np.zeros(self.nb) if xp is None else np.array(xp, dtype=np.float64)
+        _lib.check(self._so.jxcpr_solver_vcycle(self.h, _ptr(np.ascontiguousarray(rp, np.float64)), _ptr(xp), 0))
+        return xp
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._so.jxcpr_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
