@@ -38,6 +38,8 @@ extern "C" {
 
 /* Library version (major*10000 + minor*100 + patch). */
 JXCPR_API int jxcpr_version(void);
+/* Number of kernels this library has launched in the process so far. */
+JXCPR_API unsigned long long jxcpr_launch_count(void);
 /* Message describing the calling thread's last failure ("" if none). */
 JXCPR_API const char *jxcpr_last_error(void);
 
@@ -96,6 +98,8 @@ typedef struct jxcpr_solver jxcpr_solver;
 
 JXCPR_API int jxcpr_solver_create(jxcpr_solver **solver);
 JXCPR_API int jxcpr_solver_destroy(jxcpr_solver *solver);
+/* Run on the caller's CUDA stream (as void*) instead of a private one; call before setup. */
+JXCPR_API int jxcpr_solver_set_stream(jxcpr_solver *solver, void *stream);
 JXCPR_API int jxcpr_solver_set_int(jxcpr_solver *solver, const char *key, int value);
 JXCPR_API int jxcpr_solver_set_real(jxcpr_solver *solver, const char *key, double value);
 /* device != 0: ia/ja/a are device pointers. */
@@ -118,6 +122,10 @@ JXCPR_API int jxcpr_solver_decoupled_values(jxcpr_solver *solver, double *a);
 /* One CPR application z = M^{-1} r / one AMG V-cycle on the pressure system (xp in/out). */
 JXCPR_API int jxcpr_solver_cpr_apply(jxcpr_solver *solver, const double *r, double *z, int device);
 JXCPR_API int jxcpr_solver_vcycle(jxcpr_solver *solver, const double *rp, double *xp, int device);
+/* One CPR stage-2 sweep on the decoupled system A x = b, x in/out
+ * (jxf_ParBSRHGSRelax, jxfpamg-0220/csrc/amg/par_relax_bsr.c:193-573,
+ * relax_weight / omega from the stage2_* options). */
+JXCPR_API int jxcpr_solver_stage2_sweep(jxcpr_solver *solver, const double *b, double *x, int device);
 
 #ifdef __cplusplus
 }

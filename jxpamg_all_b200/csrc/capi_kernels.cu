@@ -60,6 +60,8 @@ extern "C" {
 
 int jxcpr_version(void) { return 10000; }
 
+unsigned long long jxcpr_launch_count(void) { return launch_count(); }
+
 const char *jxcpr_last_error(void) { return last_error(); }
 
 int jxcpr_bsr_matvec_dev(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a,

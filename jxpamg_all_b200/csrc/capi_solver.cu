@@ -101,6 +101,15 @@ int jxcpr_solver_destroy(jxcpr_solver *h) {
     });
 }
 
+int jxcpr_solver_set_stream(jxcpr_solver *h, void *stream) {
+    if (!h) return JXCPR_ERROR_ARG;
+    if (h->s.owns_stream && h->s.stream) cudaStreamDestroy(h->s.stream);
+    h->s.stream = (cudaStream_t)stream;
+    h->s.owns_stream = false;
+    h->s.stream_set = true;
+    return JXCPR_SUCCESS;
+}
+
 int jxcpr_solver_set_int(jxcpr_solver *h, const char *key, int value) {
     if (!h) return JXCPR_ERROR_ARG;
     return set_int_param(h->s.prm, key, value);
@@ -214,6 +223,29 @@ int jxcpr_solver_cpr_apply(jxcpr_solver *h, const double *r, double *z, int devi
         if (f) {
             set_error("smoother wait timed out");
             return JXCPR_ERROR_DEVICE;
+        }
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_stage2_sweep(jxcpr_solver *h, const double *b, double *x, int device) {
+    if (!h || !b || !x || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        Solver &S = h->s;
+        const long long n = (long long)S.A.nb * S.A.bs;
+        cudaStream_t st = S.stream;
+        const double *bd = b;
+        double *xd = x;
+        if (!device) {
+            JX_CUDA(cudaMemcpyAsync(S.b.get(), b, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            JX_CUDA(cudaMemcpyAsync(S.x.get(), x, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+            bd = S.b.get();
+            xd = S.x.get();
+        }
+        S.cpr.stage2_sweep(bd, xd, st);
+        if (!device) {
+            JX_CUDA(cudaMemcpyAsync(x, S.x.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+            JX_CUDA(cudaStreamSynchronize(st));
         }
         return JXCPR_SUCCESS;
     });

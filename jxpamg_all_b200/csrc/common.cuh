@@ -27,6 +27,7 @@ namespace jxcpr {
 // Last error message (thread-local) for diagnostics through the C ABI.
 void set_error(const char *fmt, ...);
 const char *last_error();
+unsigned long long launch_count();
 
 // Number of SMs of the current device (cached per device).
 int sm_count();
@@ -46,7 +47,14 @@ struct CudaError {
         }                                                                              \
     } while (0)
 
-#define JX_LAUNCH_CHECK() JX_CUDA(cudaGetLastError())
+// Every kernel launch site is followed by JX_LAUNCH_CHECK(), which also counts
+// the launch (reported through jxcpr_launch_count()).
+void count_launch();
+#define JX_LAUNCH_CHECK()                     \
+    do {                                      \
+        ::jxcpr::count_launch();              \
+        JX_CUDA(cudaGetLastError());          \
+    } while (0)
 
 // Owning device buffer (cudaMalloc'd, 256-byte aligned, padded by 64 bytes so
 // that 16-byte-rounded bulk copies of the tail stay inside the allocation).

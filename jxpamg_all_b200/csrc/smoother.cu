@@ -378,6 +378,7 @@ void gs_sweep(const CsrView<double> &A, const Schedule &sch, const double *f, do
     const double *aa = A.a;
     void *args[] = {&ng, &gp, &pm, &aia, &aja, &aa, &rank, &f, &u, &vt, &bar, &err};
     JX_CUDA(cudaLaunchCooperativeKernel((void *)gs_sweep_grid_kernel, blocks, kSweepThreads, args, 0, s));
+    count_launch();
 }
 
 void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
@@ -413,6 +414,7 @@ void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, d
     void *args[] = {&ng, &gp, &pm, &aia, &aja, &aa, &rank, &b, &x, &vt, &w, &omega, &plain, &bar, &err};
     void *fn = A.bs == 2 ? (void *)hgs_sweep_grid_kernel<2> : (void *)hgs_sweep_grid_kernel<3>;
     JX_CUDA(cudaLaunchCooperativeKernel(fn, blocks, kSweepThreads, args, 0, s));
+    count_launch();
 }
 
 }  // namespace jxcpr

@@ -44,16 +44,19 @@ void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
     for (int it = 0; it < prm.stage1_maxit; ++it) amg_vcycle(amg, rp.get(), xp.get(), s);
     prolong_pressure(nb, bs, prm.pressure_index, xp.get(), z, s);
     const AmgLevel &L0 = *amg.levels[0];
-    if (prm.stage2_solver_type == 2) {
-        for (int it = 0; it < prm.stage2_maxit; ++it) {
-            if (prm.smoother_order == ORDER_EXACT)
-                hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
-                          amg.err.get(), s);
-            else
-                hgs_sweep_groups(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight,
-                                 prm.stage2_omega, s);
-        }
-    }
+    (void)L0;
+    if (prm.stage2_solver_type == 2)
+        for (int it = 0; it < prm.stage2_maxit; ++it) stage2_sweep(r, z, s);
+}
+
+void CprPrecond::stage2_sweep(const double *r, double *z, cudaStream_t s) {
+    const AmgLevel &L0 = *amg.levels[0];
+    if (prm.smoother_order == ORDER_EXACT)
+        hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
+                  amg.err.get(), s);
+    else
+        hgs_sweep_groups(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
+                         s);
 }
 
 // ---------------------------------------------------------------------------
@@ -305,7 +308,7 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
 // Solver
 // ---------------------------------------------------------------------------
 void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device) {
-    if (!stream) {
+    if (!stream && !stream_set) {
         JX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         owns_stream = true;
     }

@@ -71,6 +71,8 @@ struct CprPrecond {
     bool ready = false;
     void setup(const BsrView<double> &A_, cudaStream_t s);
     void apply(const double *r, double *z, cudaStream_t s);
+    // one stage-2 block hybrid Gauss-Seidel sweep on A z = r (z in/out)
+    void stage2_sweep(const double *r, double *z, cudaStream_t s);
     int *err() { return amg.err.get(); }
 };
 
@@ -105,6 +107,7 @@ struct Solver {
     DevBuf<int> kerr;
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
+    bool stream_set = false;  // the caller chose the stream (possibly the legacy default stream)
     double setup_ms = 0.0, solve_ms = 0.0;
     GmresResult last;
     // A on the host or the device (device = 1), copied into the solver.

@@ -1,6 +1,7 @@
 // Error-message storage and device queries shared by the library.
 #include <stdarg.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -17,6 +18,10 @@ void set_error(const char *fmt, ...) {
 }
 
 const char *last_error() { return g_err; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 int sm_count() {
     static int cached[64] = {0};

@@ -53,6 +53,8 @@ def _declare_solver(lib):
     lib.jxcpr_solver_create.argtypes = [ctypes.POINTER(c_void_p)]
     lib.jxcpr_solver_destroy.argtypes = [P]
     lib.jxcpr_solver_set_int.argtypes = [P, c_char_p, c_int]
+    lib.jxcpr_solver_set_stream.argtypes = [P, P]
+    lib.jxcpr_launch_count.restype = ctypes.c_ulonglong
     lib.jxcpr_solver_set_real.argtypes = [P, c_char_p, c_double]
     lib.jxcpr_solver_setup.argtypes = [P, c_int, c_int, c_longlong, P, P, P, c_int]
     lib.jxcpr_solver_solve.argtypes = [P, P, P, c_int, P, P]
@@ -65,6 +67,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_decoupled_values.argtypes = [P, P]
     lib.jxcpr_solver_cpr_apply.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_vcycle.argtypes = [P, P, P, c_int]
+    lib.jxcpr_solver_stage2_sweep.argtypes = [P, P, P, c_int]
 
 
 _orig_declare = _declare

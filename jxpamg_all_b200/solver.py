@@ -39,6 +39,11 @@ class CprGmres:
         self.nb = self.bs = 0
         self.set(**options)
 
+    def set_stream(self, stream_handle: int):
+        """Run on an existing CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        _lib.check(self._so.jxcpr_solver_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+        return self
+
     def set(self, **options):
         for k, v in options.items():
             if isinstance(v, float):
