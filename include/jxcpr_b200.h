@@ -71,6 +71,23 @@ JXCPR_API int jxcpr_kernel_error_flag(void);
  */
 JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, double *out_host, void *stream);
 
+/* <x, y> like jxcpr_dot_dev, but allocating nothing.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory when
+ * they need the product -- code running inside a CUDA-graph capture region,
+ * where cudaMalloc is not allowed, or an application whose memory pool owns
+ * the whole device.  The partial sums live in a static device array reserved
+ * when the library loads (JXCPR_NOALLOC_DOT_MAX_PARTIALS partials of
+ * JXCPR_NOALLOC_DOT_CHUNK elements each, 512 KB per GPU, kept until exit), so
+ * n is limited to JXCPR_NOALLOC_DOT_MAX_PARTIALS * JXCPR_NOALLOC_DOT_CHUNK
+ * (268,435,456) elements; larger n returns JXCPR_ERROR_ARG with a message.
+ * The first call on each device resolves the array's device address and
+ * should come before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (concurrent streams) race and must be serialised. */
+#define JXCPR_NOALLOC_DOT_CHUNK 4096
+#define JXCPR_NOALLOC_DOT_MAX_PARTIALS 65536
+JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *y, double *out_host,
+                                    void *stream);
+
 /* ---- solver object ---------------------------------------------------------
  * CPR-GMRES on one GPU: jxcpr_solver_setup copies a BSR matrix (host or
  * device arrays), applies the configured decoupling (jxf_BSRMatrixDecouple,

@@ -30,6 +30,7 @@ def _declare(lib):
                                          c_void_p, c_double, c_void_p, c_int, c_void_p]
     lib.jxcpr_bsr_matvec_dev_f32.argtypes = lib.jxcpr_bsr_matvec_dev.argtypes
     lib.jxcpr_dot_dev.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.jxcpr_dot_dev_noalloc.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
 
 
 def load():
