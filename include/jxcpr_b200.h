@@ -129,6 +129,8 @@ JXCPR_API int jxcpr_solver_solve(jxcpr_solver *solver, const double *b, double *
 JXCPR_API int jxcpr_solver_get_norms(jxcpr_solver *solver, double *norms, int capacity);
 /* stats[0..3]: setup ms, solve ms, CPR stage-1 setup s, number of AMG levels. */
 JXCPR_API int jxcpr_solver_stats(jxcpr_solver *solver, double *stats);
+/* Text report of the last setup's phases ("name ms" per line); returns its length. */
+JXCPR_API int jxcpr_solver_setup_report(jxcpr_solver *solver, char *buf, int capacity);
 /* AMG hierarchy inspection: what = 0 A_l, 1 P_l, 2 R_l = P_l^T; sizes = {rows, cols, nnz}. */
 JXCPR_API int jxcpr_solver_num_levels(jxcpr_solver *solver);
 JXCPR_API int jxcpr_solver_level_sizes(jxcpr_solver *solver, int level, int what, int *sizes);

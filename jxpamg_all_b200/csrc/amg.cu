@@ -13,6 +13,7 @@
 // coarsest level the dense Gaussian elimination of jxf_gselim
 // (operation/matops/par_gs.c:20-74), here factored once at setup.
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "amg.cuh"
@@ -195,11 +196,35 @@ static void level_schedules(AmgLevel &L, int order, cudaStream_t s) {
     std::vector<int> perm, gptr, rank;
     build_schedule_host(n, ia.data(), ja.data(), order, true, perm, gptr, rank);
     upload_schedule(perm, gptr, rank, L.fwd, s);
-    build_schedule_host(n, ia.data(), ja.data(), order, false, perm, gptr, rank);
-    upload_schedule(perm, gptr, rank, L.bwd, s);
+    if (order == ORDER_EXACT) {
+        build_schedule_host(n, ia.data(), ja.data(), order, false, perm, gptr, rank);
+        upload_schedule(perm, gptr, rank, L.bwd, s);
+    }
+    // multicolour: the backward sweep visits the same classes in reverse order (fwd schedule, reversed)
+}
+
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+void PhaseLog::start() {
+    items.clear();
+    t_last = now_ms();
+}
+void PhaseLog::mark(const char *name, cudaStream_t s) {
+    cudaStreamSynchronize(s);
+    const double t = now_ms();
+    for (auto &kv : items)
+        if (kv.first == name) {
+            kv.second += t - t_last;
+            t_last = t;
+            return;
+        }
+    items.emplace_back(name, t - t_last);
+    t_last = t;
 }
 
 void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
+    H.log.start();
     H.levels.clear();
     H.levels.emplace_back(new AmgLevel());
     H.levels[0]->A = std::move(A0);
@@ -209,20 +234,26 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         const int n = L.A.nrows;
         DevPattern S;
         amg_strength(L.A.view(), H.prm.strong_threshold, H.prm.max_row_sum, S, s);
+        H.log.mark("strength", s);
         std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);
         S.ia.download(sia.data(), n + 1, s);
         S.ja.download(sja.data(), S.nnz, s);
         JX_CUDA(cudaStreamSynchronize(s));
         L.cf.assign(n, 0);
         rs_first_pass_host(n, sia.data(), sja.data(), L.cf.data());
+        H.log.mark("rs_first_pass(host)", s);
         DevBuf<int> cf(n > 0 ? n : 1);
         cf.upload(L.cf.data(), n, s);
         amg_pmis(S, cf.get(), s);
         cf.download(L.cf.data(), n, s);
+        H.log.mark("pmis", s);
         const int nc = amg_extpi_interp(L.A.view(), S, cf.get(), L.P, s);
+        H.log.mark("interp_extpi", s);
         csr_transpose(L.P.view(), L.R, s);
+        H.log.mark("transpose_P", s);
         std::unique_ptr<AmgLevel> next(new AmgLevel());
         amg_rap(L.A.view(), L.P, L.R, next->A, s);
+        H.log.mark("rap", s);
         H.levels.push_back(std::move(next));
         ++level;
         if (level == H.prm.max_levels - 1 || nc <= H.prm.coarse_threshold) break;
@@ -234,11 +265,16 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         L.u.alloc(n > 0 ? n : 1);
         L.lanes = lanes_for(n > 0 ? (double)L.A.nnz / n : 1.0);
         if (&L == H.levels.back().get()) continue;
-        level_schedules(L, H.prm.order, s);
+        const double mean_row = n > 0 ? (double)L.A.nnz / n : 0.0;
+        const bool dense = H.prm.order != ORDER_EXACT && mean_row > H.prm.jacobi_mean_row;
+        // level 0 always gets a schedule: stage 2 sweeps the block matrix, which has its pattern
+        if (!dense || &L == H.levels.front().get()) level_schedules(L, H.prm.order, s);
+        H.log.mark("schedules(host)", s);
         if (H.prm.order == ORDER_EXACT) {
             L.smoother = SMOOTH_EXACT_GS;
-        } else if (L.fwd.ngroups <= H.prm.max_colors) {
+        } else if (!dense && L.fwd.ngroups <= H.prm.max_colors) {
             L.smoother = SMOOTH_COLOR_GS;
+            permute_rows_csr(L.A.view(), L.fwd.perm.get(), L.Aperm, s);
         } else {
             L.smoother = SMOOTH_L1_JACOBI;
             L.dinv.alloc(n > 0 ? n : 1);
@@ -249,7 +285,9 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
     H.work.alloc((size_t)(n0 > 0 ? n0 : 1) * 2);
     H.err.alloc(1);
     H.err.zero(s);
+    H.log.mark("vectors", s);
     coarse_setup(H, s);
+    H.log.mark("coarse_lu", s);
     JX_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -261,12 +299,11 @@ static void sgs(Amg &H, AmgLevel &L, const double *f, double *u, double *vt, cud
             gs_sweep(L.A.view(), L.bwd, f, u, L.bwd.rank.get(), vt, H.err.get(), s);
             break;
         case SMOOTH_COLOR_GS:
-            gs_sweep_colors(L.A.view(), L.fwd, L.lanes, f, u, s);
-            gs_sweep_colors(L.A.view(), L.bwd, L.lanes, f, u, s);
+            gs_sweep_colors_perm(L.Aperm.view(), L.fwd, false, L.lanes, f, u, L.last_color, s);
+            gs_sweep_colors_perm(L.Aperm.view(), L.fwd, true, L.lanes, f, u, L.last_color, s);
             break;
         default:
-            jacobi_l1_sweep(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
-            jacobi_l1_sweep(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
+            jacobi_l1_sweep2(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
             break;
     }
 }
@@ -284,6 +321,7 @@ void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s) {
     }
     for (int l = 0; l < L - 1; ++l) {
         AmgLevel &Lv = *H.levels[l];
+        Lv.last_color = -1;  // u(l) was set by the caller or zeroed: nothing can be skipped
         sgs(H, Lv, F(l), U(l), vt, s);
         sgs(H, Lv, F(l), U(l), vt, s);
         const int n = Lv.A.nrows;
@@ -307,6 +345,7 @@ void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s) {
         else
             spmv_vec(Lv.P.view(), lanes_for(Lv.P.nrows > 0 ? (double)Lv.P.nnz / Lv.P.nrows : 1.0), 1.0, U(l + 1), 1.0,
                      U(l), s);
+        Lv.last_color = -1;  // the coarse correction changed every entry
         sgs(H, Lv, F(l), U(l), vt, s);
         sgs(H, Lv, F(l), U(l), vt, s);
     }

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <memory>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -46,6 +48,8 @@ struct AmgLevel {
     int smoother = SMOOTH_EXACT_GS;
     int lanes = 1;           // lanes per row of the vectorised CSR kernels
     DevBuf<double> dinv;     // l1-Jacobi inverse weights
+    DeviceCsr Aperm;         // multicolour GS: rows of A in fwd-schedule (colour) order
+    int last_color = -1;     // multicolour GS: class computed last since u last changed otherwise
     DeviceCsr A;          // level operator (diagonal first in every row)
     DeviceCsr P;          // interpolation to this level from level+1 (n x nc)
     DeviceCsr R;          // P^T, rows listing fine points ascending
@@ -62,10 +66,20 @@ struct AmgParams {
     int order = ORDER_EXACT;
     int coarse_exact = 1;  // 1: substitution in the reference's order; 0: explicit inverse (GEMV)
     int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
+    double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows go straight to l1-Jacobi
+};
+
+// Wall-clock phase log of a setup (host time between marks, stream drained at each mark).
+struct PhaseLog {
+    std::vector<std::pair<std::string, double>> items;
+    double t_last = 0.0;
+    void start();
+    void mark(const char *name, cudaStream_t s);
 };
 
 struct Amg {
     AmgParams prm;
+    PhaseLog log;
     std::vector<std::unique_ptr<AmgLevel>> levels;
     // coarsest level dense factors (row-major n x n), L stored transposed
     int nc = 0;
@@ -103,6 +117,12 @@ void gs_sweep_colors(const CsrView<double> &A, const Schedule &sch, int V, const
                      cudaStream_t s);
 void jacobi_l1_sweep(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u,
                      double *tmp, cudaStream_t s);
+void jacobi_l1_sweep2(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u, double *tmp,
+                      cudaStream_t s);
+void gs_sweep_colors_perm(const CsrView<double> &Aperm, const Schedule &fwd, bool backward, int V, const double *f,
+                          double *u, int &last_color, cudaStream_t s);
+void permute_rows_csr(const CsrView<double> &A, const int *perm, DeviceCsr &P, cudaStream_t s);
+void permute_rows_bsr(const BsrView<double> &A, const int *perm, DeviceBsr &P, cudaStream_t s);
 void residual_vec(const CsrView<double> &A, int V, const double *f, const double *u, double *r, cudaStream_t s);
 void spmv_vec(const CsrView<double> &A, int V, double alpha, const double *x, double beta, double *y,
               cudaStream_t s);
@@ -110,6 +130,9 @@ void spmv_vec(const CsrView<double> &A, int V, double alpha, const double *x, do
 // smoother.cu
 void hgs_sweep_groups(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
                       double *vt, double w, double omega, cudaStream_t s);
+// Multicolour HGS on a copy of A whose rows are in `fwd` order (class c = rows [ptr[c], ptr[c+1])).
+void hgs_sweep_colors_perm(const BsrView<double> &Aperm, const Schedule &fwd, const double *b, double *x,
+                           double *vt, double w, double omega, cudaStream_t s);
 // One Gauss-Seidel sweep of A u = f along `sch` (relax_weight = omega = 1,
 // rows with a zero diagonal skipped): jxf_PAMGRelax6's forward or backward
 // pass.

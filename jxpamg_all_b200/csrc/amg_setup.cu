@@ -472,25 +472,6 @@ int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *c
 // ---------------------------------------------------------------------------
 // Galerkin coarse operator A_c = R A P (R = P^T, stable transpose)
 // ---------------------------------------------------------------------------
-__global__ void rap_bound_kernel(int nc, const int *__restrict__ ria, const int *__restrict__ rja,
-                                 const int *__restrict__ aia, const int *__restrict__ aja,
-                                 const int *__restrict__ pia, long long *__restrict__ tsize) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= nc) return;
-    long long b = 1;
-    for (int r = ria[I]; r < ria[I + 1]; ++r) {
-        const int i = rja[r];
-        for (int k = aia[i]; k < aia[i + 1]; ++k) {
-            const int j = aja[k];
-            b += pia[j + 1] - pia[j];
-        }
-    }
-    // open-addressing table of at least 2x the bound, power of two
-    long long t = 16;
-    while (t < 2 * b) t <<= 1;
-    tsize[I] = t;
-}
-
 __device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 2654435761u; }
 
 // Returns the slot of column J (inserting it with slot `next` if absent).
@@ -512,26 +493,186 @@ __device__ __forceinline__ int table_slot(int *keys, int *vals, long long tsz, i
     }
 }
 
+// Warp-cooperative Galerkin product with the same discovery and accumulation
+// order as the sequential traversal (R row I -> A row i -> P row j): the 32
+// lanes take 32 consecutive products of the traversal; lanes with the same
+// coarse column are grouped (__match_any_sync) and the group's lowest lane adds
+// the members' products to the column's sum one by one in lane order, so
+// every column's sum is formed in traversal order.  New columns get slots in
+// order of first occurrence.  The row's column table lives in shared memory;
+// a row with more than kRapWarpMaxCols columns sets its overflow flag and is
+// redone by rap_fallback_kernel (one thread, table in global memory).
+static constexpr int kRapTable = 2048;        // shared-memory table entries per warp
+static constexpr int kRapWarpMaxCols = 1024;  // columns a warp row may hold
+static constexpr int kRapWarps = 2;           // warps per block
+
+__device__ __forceinline__ int rap_find(const int *keys, int J) {
+    unsigned h = hash_col(J) & (kRapTable - 1);
+    while (true) {
+        const int k = keys[h];
+        if (k == J) return (int)h;
+        if (k < 0) return -1;
+        h = (h + 1) & (kRapTable - 1);
+    }
+}
+
+__device__ __forceinline__ int rap_insert(int *keys, int J) {
+    unsigned h = hash_col(J) & (kRapTable - 1);
+    while (true) {
+        const int prev = atomicCAS(keys + h, -1, J);
+        if (prev == -1 || prev == J) return (int)h;
+        h = (h + 1) & (kRapTable - 1);
+    }
+}
+
 template <bool FILL>
-__global__ void rap_row_kernel(int I0, int I1, const int *__restrict__ ria, const int *__restrict__ rja,
-                               const double *__restrict__ ra, const int *__restrict__ aia,
-                               const int *__restrict__ aja, const double *__restrict__ aa,
-                               const int *__restrict__ pia, const int *__restrict__ pja,
-                               const double *__restrict__ pa, const long long *__restrict__ toff,
-                               long long tbase, int *__restrict__ tkeys, int *__restrict__ tvals,
-                               int *__restrict__ cnt, const int *__restrict__ cia, int *__restrict__ cja,
-                               double *__restrict__ ca) {
-    const int I = I0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= I1) return;
-    const long long off = toff[I] - tbase;
-    const long long tsz = toff[I + 1] - toff[I];
-    int *keys = tkeys + off;
-    int *vals = tvals + off;
-    for (long long t = 0; t < tsz; ++t) keys[t] = -1;
+__global__ void __launch_bounds__(32 * kRapWarps)
+    rap_warp_kernel(int nrows, const int *__restrict__ ria, const int *__restrict__ rja,
+                    const double *__restrict__ ra, const int *__restrict__ aia, const int *__restrict__ aja,
+                    const double *__restrict__ aa, const int *__restrict__ pia, const int *__restrict__ pja,
+                    const double *__restrict__ pa, int *__restrict__ cnt, unsigned char *__restrict__ overflow,
+                    const int *__restrict__ cia, int *__restrict__ cja, double *__restrict__ ca) {
+    extern __shared__ __align__(16) unsigned char rap_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *keys = reinterpret_cast<int *>(rap_smem) + warp * kRapTable;
+    int *slots = reinterpret_cast<int *>(rap_smem) + kRapWarps * kRapTable + warp * kRapTable;
+    double *vals = reinterpret_cast<double *>(rap_smem + (size_t)2 * kRapWarps * kRapTable * sizeof(int)) +
+                   warp * kRapTable;
+    const unsigned FULL = 0xffffffffu;
+    for (int I = blockIdx.x * kRapWarps + warp; I < nrows; I += gridDim.x * kRapWarps) {
+        if (FILL && overflow[I]) continue;
+        for (int t = lane; t < kRapTable; t += 32) keys[t] = -1;
+        __syncwarp();
+        int next = 1;
+        if (lane == 0) {
+            const int h = rap_insert(keys, I);  // diagonal first, starting from zero
+            slots[h] = 0;
+            if (FILL) vals[h] = 0.0;
+        }
+        __syncwarp();
+        bool over = false;
+        for (int r = ria[I]; r < ria[I + 1] && !over; ++r) {
+            const int i = rja[r];
+            const double rv = FILL ? ra[r] : 0.0;
+            const int kb = aia[i], ke = aia[i + 1];
+            for (int kc = kb; kc < ke && !over; kc += 32) {
+                const int k = kc + lane;
+                int len = 0, j = 0;
+                double av = 0.0;
+                if (k < ke) {
+                    j = aja[k];
+                    av = FILL ? aa[k] : 0.0;
+                    len = pia[j + 1] - pia[j];
+                }
+                int incl = len;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int pre = incl - len;
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int pb = 0; pb < total; pb += 32) {
+                    const int p = pb + lane;
+                    const bool valid = p < total;
+                    // owner: the last lane whose prefix is <= p
+                    int lo = 0, hi = 31;
+#pragma unroll
+                    for (int it = 0; it < 5; ++it) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        const int pm = __shfl_sync(FULL, pre, mid);
+                        if (pm <= p) lo = mid; else hi = mid - 1;
+                    }
+                    const int o = lo;
+                    const int jo = __shfl_sync(FULL, j, o);
+                    const double ao = __shfl_sync(FULL, av, o);
+                    const int preo = __shfl_sync(FULL, pre, o);
+                    int J = -1 - lane;  // unique dummy key for idle lanes
+                    double prod = 0.0;
+                    if (valid) {
+                        const int q = pia[jo] + (p - preo);
+                        J = pja[q];
+                        if (FILL) prod = (rv * ao) * pa[q];
+                    }
+                    const unsigned grp = __match_any_sync(FULL, J);
+                    const int leader = __ffs(grp) - 1;
+                    const bool is_leader = valid && lane == leader;
+                    int h = -1;
+                    if (is_leader) h = rap_find(keys, J);
+                    const bool fresh = is_leader && h < 0;
+                    const unsigned fresh_mask = __ballot_sync(FULL, fresh);
+                    if (next + __popc(fresh_mask) > kRapWarpMaxCols) {
+                        over = true;  // warp-uniform
+                        break;
+                    }
+                    if (fresh) {
+                        h = rap_insert(keys, J);
+                        slots[h] = next + __popc(fresh_mask & ((1u << lane) - 1u));
+                    }
+                    next += __popc(fresh_mask);
+                    if (FILL) {
+                        double acc = 0.0;
+                        bool first = fresh;
+                        if (is_leader && !fresh) acc = vals[h];
+                        for (int src = 0; src < 32; ++src) {
+                            const double v = __shfl_sync(FULL, prod, src);
+                            if (is_leader && ((grp >> src) & 1u)) {
+                                if (first) {
+                                    acc = v;
+                                    first = false;
+                                } else {
+                                    acc += v;
+                                }
+                            }
+                        }
+                        if (is_leader) vals[h] = acc;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        if (over) {
+            if (!FILL && lane == 0) overflow[I] = 1;
+            __syncwarp();
+            continue;
+        }
+        if (!FILL) {
+            if (lane == 0) cnt[I] = next;
+        } else {
+            const int base = cia[I];
+            for (int t = lane; t < kRapTable; t += 32) {
+                const int key = keys[t];
+                if (key >= 0) {
+                    cja[base + slots[t]] = key;
+                    ca[base + slots[t]] = vals[t];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Thread-per-row fallback for the rows the warp kernel could not hold.
+template <bool FILL>
+__global__ void rap_fallback_kernel(int nlist, const int *__restrict__ list, const int *__restrict__ ria,
+                                    const int *__restrict__ rja, const double *__restrict__ ra,
+                                    const int *__restrict__ aia, const int *__restrict__ aja,
+                                    const double *__restrict__ aa, const int *__restrict__ pia,
+                                    const int *__restrict__ pja, const double *__restrict__ pa,
+                                    const long long *__restrict__ toff, int *__restrict__ tkeys,
+                                    int *__restrict__ tvals, int *__restrict__ cnt, const int *__restrict__ cia,
+                                    int *__restrict__ cja, double *__restrict__ ca) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nlist) return;
+    const int I = list[t];
+    const long long tsz = toff[t + 1] - toff[t];
+    int *keys = tkeys + toff[t];
+    int *vals = tvals + toff[t];
+    for (long long q = 0; q < tsz; ++q) keys[q] = -1;
     int next = 0;
     bool fresh;
     const int base = FILL ? cia[I] : 0;
-    table_slot(keys, vals, tsz, I, next, fresh);  // diagonal first
+    table_slot(keys, vals, tsz, I, next, fresh);
     if (FILL) {
         cja[base] = I;
         ca[base] = 0.0;
@@ -561,35 +702,52 @@ __global__ void rap_row_kernel(int I0, int I1, const int *__restrict__ ria, cons
 
 void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, DeviceCsr &Ac, cudaStream_t s,
              long long table_budget_entries) {
+    (void)table_budget_entries;
     const int nc = P.ncols;
-    DevBuf<long long> tsize(nc + 1), toff(nc + 1);
-    tsize.zero(s);
-    rap_bound_kernel<<<div_up(nc, 256), 256, 0, s>>>(nc, R.ia.get(), R.ja.get(), A.ia, A.ja, P.ia.get(),
-                                                     tsize.get());
-    JX_LAUNCH_CHECK();
-    exclusive_scan_ll(tsize.get(), toff.get(), nc + 1, s);
-    std::vector<long long> h_off(nc + 1);
-    JX_CUDA(cudaMemcpyAsync(h_off.data(), toff.get(), sizeof(long long) * (nc + 1), cudaMemcpyDeviceToHost, s));
-    JX_CUDA(cudaStreamSynchronize(s));
-    // chunks of coarse rows whose tables fit the budget
-    std::vector<int> cuts{0};
-    while (cuts.back() < nc) {
-        const int a0 = cuts.back();
-        int b = (int)(std::upper_bound(h_off.begin() + a0 + 1, h_off.end(), h_off[a0] + table_budget_entries) -
-                      h_off.begin()) - 1;
-        if (b <= a0) b = a0 + 1;
-        if (b > nc) b = nc;
-        cuts.push_back(b);
+    const size_t smem = (size_t)kRapWarps * kRapTable * (2 * sizeof(int) + sizeof(double));
+    static bool attr[64] = {};
+    int dev = 0;
+    JX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (dev >= 0 && dev < 64) attr[dev] = true;
     }
-    long long max_chunk = 1;
-    for (size_t c = 1; c < cuts.size(); ++c) max_chunk = std::max(max_chunk, h_off[cuts[c]] - h_off[cuts[c - 1]]);
-    DevBuf<int> tkeys(max_chunk), tvals(max_chunk), cnt(nc + 1);
+    DevBuf<int> cnt(nc + 1);
+    DevBuf<unsigned char> over(nc + 1);
     cnt.zero(s);
-    for (size_t c = 1; c < cuts.size(); ++c) {
-        const int I0 = cuts[c - 1], I1 = cuts[c];
-        rap_row_kernel<false><<<div_up(I1 - I0, 128), 128, 0, s>>>(
-            I0, I1, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
-            toff.get(), h_off[I0], tkeys.get(), tvals.get(), cnt.get(), nullptr, nullptr, nullptr);
+    over.zero(s);
+    const int grid = std::max(1, std::min(div_up(nc, kRapWarps), 64 * sm_count()));
+    if (nc > 0) {
+        rap_warp_kernel<false><<<grid, 32 * kRapWarps, smem, s>>>(nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja,
+                                                                 A.a, P.ia.get(), P.ja.get(), P.a.get(), cnt.get(),
+                                                                 over.get(), nullptr, nullptr, nullptr);
+        JX_LAUNCH_CHECK();
+    }
+    // rows that overflowed the shared table: thread-per-row with a global table
+    std::vector<unsigned char> h_over(nc > 0 ? nc : 1);
+    over.download(h_over.data(), nc, s);
+    JX_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> list;
+    for (int I = 0; I < nc; ++I)
+        if (h_over[I]) list.push_back(I);
+    const int nl = (int)list.size();
+    DevBuf<int> d_list(nl > 0 ? nl : 1);
+    DevBuf<long long> toff(nl + 1);
+    DevBuf<int> tkeys, tvals;
+    if (nl > 0) {
+        d_list.upload(list.data(), nl, s);
+        // table per listed row: 2 x (columns reachable) <= 2 x nc, power of two
+        long long t = 16;
+        while (t < 2LL * nc) t <<= 1;
+        std::vector<long long> h_off(nl + 1);
+        for (int q = 0; q <= nl; ++q) h_off[q] = (long long)q * t;
+        toff.upload(h_off.data(), nl + 1, s);
+        tkeys.alloc((size_t)nl * t);
+        tvals.alloc((size_t)nl * t);
+        rap_fallback_kernel<false><<<div_up(nl, 64), 64, 0, s>>>(
+            nl, d_list.get(), R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
+            toff.get(), tkeys.get(), tvals.get(), cnt.get(), nullptr, nullptr, nullptr);
         JX_LAUNCH_CHECK();
     }
     DevBuf<int> cia(nc + 1);
@@ -603,11 +761,16 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
     Ac.ia = std::move(cia);
     Ac.ja.alloc(nnz > 0 ? nnz : 1);
     Ac.a.alloc(nnz > 0 ? nnz : 1);
-    for (size_t c = 1; c < cuts.size(); ++c) {
-        const int I0 = cuts[c - 1], I1 = cuts[c];
-        rap_row_kernel<true><<<div_up(I1 - I0, 128), 128, 0, s>>>(
-            I0, I1, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
-            toff.get(), h_off[I0], tkeys.get(), tvals.get(), nullptr, Ac.ia.get(), Ac.ja.get(), Ac.a.get());
+    if (nc > 0) {
+        rap_warp_kernel<true><<<grid, 32 * kRapWarps, smem, s>>>(nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja,
+                                                                A.a, P.ia.get(), P.ja.get(), P.a.get(), nullptr,
+                                                                over.get(), Ac.ia.get(), Ac.ja.get(), Ac.a.get());
+        JX_LAUNCH_CHECK();
+    }
+    if (nl > 0) {
+        rap_fallback_kernel<true><<<div_up(nl, 64), 64, 0, s>>>(
+            nl, d_list.get(), R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(),
+            toff.get(), tkeys.get(), tvals.get(), nullptr, Ac.ia.get(), Ac.ja.get(), Ac.a.get());
         JX_LAUNCH_CHECK();
     }
     JX_CUDA(cudaStreamSynchronize(s));

@@ -3,7 +3,9 @@
 // inspection of the AMG hierarchy for parity tests.
 #include <string.h>
 
+#include <algorithm>
 #include <new>
+#include <string>
 
 #include "jxcpr_b200.h"
 #include "solver.cuh"
@@ -161,6 +163,24 @@ int jxcpr_solver_stats(jxcpr_solver *h, double *stats) {
     stats[2] = h->s.cpr.stats[0];
     stats[3] = (double)h->s.cpr.amg.num_levels();
     return JXCPR_SUCCESS;
+}
+
+int jxcpr_solver_setup_report(jxcpr_solver *h, char *buf, int capacity) {
+    if (!h || !buf || capacity <= 0) return -1;
+    std::string out;
+    char line[160];
+    snprintf(line, sizeof line, "upload %.2f ms\ndecouple %.2f ms\n", h->s.upload_ms, h->s.decouple_ms);
+    out += line;
+    for (auto &kv : h->s.cpr.amg.log.items) {
+        snprintf(line, sizeof line, "%s %.2f ms\n", kv.first.c_str(), kv.second);
+        out += line;
+    }
+    snprintf(line, sizeof line, "total %.2f ms\n", h->s.setup_ms);
+    out += line;
+    const int n = (int)std::min<size_t>(out.size(), (size_t)capacity - 1);
+    memcpy(buf, out.data(), n);
+    buf[n] = 0;
+    return n;
 }
 
 int jxcpr_solver_num_levels(jxcpr_solver *h) { return h ? h->s.cpr.amg.num_levels() : -1; }

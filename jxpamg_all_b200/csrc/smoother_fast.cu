@@ -48,6 +48,25 @@ __global__ void gs_color_kernel(int r0, int r1, const int *__restrict__ perm, co
     if (live && lane == 0 && diag != 0.0) u[i] = (f[i] - s) / diag;
 }
 
+// Rows stored in schedule order (row t of the copy is row perm[t] of A), so a
+// colour class is a contiguous slab of the copy.
+template <int V>
+__global__ void gs_color_perm_kernel(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
+                                     const int *__restrict__ ja, const double *__restrict__ a,
+                                     const double *__restrict__ f, double *u) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = r0 + (int)(gt / V);
+    const int lane = (int)(gt % V);
+    const bool live = t < r1;
+    const int d = live ? ia[t] : 0, e = live ? ia[t + 1] : 0;
+    const double diag = d < e ? __ldg(a + d) : 0.0;
+    const double s = row_dot<V>(ja, a, d + 1 < e ? d + 1 : e, e, u, lane);
+    if (live && lane == 0 && diag != 0.0) {
+        const int i = perm[t];
+        u[i] = (f[i] - s) / diag;
+    }
+}
+
 template <int V>
 __global__ void jacobi_l1_kernel(int n, const int *__restrict__ ia, const int *__restrict__ ja,
                                  const double *__restrict__ a, const double *__restrict__ dinv,
@@ -118,6 +137,27 @@ void l1_diag(const CsrView<double> &A, double *dinv, cudaStream_t s) {
     JX_LAUNCH_CHECK();
 }
 
+// Colour classes of `sch` in order; `last_color` carries the class computed
+// last (or -1 after u changed by other means): a class is skipped when it
+// equals that one, since its rows would be recomputed from unchanged inputs.
+// With `Aperm` (rows in fwd-schedule order) each class is a contiguous slab;
+// `color_of_group` maps this schedule's groups to fwd class ids.
+void gs_sweep_colors_perm(const CsrView<double> &Aperm, const Schedule &fwd, bool backward, int V, const double *f,
+                          double *u, int &last_color, cudaStream_t s) {
+    const int nc = fwd.ngroups;
+    for (int g = 0; g < nc; ++g) {
+        const int c = backward ? nc - 1 - g : g;
+        if (c == last_color) continue;
+        const int r0 = fwd.h_group_ptr[c], r1 = fwd.h_group_ptr[c + 1];
+        last_color = c;
+        if (r1 <= r0) continue;
+        const long long threads = (long long)(r1 - r0) * V;
+        JX_DISPATCH_V(V, (gs_color_perm_kernel<VV><<<div_up(threads, 256), 256, 0, s>>>(
+                             r0, r1, fwd.perm.get(), Aperm.ia, Aperm.ja, Aperm.a, f, u)));
+        JX_LAUNCH_CHECK();
+    }
+}
+
 void gs_sweep_colors(const CsrView<double> &A, const Schedule &sch, int V, const double *f, double *u,
                      cudaStream_t s) {
     for (int g = 0; g < sch.ngroups; ++g) {
@@ -130,6 +170,20 @@ void gs_sweep_colors(const CsrView<double> &A, const Schedule &sch, int V, const
     }
 }
 
+// Two l1-Jacobi sweeps, u -> tmp -> u (no copies).
+void jacobi_l1_sweep2(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u, double *tmp,
+                      cudaStream_t s) {
+    const int n = A.nrows;
+    if (n == 0) return;
+    const long long threads = (long long)n * V;
+    JX_DISPATCH_V(V, (jacobi_l1_kernel<VV><<<div_up(threads, 256), 256, 0, s>>>(n, A.ia, A.ja, A.a, dinv, f, u,
+                                                                             tmp)));
+    JX_LAUNCH_CHECK();
+    JX_DISPATCH_V(V, (jacobi_l1_kernel<VV><<<div_up(threads, 256), 256, 0, s>>>(n, A.ia, A.ja, A.a, dinv, f, tmp,
+                                                                             u)));
+    JX_LAUNCH_CHECK();
+}
+
 void jacobi_l1_sweep(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u,
                      double *tmp, cudaStream_t s) {
     const int n = A.nrows;
@@ -139,6 +193,59 @@ void jacobi_l1_sweep(const CsrView<double> &A, int V, const double *dinv, const 
                                                                              tmp)));
     JX_LAUNCH_CHECK();
     JX_CUDA(cudaMemcpyAsync(u, tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+}
+
+// ---- row permutation of CSR / BSR storage (rows in schedule order) ----------
+__global__ void perm_row_len_kernel(int n, const int *__restrict__ perm, const int *__restrict__ ia,
+                                    int *__restrict__ len) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) len[t] = ia[perm[t] + 1] - ia[perm[t]];
+}
+
+template <int W>
+__global__ void perm_row_copy_kernel(int n, const int *__restrict__ perm, const int *__restrict__ ia,
+                                     const int *__restrict__ ja, const double *__restrict__ a,
+                                     const int *__restrict__ pia, int *__restrict__ pja, double *__restrict__ pa) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = perm[t];
+    const int k0 = ia[i], k1 = ia[i + 1], q0 = pia[t];
+    for (int k = k0; k < k1; ++k) {
+        pja[q0 + k - k0] = ja[k];
+        for (int w = 0; w < W; ++w) pa[(long long)(q0 + k - k0) * W + w] = a[(long long)k * W + w];
+    }
+}
+
+void permute_rows_csr(const CsrView<double> &A, const int *perm, DeviceCsr &P, cudaStream_t s) {
+    const int n = A.nrows;
+    P.alloc(n, A.ncols, A.nnz);
+    DevBuf<int> len(n + 1);
+    len.zero(s);
+    perm_row_len_kernel<<<div_up(n, 256), 256, 0, s>>>(n, perm, A.ia, len.get());
+    JX_LAUNCH_CHECK();
+    exclusive_scan_int(len.get(), P.ia.get(), n + 1, s);
+    perm_row_copy_kernel<1><<<div_up(n, 256), 256, 0, s>>>(n, perm, A.ia, A.ja, A.a, P.ia.get(), P.ja.get(),
+                                                          P.a.get());
+    JX_LAUNCH_CHECK();
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+void permute_rows_bsr(const BsrView<double> &A, const int *perm, DeviceBsr &P, cudaStream_t s) {
+    const int n = A.nb;
+    P.alloc(n, A.bs, A.nnzb);
+    DevBuf<int> len(n + 1);
+    len.zero(s);
+    perm_row_len_kernel<<<div_up(n, 256), 256, 0, s>>>(n, perm, A.ia, len.get());
+    JX_LAUNCH_CHECK();
+    exclusive_scan_int(len.get(), P.ia.get(), n + 1, s);
+    if (A.bs == 2)
+        perm_row_copy_kernel<4><<<div_up(n, 256), 256, 0, s>>>(n, perm, A.ia, A.ja, A.a, P.ia.get(), P.ja.get(),
+                                                              P.a.get());
+    else
+        perm_row_copy_kernel<9><<<div_up(n, 256), 256, 0, s>>>(n, perm, A.ia, A.ja, A.a, P.ia.get(), P.ja.get(),
+                                                              P.a.get());
+    JX_LAUNCH_CHECK();
+    JX_CUDA(cudaStreamSynchronize(s));
 }
 
 void residual_vec(const CsrView<double> &A, int V, const double *f, const double *u, double *r, cudaStream_t s) {

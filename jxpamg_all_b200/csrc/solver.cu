@@ -29,6 +29,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     DeviceCsr Ap;
     bsr_pressure_csr(A, prm.pressure_index, Ap, s);
     amg_setup(amg, std::move(Ap), s);
+    if (prm.smoother_order != ORDER_EXACT) permute_rows_bsr(A, amg.levels[0]->fwd.perm.get(), Aperm, s);
     rp.alloc(A.nb > 0 ? A.nb : 1);
     xp.alloc(A.nb > 0 ? A.nb : 1);
     vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
@@ -55,8 +56,7 @@ void CprPrecond::stage2_sweep(const double *r, double *z, cudaStream_t s) {
         hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
                   amg.err.get(), s);
     else
-        hgs_sweep_groups(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
-                         s);
+        hgs_sweep_colors_perm(Aperm.view(), L0.fwd, r, z, vt.get(), prm.stage2_relax_weight, prm.stage2_omega, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -319,9 +319,13 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     JX_CUDA(cudaMemcpyAsync(A.ia.get(), ia, sizeof(int) * (nb + 1), kind, s));
     JX_CUDA(cudaMemcpyAsync(A.ja.get(), ja, sizeof(int) * nnzb, kind, s));
     JX_CUDA(cudaMemcpyAsync(A.a.get(), a, sizeof(double) * nnzb * bs * bs, kind, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const int csz = decouple_coef_size(bs, prm.decouple);
     dcoef.alloc((size_t)(nb > 0 ? nb : 1) * (csz > 0 ? csz : 1));
     if (prm.decouple) bsr_decouple_matrix(A, prm.decouple, dcoef.get(), s);
+    JX_CUDA(cudaStreamSynchronize(s));
+    decouple_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() - upload_ms;
     kerr.alloc(1);
     kerr.zero(s);
     cpr.prm = prm;

@@ -65,6 +65,7 @@ struct Timer {
 struct CprPrecond {
     SolverParams prm;
     BsrView<double> A;  // decoupled system matrix (owned by the solver)
+    DeviceBsr Aperm;    // throughput mode: rows of A in level-0 colour order (stage 2)
     Amg amg;
     DevBuf<double> rp, xp, vt;
     double stats[4] = {0, 0, 0, 0};  // stage1 setup, stage1 solve, stage2 setup, stage2 solve (seconds)
@@ -108,7 +109,7 @@ struct Solver {
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     bool stream_set = false;  // the caller chose the stream (possibly the legacy default stream)
-    double setup_ms = 0.0, solve_ms = 0.0;
+    double setup_ms = 0.0, solve_ms = 0.0, upload_ms = 0.0, decouple_ms = 0.0;
     GmresResult last;
     // A on the host or the device (device = 1), copied into the solver.
     void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);

@@ -61,6 +61,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_solve.argtypes = [P, P, P, c_int, P, P]
     lib.jxcpr_solver_get_norms.argtypes = [P, P, c_int]
     lib.jxcpr_solver_stats.argtypes = [P, P]
+    lib.jxcpr_solver_setup_report.argtypes = [P, ctypes.c_char_p, c_int]
     lib.jxcpr_solver_num_levels.argtypes = [P]
     lib.jxcpr_solver_level_sizes.argtypes = [P, c_int, c_int, P]
     lib.jxcpr_solver_level_matrix.argtypes = [P, c_int, c_int, P, P, P]

@@ -91,6 +91,11 @@ class CprGmres:
         _lib.check(self._so.jxcpr_solver_stats(self.h, _ptr(s)))
         return dict(setup_ms=s[0], solve_ms=s[1], cpr_stage1_setup_s=s[2], levels=int(s[3]))
 
+    def setup_report(self):
+        buf = ctypes.create_string_buffer(8192)
+        self._so.jxcpr_solver_setup_report(self.h, buf, len(buf))
+        return buf.value.decode()
+
     # ---- inspection -----------------------------------------------------------
     def num_levels(self):
         return int(self._so.jxcpr_solver_num_levels(self.h))
