@@ -51,6 +51,7 @@ REF_ITERS = {"c1": 51, "c0": 23}
 WORKLOADS = {
     "c1": "config-1 system: 60x220x85 channelised two-phase Jacobian, 1,122,000 cells, 2x2 BSR, 7,780,000 blocks, seed 1",
     "c0": "config-0 system: 20x40x10 two-phase Jacobian, 8,000 cells, 2x2 BSR, 53,200 blocks, seed 0",
+    "slab45": "60x220x45 slab of the channelised geometry, 594,000 cells, 2x2 BSR, seed 5 (profiling case)",
 }
 SOLVER_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0)
 
@@ -147,6 +148,7 @@ def reference_sample(s, threads, cfg):
                 f"is scaled to the {iters_full} iterations the reference needs on this system")
         return est, wall, desc, "reference"
     # fallback: the oracle restatement (single thread)
+    sample_iters = 4
     t0 = time.perf_counter()
     a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
     C = oracle.OracleCPR(s.ia, s.ja, a, s.block_size)
@@ -224,6 +226,15 @@ def run_ours(args):
     for _ in range(args.warmup):
         _, it, rel, conv = solve_device()
     torch.cuda.synchronize()
+    if args.profile_solve:
+        # one solve inside a profiler range (ncu --profile-from-start off), nothing else
+        torch.cuda.profiler.start()
+        _, it, rel, conv = solve_device()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_solve": args.config, "iterations": it, "rel": rel, "converged": conv}))
+        G.close()
+        return 0 if conv else 1
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -374,6 +385,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="set up, run --warmup solves, then one solve inside a profiler range, and exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -228,6 +228,7 @@ CONFIGS = {
     "tiny": (6, 5, 4, 2, 0, 7),  # 120 cells, unit tests
     "small": (12, 10, 6, 2, 2, 3),  # 720 cells, unit tests with facies
     "tiny3": (5, 4, 3, 3, 0, 11),  # 60 cells, 3x3 unit tests
+    "slab45": (60, 220, 45, 2, 15, 5),  # 594,000 cells: profiling case, level-0 sweep larger than L2
 }
 
 
