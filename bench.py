@@ -56,6 +56,14 @@ WORKLOADS = {
 SOLVER_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0)
 
 
+def solver_opts(args):
+    opts = dict(SOLVER_OPTS)
+    for kv in getattr(args, "opt", []) or []:
+        k, v = kv.split("=", 1)
+        opts[k] = float(v) if ("." in v or "e" in v.lower()) else int(v)
+    return opts
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -213,7 +221,7 @@ def run_ours(args):
     d_ia, d_ja, d_a, d_b = dev(s.ia), dev(s.ja), dev(s.a), dev(s.b)
     d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
 
-    G = CprGmres(**SOLVER_OPTS)
+    G = CprGmres(**solver_opts(args))
     G.set_stream(stream.cuda_stream)
     G.setup(d_ia.data_ptr(), d_ja.data_ptr(), d_a.data_ptr(), s.block_size, nb=s.num_block_rows, nnzb=s.nnzb,
             device=True)
@@ -272,7 +280,7 @@ def run_ours(args):
     d2h = h_x.numel() * 8
 
     def e2e_step():
-        E = CprGmres(**SOLVER_OPTS)
+        E = CprGmres(**solver_opts(args))
         E.set_stream(stream.cuda_stream)
         E.nb, E.bs = s.num_block_rows, s.block_size
         lib.check(E._so.jxcpr_solver_setup(E.h, s.num_block_rows, s.block_size, s.nnzb,
@@ -385,6 +393,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
+                    help="override a solver option of the measured path (repeatable)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="set up, run --warmup solves, then one solve inside a profiler range, and exit")
     args = ap.parse_args()

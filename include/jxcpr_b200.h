@@ -146,6 +146,36 @@ JXCPR_API int jxcpr_solver_vcycle(jxcpr_solver *solver, const double *rp, double
  * relax_weight / omega from the stage2_* options). */
 JXCPR_API int jxcpr_solver_stage2_sweep(jxcpr_solver *solver, const double *b, double *x, int device);
 
+/* ---- fast path (smoother_order 1) inspection: no reference counterpart ---------------------
+ * level_info: smoother (1 multicolour GS, 2 l1-Jacobi, 3 Chebyshev-3; 0 exact path), storage
+ * (0 FP64, 1 FP32, 2 BF16 + row scale), the strength threshold the level was coarsened with and
+ * cheb[6] = {c0, c1, c2, interval low, interval high, lambda_max(D^-1 A)}.  Returns 0 or -1. */
+JXCPR_API int jxcpr_solver_level_info(jxcpr_solver *solver, int level, int *smoother, int *storage, double *theta,
+                                      double *cheb);
+/* Features (16 floats) recorded for `level` by a setup with fast_smoother 2 or record_features 1;
+ * returns the count or -1. */
+JXCPR_API int jxcpr_solver_level_features(jxcpr_solver *solver, int level, float *features);
+/* out[3] = {learned settings in use (1/0), V-cycle factor with them, with the plain smoothers}. */
+JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
+
+/* ---- learned settings: 16 -> 64 (tanh) -> 3 MLP, FP32; no reference counterpart -----------------
+ * Weight blob (jxcpr_mlp_num_weights() floats): mu[16], sigma[16], W1[64][16], b1[64], W2[3][64], b2[3];
+ * outputs y -> strength threshold 0.1 + 0.8 sigmoid(y0), Chebyshev interval
+ * [0.02 + 0.68 sigmoid(y1), 0.8 + 0.7 sigmoid(y2)] x lambda_max(D^-1 A).
+ * set/get: the weights the solver's learned mode (fast_smoother 2) uses (host arrays).
+ * forward / loss_grad / adam: batch kernels on DEVICE arrays X[B][16], T[B][3], Y[B][3], H[B][64]
+ * (H may be NULL); loss_grad needs work[B * 134] floats and writes the mean squared error to *loss
+ * (device) and its gradient to grad[num_weights] (mu and sigma get zero gradient). */
+JXCPR_API int jxcpr_mlp_num_weights(void);
+JXCPR_API int jxcpr_mlp_set_weights(const float *w);
+JXCPR_API int jxcpr_mlp_get_weights(float *w);
+JXCPR_API int jxcpr_mlp_forward_host(const float *w, const float *x, float *y);
+JXCPR_API int jxcpr_mlp_forward(const float *w, const float *X, int B, float *H, float *Y, void *stream);
+JXCPR_API int jxcpr_mlp_loss_grad(const float *w, const float *X, const float *T, int B, float *grad, float *loss,
+                                  float *work, void *stream);
+JXCPR_API int jxcpr_mlp_adam(float *w, const float *grad, float *m, float *v, float lr, float beta1, float beta2,
+                             float eps, int step, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

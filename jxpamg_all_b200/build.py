@@ -33,7 +33,8 @@ def _sources():
 
 
 def _headers():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.inc"))
+                  + glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
 def _stale() -> bool:

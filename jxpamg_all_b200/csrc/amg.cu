@@ -233,7 +233,8 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         AmgLevel &L = *H.levels[level];
         const int n = L.A.nrows;
         DevPattern S;
-        amg_strength(L.A.view(), H.prm.strong_threshold, H.prm.max_row_sum, S, s);
+        L.theta = H.prm.theta_for_level ? H.prm.theta_for_level(level, L.A.view()) : H.prm.strong_threshold;
+        amg_strength(L.A.view(), L.theta, H.prm.max_row_sum, S, s);
         H.log.mark("strength", s);
         std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);
         S.ia.download(sia.data(), n + 1, s);
@@ -261,25 +262,22 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
     for (auto &Lp : H.levels) {
         AmgLevel &L = *Lp;
         const int n = L.A.nrows;
-        L.f.alloc(n > 0 ? n : 1);
-        L.u.alloc(n > 0 ? n : 1);
-        L.lanes = lanes_for(n > 0 ? (double)L.A.nnz / n : 1.0);
+        if (H.prm.order == ORDER_EXACT) {
+            L.f.alloc(n > 0 ? n : 1);
+            L.u.alloc(n > 0 ? n : 1);
+        }
         if (&L == H.levels.back().get()) continue;
         const double mean_row = n > 0 ? (double)L.A.nnz / n : 0.0;
         const bool dense = H.prm.order != ORDER_EXACT && mean_row > H.prm.jacobi_mean_row;
         // level 0 always gets a schedule: stage 2 sweeps the block matrix, which has its pattern
         if (!dense || &L == H.levels.front().get()) level_schedules(L, H.prm.order, s);
         H.log.mark("schedules(host)", s);
-        if (H.prm.order == ORDER_EXACT) {
+        if (H.prm.order == ORDER_EXACT)
             L.smoother = SMOOTH_EXACT_GS;
-        } else if (!dense && L.fwd.ngroups <= H.prm.max_colors) {
-            L.smoother = SMOOTH_COLOR_GS;
-            permute_rows_csr(L.A.view(), L.fwd.perm.get(), L.Aperm, s);
-        } else {
+        else if (!dense && L.fwd.ngroups <= H.prm.max_colors)
+            L.smoother = SMOOTH_COLOR_GS;  // storage built by the fast path
+        else
             L.smoother = SMOOTH_L1_JACOBI;
-            L.dinv.alloc(n > 0 ? n : 1);
-            l1_diag(L.A.view(), L.dinv.get(), s);
-        }
     }
     const int n0 = H.levels[0]->A.nrows;
     H.work.alloc((size_t)(n0 > 0 ? n0 : 1) * 2);
@@ -291,24 +289,14 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
     JX_CUDA(cudaStreamSynchronize(s));
 }
 
-// One "symmetric Gauss-Seidel application" of the level's smoother.
+// One symmetric Gauss-Seidel application (forward then backward sweep).
 static void sgs(Amg &H, AmgLevel &L, const double *f, double *u, double *vt, cudaStream_t s) {
-    switch (L.smoother) {
-        case SMOOTH_EXACT_GS:
-            gs_sweep(L.A.view(), L.fwd, f, u, L.fwd.rank.get(), vt, H.err.get(), s);
-            gs_sweep(L.A.view(), L.bwd, f, u, L.bwd.rank.get(), vt, H.err.get(), s);
-            break;
-        case SMOOTH_COLOR_GS:
-            gs_sweep_colors_perm(L.Aperm.view(), L.fwd, false, L.lanes, f, u, L.last_color, s);
-            gs_sweep_colors_perm(L.Aperm.view(), L.fwd, true, L.lanes, f, u, L.last_color, s);
-            break;
-        default:
-            jacobi_l1_sweep2(L.A.view(), L.lanes, L.dinv.get(), f, u, vt, s);
-            break;
-    }
+    gs_sweep(L.A.view(), L.fwd, f, u, L.fwd.rank.get(), vt, H.err.get(), s);
+    gs_sweep(L.A.view(), L.bwd, f, u, L.bwd.rank.get(), vt, H.err.get(), s);
 }
 
 void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s) {
+    // exact-order cycle; the throughput / mixed cycles are in fast_cpr.cu
     const int L = H.num_levels();
     double *vt = H.work.get();
     double *res = H.work.get() + H.levels[0]->A.nrows;
@@ -321,31 +309,18 @@ void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s) {
     }
     for (int l = 0; l < L - 1; ++l) {
         AmgLevel &Lv = *H.levels[l];
-        Lv.last_color = -1;  // u(l) was set by the caller or zeroed: nothing can be skipped
         sgs(H, Lv, F(l), U(l), vt, s);
         sgs(H, Lv, F(l), U(l), vt, s);
         const int n = Lv.A.nrows;
         JX_CUDA(cudaMemsetAsync(U(l + 1), 0, sizeof(double) * H.levels[l + 1]->A.nrows, s));
-        if (H.prm.order == ORDER_EXACT) {
-            JX_CUDA(cudaMemcpyAsync(res, F(l), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-            csr_spmv(Lv.A.view(), -1.0, U(l), 1.0, res, s);
-            csr_spmv(Lv.R.view(), 1.0, res, 0.0, H.levels[l + 1]->f.get(), s);
-        } else {
-            residual_vec(Lv.A.view(), Lv.lanes, F(l), U(l), res, s);
-            const int nr = Lv.R.nrows;
-            spmv_vec(Lv.R.view(), lanes_for(nr > 0 ? (double)Lv.R.nnz / nr : 1.0), 1.0, res, 0.0,
-                     H.levels[l + 1]->f.get(), s);
-        }
+        JX_CUDA(cudaMemcpyAsync(res, F(l), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        csr_spmv(Lv.A.view(), -1.0, U(l), 1.0, res, s);
+        csr_spmv(Lv.R.view(), 1.0, res, 0.0, H.levels[l + 1]->f.get(), s);
     }
     coarse_solve(H, F(L - 1), U(L - 1), s);
     for (int l = L - 2; l >= 0; --l) {
         AmgLevel &Lv = *H.levels[l];
-        if (H.prm.order == ORDER_EXACT)
-            csr_spmv(Lv.P.view(), 1.0, U(l + 1), 1.0, U(l), s);
-        else
-            spmv_vec(Lv.P.view(), lanes_for(Lv.P.nrows > 0 ? (double)Lv.P.nnz / Lv.P.nrows : 1.0), 1.0, U(l + 1), 1.0,
-                     U(l), s);
-        Lv.last_color = -1;  // the coarse correction changed every entry
+        csr_spmv(Lv.P.view(), 1.0, U(l + 1), 1.0, U(l), s);
         sgs(H, Lv, F(l), U(l), vt, s);
         sgs(H, Lv, F(l), U(l), vt, s);
     }

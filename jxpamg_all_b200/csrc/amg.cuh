@@ -1,6 +1,7 @@
 // AMG hierarchy, smoother schedules and the setup / cycle entry points.
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <utility>
@@ -46,10 +47,7 @@ enum LevelSmoother {
 
 struct AmgLevel {
     int smoother = SMOOTH_EXACT_GS;
-    int lanes = 1;           // lanes per row of the vectorised CSR kernels
-    DevBuf<double> dinv;     // l1-Jacobi inverse weights
-    DeviceCsr Aperm;         // multicolour GS: rows of A in fwd-schedule (colour) order
-    int last_color = -1;     // multicolour GS: class computed last since u last changed otherwise
+    double theta = 0.25;  // strength threshold this level was coarsened with
     DeviceCsr A;          // level operator (diagonal first in every row)
     DeviceCsr P;          // interpolation to this level from level+1 (n x nc)
     DeviceCsr R;          // P^T, rows listing fine points ascending
@@ -67,6 +65,9 @@ struct AmgParams {
     int coarse_exact = 1;  // 1: substitution in the reference's order; 0: explicit inverse (GEMV)
     int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
     double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows go straight to l1-Jacobi
+    // Optional per-level strength thresholds: called before level l is
+    // coarsened with its operator; returns the threshold to use (learned model).
+    std::function<double(int level, const CsrView<double> &A)> theta_for_level;
 };
 
 // Wall-clock phase log of a setup (host time between marks, stream drained at each mark).
@@ -112,27 +113,10 @@ void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s);
 
 // smoother_fast.cu
 int lanes_for(double mean_row);
-void l1_diag(const CsrView<double> &A, double *dinv, cudaStream_t s);
-void gs_sweep_colors(const CsrView<double> &A, const Schedule &sch, int V, const double *f, double *u,
-                     cudaStream_t s);
-void jacobi_l1_sweep(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u,
-                     double *tmp, cudaStream_t s);
-void jacobi_l1_sweep2(const CsrView<double> &A, int V, const double *dinv, const double *f, double *u, double *tmp,
-                      cudaStream_t s);
-void gs_sweep_colors_perm(const CsrView<double> &Aperm, const Schedule &fwd, bool backward, int V, const double *f,
-                          double *u, int &last_color, cudaStream_t s);
 void permute_rows_csr(const CsrView<double> &A, const int *perm, DeviceCsr &P, cudaStream_t s);
 void permute_rows_bsr(const BsrView<double> &A, const int *perm, DeviceBsr &P, cudaStream_t s);
-void residual_vec(const CsrView<double> &A, int V, const double *f, const double *u, double *r, cudaStream_t s);
-void spmv_vec(const CsrView<double> &A, int V, double alpha, const double *x, double beta, double *y,
-              cudaStream_t s);
 
 // smoother.cu
-void hgs_sweep_groups(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
-                      double *vt, double w, double omega, cudaStream_t s);
-// Multicolour HGS on a copy of A whose rows are in `fwd` order (class c = rows [ptr[c], ptr[c+1])).
-void hgs_sweep_colors_perm(const BsrView<double> &Aperm, const Schedule &fwd, const double *b, double *x,
-                           double *vt, double w, double omega, cudaStream_t s);
 // One Gauss-Seidel sweep of A u = f along `sch` (relax_weight = omega = 1,
 // rows with a zero diagonal skipped): jxf_PAMGRelax6's forward or backward
 // pass.

@@ -52,7 +52,16 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"smoother_order", &p.smoother_order},
                {"coarse_exact", &p.coarse_exact},
                {"max_colors", &p.max_colors},
-               {"use_tma_spmv", &p.use_tma_spmv}};
+               {"use_tma_spmv", &p.use_tma_spmv},
+               {"precision", &p.precision},
+               {"bf16_level", &p.bf16_level},
+               {"fast_smoother", &p.fast_smoother},
+               {"stage2_lanes", &p.stage2_lanes},
+               {"learned_fallback", &p.learned_fallback},
+               {"record_features", &p.record_features},
+               {"flexible", &p.flexible},
+               {"autotune", &p.autotune},
+               {"graphs", &p.graphs}};
     if (!key) return JXCPR_ERROR_ARG;
     if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
     for (auto &e : tab)
@@ -73,7 +82,10 @@ int set_real_param(SolverParams &p, const char *key, double v) {
                {"threshold", &p.threshold},
                {"convfac_threshold", &p.convfac_threshold},
                {"stage2_relax_weight", &p.stage2_relax_weight},
-               {"stage2_omega", &p.stage2_omega}};
+               {"stage2_omega", &p.stage2_omega},
+               {"strong_threshold", &p.strong_threshold},
+               {"cheb_lower", &p.cheb_lower},
+               {"cheb_upper", &p.cheb_upper}};
     if (!key) return JXCPR_ERROR_ARG;
     for (auto &e : tab)
         if (!strcmp(key, e.k)) {
@@ -177,6 +189,8 @@ int jxcpr_solver_setup_report(jxcpr_solver *h, char *buf, int capacity) {
     }
     snprintf(line, sizeof line, "total %.2f ms\n", h->s.setup_ms);
     out += line;
+    if (h->s.cpr.fast)
+        for (const std::string &t : h->s.cpr.fast->tune_log) out += "tuned " + t + "\n";
     const int n = (int)std::min<size_t>(out.size(), (size_t)capacity - 1);
     memcpy(buf, out.data(), n);
     buf[n] = 0;
@@ -207,6 +221,37 @@ int jxcpr_solver_level_matrix(jxcpr_solver *h, int lev, int what, int *ia, int *
         JX_CUDA(cudaMemcpy(a, M.a.get(), sizeof(double) * sz[2], cudaMemcpyDeviceToHost));
         return 0;
     });
+}
+
+int jxcpr_solver_level_info(jxcpr_solver *h, int lev, int *smoother, int *storage, double *theta,
+                            double *cheb) {
+    if (!h || lev < 0 || lev >= h->s.cpr.amg.num_levels()) return -1;
+    const CprPrecond &C = h->s.cpr;
+    if (theta) *theta = C.amg.levels[lev]->theta;
+    if (C.fast) {
+        C.fast->level_info(lev, smoother, storage, cheb);
+    } else {
+        if (smoother) *smoother = 0;
+        if (storage) *storage = 0;
+        if (cheb)
+            for (int k = 0; k < 6; ++k) cheb[k] = 0.0;
+    }
+    return 0;
+}
+
+int jxcpr_solver_level_features(jxcpr_solver *h, int lev, float *out) {
+    if (!h || !out || lev < 0 || lev >= (int)h->s.cpr.plan.features.size()) return -1;
+    const std::vector<float> &f = h->s.cpr.plan.features[lev];
+    memcpy(out, f.data(), sizeof(float) * f.size());
+    return (int)f.size();
+}
+
+int jxcpr_solver_learned_status(jxcpr_solver *h, double *out) {
+    if (!h || !out) return JXCPR_ERROR_ARG;
+    out[0] = h->s.cpr.learned_used;
+    out[1] = h->s.cpr.factor_fast;
+    out[2] = h->s.cpr.factor_plain;
+    return JXCPR_SUCCESS;
 }
 
 int jxcpr_solver_level_cf(jxcpr_solver *h, int lev, int *cf) {
@@ -280,7 +325,7 @@ int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int devic
         const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
         JX_CUDA(cudaMemcpyAsync(S.cpr.rp.get(), rp, sizeof(double) * nb, in, st));
         JX_CUDA(cudaMemcpyAsync(S.cpr.xp.get(), xp, sizeof(double) * nb, in, st));
-        amg_vcycle(S.cpr.amg, S.cpr.rp.get(), S.cpr.xp.get(), st);
+        S.cpr.vcycle(S.cpr.rp.get(), S.cpr.xp.get(), st);
         const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
         JX_CUDA(cudaMemcpyAsync(xp, S.cpr.xp.get(), sizeof(double) * nb, out, st));
         JX_CUDA(cudaStreamSynchronize(st));

@@ -50,6 +50,7 @@ struct CudaError {
 // Every kernel launch site is followed by JX_LAUNCH_CHECK(), which also counts
 // the launch (reported through jxcpr_launch_count()).
 void count_launch();
+void count_launches(unsigned long long n);  // kernels replayed by a CUDA graph launch
 #define JX_LAUNCH_CHECK()                     \
     do {                                      \
         ::jxcpr::count_launch();              \

@@ -1,0 +1,745 @@
+// Fast CPR preconditioner: storage conversion (CSR / sliced ELL, FP64 / FP32 /
+// BF16), V-cycle and stage 2 (see fast.cuh for the modes).
+#include <math.h>
+
+#include <algorithm>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <type_traits>
+
+#include "fast.cuh"
+#include "fast_kernels.cuh"
+
+namespace jxcpr {
+
+namespace {
+constexpr int kThreads = 256;
+constexpr int kSellWindow = 512;  // rows sorted by length inside windows of this many rows
+
+// Calls f(values pointer) with the storage type of M: FP64 for the FP64 path,
+// FP32 / BF16 for the mixed path.
+template <typename TX, typename F>
+void with_values(const LevelMat &M, F &&f) {
+    if constexpr (std::is_same<TX, double>::value) {
+        f(M.a64.get());
+    } else {
+        if (M.kind == VAL_BF16) f(M.a16.get());
+        else f(M.a32.get());
+    }
+}
+
+template <typename T>
+void alloc_vec(DevBuf<T> &b, long long n) {
+    b.alloc(n > 0 ? n : 1);
+}
+
+// ---- launch of a row operation over stored rows [r0, r1) -------------------------
+template <typename TX, int V, typename TV, class Op>
+void launch_csr(const LevelMat &M, const TV *a, const Op &op, int r0, int r1, cudaStream_t s) {
+    fk::CsrFmt<V, TV> f{M.ia.get(), M.ja.get(), a, M.rscale.get(), M.perm};
+    const long long threads = (long long)(r1 - r0) * V;
+    fk::row_kernel<fk::CsrFmt<V, TV>, Op, TX><<<div_up(threads, kThreads), kThreads, 0, s>>>(f, op, r0, r1);
+}
+
+template <typename TX, class Op>
+void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s) {
+    if (r1 <= r0) return;
+    with_values<TX>(M, [&](auto a) {
+        using TV = typename std::remove_cv<typename std::remove_pointer<decltype(a)>::type>::type;
+        if (M.sell) {
+            fk::SellFmt<TV> f{M.sp.get(), M.ja.get(), a, M.rscale.get(), M.rows.get()};
+            fk::row_kernel<fk::SellFmt<TV>, Op, TX><<<div_up(r1 - r0, kThreads), kThreads, 0, s>>>(f, op, r0, r1);
+            return;
+        }
+        switch (M.lanes) {
+            case 1: launch_csr<TX, 1>(M, a, op, r0, r1, s); break;
+            case 2: launch_csr<TX, 2>(M, a, op, r0, r1, s); break;
+            case 4: launch_csr<TX, 4>(M, a, op, r0, r1, s); break;
+            case 8: launch_csr<TX, 8>(M, a, op, r0, r1, s); break;
+            case 16: launch_csr<TX, 16>(M, a, op, r0, r1, s); break;
+            default: launch_csr<TX, 32>(M, a, op, r0, r1, s); break;
+        }
+    });
+    JX_LAUNCH_CHECK();
+}
+
+// ---- construction -----------------------------------------------------------------
+// Sliced-ELL layout on the host: segments of `order` (offsets seg_in), rows
+// sorted by decreasing length inside windows, each segment padded to whole slices.
+void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, const std::vector<int> &seg_in,
+                 std::vector<int> &rows, std::vector<long long> &sp, std::vector<int> &seg_out) {
+    rows.clear();
+    seg_out.assign(1, 0);
+    std::vector<int> win;
+    for (size_t c = 0; c + 1 < seg_in.size(); ++c) {
+        for (int w0 = seg_in[c]; w0 < seg_in[c + 1]; w0 += kSellWindow) {
+            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow);
+            win.assign(order.begin() + w0, order.begin() + w1);
+            std::stable_sort(win.begin(), win.end(),
+                             [&](int x, int y) { return ia[x + 1] - ia[x] > ia[y + 1] - ia[y]; });
+            rows.insert(rows.end(), win.begin(), win.end());
+        }
+        while (rows.size() % 32) rows.push_back(-1);
+        seg_out.push_back((int)rows.size());
+    }
+    const size_t ns = rows.size() / 32;
+    sp.assign(ns + 1, 0);
+    for (size_t sl = 0; sl < ns; ++sl) {
+        int w = 0;
+        for (int q = 0; q < 32; ++q) {
+            const int i = rows[sl * 32 + q];
+            if (i >= 0) w = std::max(w, ia[i + 1] - ia[i]);
+        }
+        sp[sl + 1] = sp[sl] + 32LL * w;
+    }
+}
+
+template <typename TV>
+void sell_fill_launch(LevelMat &M, const int *ia, const int *ja, const double *a, TV *val, float *rscale,
+                      cudaStream_t s) {
+    if (!M.nstored) return;
+    fk::sell_fill<TV><<<div_up(M.nstored, kThreads), kThreads, 0, s>>>(M.nstored, M.rows.get(), M.sp.get(), ia, ja,
+                                                                      a, M.E, M.ja.get(), val, rscale);
+    JX_LAUNCH_CHECK();
+}
+
+// Builds M from a CSR (E = 1) or BSR (E = bs*bs) operator on the device.
+//  order / seg: host storage order of the rows and its segments (empty order:
+//  natural order, one segment); order_dev: the same order on the device (CSR layout).
+void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const int *ja, const double *a, int kind,
+                     bool sell, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
+                     LevelMat &M, cudaStream_t s) {
+    M.n = n;
+    M.m = m;
+    M.nnz = nnz;
+    M.E = E;
+    M.kind = kind;
+    M.sell = sell ? 1 : 0;
+    const bool natural = order.empty();
+    if (sell) {
+        std::vector<int> ia_h(n + 1);
+        JX_CUDA(cudaMemcpyAsync(ia_h.data(), ia, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+        std::vector<int> ord, sg;
+        if (natural) {
+            ord.resize(n);
+            std::iota(ord.begin(), ord.end(), 0);
+            sg = {0, n};
+        }
+        std::vector<int> rows;
+        std::vector<long long> sp;
+        sell_layout(ia_h, natural ? ord : order, natural ? sg : seg, rows, sp, M.seg);
+        M.nstored = (int)rows.size();
+        const long long slots = sp.back();
+        M.rows.alloc(rows.size() + 1);
+        M.rows.upload(rows.data(), rows.size(), s);
+        M.sp.alloc(sp.size());
+        M.sp.upload(sp.data(), sp.size(), s);
+        M.ja.alloc(slots > 0 ? slots : 1);
+        const long long nv = (slots > 0 ? slots : 1) * E;
+        if (kind == VAL_F64) {
+            M.a64.alloc(nv);
+            sell_fill_launch<double>(M, ia, ja, a, M.a64.get(), nullptr, s);
+        } else if (kind == VAL_F32) {
+            M.a32.alloc(nv);
+            sell_fill_launch<float>(M, ia, ja, a, M.a32.get(), nullptr, s);
+        } else {
+            M.a16.alloc(nv);
+            M.rscale.alloc(M.nstored > 0 ? M.nstored : 1);
+            sell_fill_launch<__nv_bfloat16>(M, ia, ja, a, M.a16.get(), M.rscale.get(), s);
+        }
+        JX_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    // CSR layout (rows permuted into `order` when given)
+    M.nstored = n;
+    M.seg = natural ? std::vector<int>{0, n} : seg;
+    M.perm = natural ? nullptr : order_dev;
+    M.lanes = lanes_for(n > 0 ? (double)nnz / n : 1.0);
+    const int *src_ia = ia, *src_ja = ja;
+    const double *src_a = a;
+    DeviceCsr pc;
+    DeviceBsr pb;
+    if (!natural) {
+        if (E == 1) {
+            permute_rows_csr(CsrView<double>{n, m, nnz, ia, ja, a}, order_dev, pc, s);
+            src_ia = pc.ia.get();
+            src_ja = pc.ja.get();
+            src_a = pc.a.get();
+        } else {
+            const int bs = E == 4 ? 2 : 3;
+            permute_rows_bsr(BsrView<double>{n, bs, nnz, ia, ja, a}, order_dev, pb, s);
+            src_ia = pb.ia.get();
+            src_ja = pb.ja.get();
+            src_a = pb.a.get();
+        }
+    }
+    M.ia.alloc((size_t)n + 1);
+    JX_CUDA(cudaMemcpyAsync(M.ia.get(), src_ia, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+    M.ja.alloc(nnz > 0 ? nnz : 1);
+    if (nnz) JX_CUDA(cudaMemcpyAsync(M.ja.get(), src_ja, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+    const long long nv = (nnz > 0 ? nnz : 1) * E;
+    if (kind == VAL_F64) {
+        M.a64.alloc(nv);
+        if (nnz) JX_CUDA(cudaMemcpyAsync(M.a64.get(), src_a, sizeof(double) * nnz * E, cudaMemcpyDeviceToDevice, s));
+    } else if (kind == VAL_F32) {
+        M.a32.alloc(nv);
+        if (nnz) {
+            fk::to_f32<<<div_up(nnz * E, kThreads), kThreads, 0, s>>>(nnz * E, src_a, M.a32.get());
+            JX_LAUNCH_CHECK();
+        }
+    } else {
+        M.a16.alloc(nv);
+        M.rscale.alloc(n > 0 ? n : 1);
+        if (n) {
+            fk::to_bf16_rows<<<div_up(n, kThreads), kThreads, 0, s>>>(n, src_ia, src_a, M.rscale.get(), M.a16.get());
+            JX_LAUNCH_CHECK();
+        }
+    }
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
+bool use_sell(const FastOptions &o, int n, long long nnz) {
+    return n >= o.sell_min_rows && n > 0 && (double)nnz / n <= o.sell_max_mean;
+}
+
+// Device time (us) of one y = A x pass over M, averaged over `reps` after a warm-up.
+template <typename TX>
+double time_pass(const LevelMat &M, const TX *x, TX *y, cudaStream_t s, int reps = 3) {
+    fk::OpSpmv<TX> op{x, y, 0};
+    launch_rows<TX>(M, op, 0, M.nstored, s);
+    cudaEvent_t e0, e1;
+    JX_CUDA(cudaEventCreate(&e0));
+    JX_CUDA(cudaEventCreate(&e1));
+    JX_CUDA(cudaEventRecord(e0, s));
+    for (int k = 0; k < reps; ++k) launch_rows<TX>(M, op, 0, M.nstored, s);
+    JX_CUDA(cudaEventRecord(e1, s));
+    JX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    JX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 1e3 * ms / reps;
+}
+
+std::string layout_name(const LevelMat &M) {
+    return M.sell ? std::string("sell") : ("csr/" + std::to_string(M.lanes));
+}
+
+// Builds a scalar operator in the layout that runs fastest here: CSR with
+// 1..32 lanes per row, or sliced ELL (operators with >= 2048 rows).
+template <typename TX>
+void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, const int *ja, const double *a,
+                 int kind, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
+                 const FastOptions &opt, LevelMat &M, std::vector<std::string> &log, cudaStream_t s) {
+    if (!opt.autotune || n == 0) {
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, use_sell(opt, n, nnz), order, seg, order_dev, M, s);
+        return;
+    }
+    build_level_mat(n, m, nnz, 1, ia, ja, a, kind, false, order, seg, order_dev, M, s);
+    DevBuf<TX> x(m > 0 ? m : 1), y(n > 0 ? n : 1);
+    x.zero(s);
+    y.zero(s);
+    double best = 1e30;
+    int best_lanes = M.lanes;
+    for (int V = 1; V <= 32; V *= 2) {
+        M.lanes = V;
+        const double t = time_pass<TX>(M, x.get(), y.get(), s);
+        if (t < best) {
+            best = t;
+            best_lanes = V;
+        }
+    }
+    M.lanes = best_lanes;
+    if (n >= 2048) {
+        LevelMat S;
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, true, order, seg, order_dev, S, s);
+        const double t = time_pass<TX>(S, x.get(), y.get(), s);
+        if (t < best) {
+            best = t;
+            M = std::move(S);
+        }
+    }
+    char line[200];
+    snprintf(line, sizeof line, "%s rows %d mean %.1f layout %s %.2f us", name, n, n ? (double)nnz / n : 0.0,
+             layout_name(M).c_str(), best);
+    log.emplace_back(line);
+}
+
+std::vector<int> download_ints(const int *d, int n, cudaStream_t s) {
+    std::vector<int> h(n > 0 ? n : 0);
+    if (n) {
+        JX_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+    }
+    return h;
+}
+
+template <typename TX>
+__global__ void add_kernel(int n, TX *__restrict__ u, const TX *__restrict__ c) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) u[i] += c[i];
+}
+
+// deterministic pseudo-random probe in [-1, 1) (splitmix-style integer hash)
+__global__ void probe_kernel(int n, double *__restrict__ e) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    e[i] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+}  // namespace
+
+void chebyshev3_coefficients(double lo, double hi, double c[3]) {
+    // q(t) = T3(sigma - tau t) / T3(sigma), T3(s) = 4 s^3 - 3 s, sigma = (hi+lo)/(hi-lo), tau = 2/(hi-lo);
+    // p(t) = (1 - q(t)) / t = -(q1 + q2 t + q3 t^2).
+    if (!(hi > lo) || lo <= 0.0) {
+        c[0] = hi > 0.0 ? 1.0 / hi : 0.0;  // degenerate interval: damped Jacobi
+        c[1] = c[2] = 0.0;
+        return;
+    }
+    const double sg = (hi + lo) / (hi - lo), tau = 2.0 / (hi - lo);
+    const double n0 = 4.0 * sg * sg * sg - 3.0 * sg;
+    const double n1 = -12.0 * sg * sg * tau + 3.0 * tau;
+    const double n2 = 12.0 * sg * tau * tau;
+    const double n3 = -4.0 * tau * tau * tau;
+    c[0] = -n1 / n0;
+    c[1] = -n2 / n0;
+    c[2] = -n3 / n0;
+}
+
+double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s) {
+    const int n = A.nrows;
+    if (n == 0) return 1.0;
+    DevBuf<double> dinv(n), x(n), y(n), partials(reduce_partials() + 8), nrm(2);
+    fk::dinv_diag<double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get());
+    JX_LAUNCH_CHECK();
+    fill_dev(n, 1.0, x.get(), s);
+    double lam = 1.0;
+    for (int it = 0; it < iters; ++it) {
+        fk::dinv_a_x<<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get(), x.get(), y.get());
+        JX_LAUNCH_CHECK();
+        dot_dev(n, y.get(), y.get(), partials.get(), nrm.get(), s);
+        dot_dev(n, x.get(), x.get(), partials.get(), nrm.get() + 1, s);
+        double h[2];
+        JX_CUDA(cudaMemcpyAsync(h, nrm.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+        if (!(h[0] > 0.0) || !(h[1] > 0.0)) break;
+        lam = sqrt(h[0] / h[1]);
+        scale_dev(n, 1.0 / sqrt(h[0]), y.get(), s);
+        std::swap(x.p, y.p);
+    }
+    return lam;
+}
+
+template <typename TX>
+struct FastCpr final : FastCprBase {
+    using TA = TX;
+    CprConfig cfg;
+    FastOptions opt;
+    int nb = 0, bs = 0;
+    std::vector<std::unique_ptr<FastLevel<TX>>> lv;
+    const double *Ainv = nullptr;
+    int nc = 0;
+    LevelMat st2;  // decoupled block matrix, level-0 colour classes as segments
+    DevBuf<double> vt;
+    CsrView<double> A0;  // FP64 level-0 operator (convergence-factor probe)
+    DevBuf<double> pe, pr, pc, partials, nrm;
+
+    int num_levels() const override { return (int)lv.size(); }
+    void level_info(int l, int *smoother, int *kind, double *cheb) const override {
+        const FastLevel<TX> &L = *lv[l];
+        const bool coarsest = l + 1 == (int)lv.size();
+        if (smoother) *smoother = coarsest ? 0 : L.smoother;
+        if (kind) *kind = coarsest ? VAL_F64 : L.A.kind;
+        if (cheb) {
+            cheb[0] = L.cheb[0];
+            cheb[1] = L.cheb[1];
+            cheb[2] = L.cheb[2];
+            cheb[3] = L.cheb_lo;
+            cheb[4] = L.cheb_hi;
+            cheb[5] = L.lambda_max;
+        }
+    }
+
+    // ---- level operations ----------------------------------------------------
+    void smooth(FastLevel<TX> &L, const TX *f, TX *u, bool zero, cudaStream_t s) {
+        if (L.n == 0) return;
+        const LevelMat &M = L.A;
+        if (L.smoother == FS_COLOR_GS) {
+            const int ncol = (int)M.seg.size() - 1;
+            L.last_color = -1;
+            for (int rep = 0; rep < 4; ++rep) {  // two symmetric GS applications: fwd, bwd, fwd, bwd
+                const bool backward = rep & 1;
+                for (int g = 0; g < ncol; ++g) {
+                    const int c = backward ? ncol - 1 - g : g;
+                    if (c == L.last_color) continue;  // recomputing the last class changes nothing
+                    L.last_color = c;
+                    fk::OpGs<TX> op{f, L.dinv.get(), u, zero ? 1 : 0};
+                    launch_rows<TX>(M, op, M.seg[c], M.seg[c + 1], s);
+                    zero = false;
+                }
+            }
+        } else if (L.smoother == FS_L1_JACOBI) {
+            for (int rep = 0; rep < 2; ++rep) {  // 2 x (u -> tmp -> u)
+                fk::OpJacobi<TX> a{f, L.dinv.get(), u, L.z.get(), zero ? 1 : 0};
+                launch_rows<TX>(M, a, 0, M.nstored, s);
+                fk::OpJacobi<TX> b{f, L.dinv.get(), L.z.get(), u, 0};
+                launch_rows<TX>(M, b, 0, M.nstored, s);
+                zero = false;
+            }
+        } else {
+            fk::OpCheb<TX> c0{0, zero ? 1 : 0, (TX)L.cheb[2], f, L.dinv.get(), nullptr, u, L.z.get(), L.y1.get()};
+            launch_rows<TX>(M, c0, 0, M.nstored, s);
+            fk::OpCheb<TX> c1{1, 0, (TX)L.cheb[1], f, L.dinv.get(), L.y1.get(), u, L.z.get(), L.y2.get()};
+            launch_rows<TX>(M, c1, 0, M.nstored, s);
+            fk::OpCheb<TX> c2{2, zero ? 1 : 0, (TX)L.cheb[0], f, L.dinv.get(), L.y2.get(), u, L.z.get(), nullptr};
+            launch_rows<TX>(M, c2, 0, M.nstored, s);
+        }
+    }
+    void residual(FastLevel<TX> &L, const TX *f, const TX *u, TX *r, cudaStream_t s) {
+        fk::OpResid<TX> op{f, u, r};
+        launch_rows<TX>(L.A, op, 0, L.A.nstored, s);
+    }
+    void spmv(const LevelMat &M, const TX *x, bool beta_one, TX *y, cudaStream_t s) {
+        fk::OpSpmv<TX> op{x, y, beta_one ? 1 : 0};
+        launch_rows<TX>(M, op, 0, M.nstored, s);
+    }
+    void coarse(const TX *f, TX *u, cudaStream_t s) {
+        if (nc == 0) return;
+        fk::dense_gemv<TX><<<div_up((long long)nc * 32, kThreads), kThreads, 0, s>>>(nc, Ainv, f, u);
+        JX_LAUNCH_CHECK();
+    }
+
+    // u0 = V-cycle(f0) from a zero initial guess
+    void vcycle_tx(const TX *f0, TX *u0, cudaStream_t s) {
+        const int L = (int)lv.size();
+        auto F = [&](int l) -> const TX * { return l == 0 ? f0 : lv[l]->f.get(); };
+        auto U = [&](int l) -> TX * { return l == 0 ? u0 : lv[l]->u.get(); };
+        if (L == 1) {
+            coarse(f0, u0, s);
+            return;
+        }
+        for (int l = 0; l < L - 1; ++l) {
+            FastLevel<TX> &Lv = *lv[l];
+            if (Lv.smoother == FS_COLOR_GS && Lv.n) JX_CUDA(cudaMemsetAsync(U(l), 0, sizeof(TX) * Lv.n, s));
+            smooth(Lv, F(l), U(l), true, s);
+            residual(Lv, F(l), U(l), Lv.r.get(), s);
+            spmv(Lv.R, Lv.r.get(), false, lv[l + 1]->f.get(), s);
+        }
+        coarse(F(L - 1), U(L - 1), s);
+        for (int l = L - 2; l >= 0; --l) {
+            FastLevel<TX> &Lv = *lv[l];
+            spmv(Lv.P, U(l + 1), true, U(l), s);
+            smooth(Lv, F(l), U(l), false, s);
+        }
+    }
+
+    template <typename TV>
+    void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const double *r, double *z, TA w,
+                        TA om, int plain, cudaStream_t s) {
+        const int grid = div_up((long long)(r1 - r0) * V, 128);
+#define JX_HGS_CSR(VV)                                                                                        \
+    do {                                                                                                      \
+        if (bs == 2)                                                                                          \
+            fk::hgs_color<2, VV, TV, TA><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, z, \
+                                                               vt.get(), w, om, plain);                       \
+        else                                                                                                  \
+            fk::hgs_color<3, VV, TV, TA><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, z, \
+                                                               vt.get(), w, om, plain);                       \
+    } while (0)
+        switch (V) {
+            case 1: JX_HGS_CSR(1); break;
+            case 2: JX_HGS_CSR(2); break;
+            case 4: JX_HGS_CSR(4); break;
+            case 8: JX_HGS_CSR(8); break;
+            case 16: JX_HGS_CSR(16); break;
+            default: JX_HGS_CSR(32); break;
+        }
+#undef JX_HGS_CSR
+    }
+
+    void stage2_sweep(const double *r, double *z, cudaStream_t s) override {
+        const LevelMat &M = st2;
+        if (M.n == 0) return;
+        JX_CUDA(cudaMemcpyAsync(vt.get(), z, sizeof(double) * M.n * bs, cudaMemcpyDeviceToDevice, s));
+        const double eps = 2.220446049250313e-16;
+        const int plain = (fabs(cfg.stage2_w - 1) < eps && fabs(cfg.stage2_omega - 1) < eps) ? 1 : 0;
+        const TA w = (TA)cfg.stage2_w, om = (TA)cfg.stage2_omega;
+        for (size_t c = 0; c + 1 < M.seg.size(); ++c) {
+            const int r0 = M.seg[c], r1 = M.seg[c + 1];
+            if (r1 <= r0) continue;
+            if constexpr (std::is_same<TX, double>::value) {
+                launch_stage2<double>(M, M.a64.get(), r0, r1, r, z, w, om, plain, s);
+            } else {
+                launch_stage2<float>(M, M.a32.get(), r0, r1, r, z, w, om, plain, s);
+            }
+            JX_LAUNCH_CHECK();
+        }
+    }
+    template <typename TV>
+    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const double *r, double *z, TA w, TA om,
+                       int plain, cudaStream_t s) {
+        if (M.sell) {
+            const int grid = div_up(r1 - r0, kThreads);
+            if (bs == 2)
+                fk::hgs_sell<2, TV, TA><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a, M.rows.get(), r,
+                                                                  z, vt.get(), w, om, plain);
+            else
+                fk::hgs_sell<3, TV, TA><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a, M.rows.get(), r,
+                                                                  z, vt.get(), w, om, plain);
+        } else {
+            launch_hgs_csr<TV>(opt.stage2_lanes, M, a, r0, r1, r, z, w, om, plain, s);
+        }
+    }
+
+    // CUDA graph of apply_direct(in_buf -> out_buf), captured on a private
+    // stream at the first application and replayed on the caller's stream.
+    cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    unsigned long long graph_kernels = 0;
+    DevBuf<double> in_buf, out_buf;
+
+    ~FastCpr() override {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+    }
+
+    void capture() {
+        const size_t n = (size_t)nb * bs;
+        in_buf.alloc(n > 0 ? n : 1);
+        out_buf.alloc(n > 0 ? n : 1);
+        JX_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        const unsigned long long k0 = launch_count();
+        JX_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            apply_direct(in_buf.get(), out_buf.get(), cap_stream);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(cap_stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        JX_CUDA(cudaStreamEndCapture(cap_stream, &graph));
+        graph_kernels = launch_count() - k0;
+        JX_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+    }
+
+    void apply(const double *r, double *z, cudaStream_t s) override {
+        if (!opt.graphs) {
+            apply_direct(r, z, s);
+            return;
+        }
+        if (!graph_exec) capture();
+        const size_t bytes = sizeof(double) * (size_t)nb * bs;
+        JX_CUDA(cudaMemcpyAsync(in_buf.get(), r, bytes, cudaMemcpyDeviceToDevice, s));
+        JX_CUDA(cudaGraphLaunch(graph_exec, s));
+        count_launches(graph_kernels);
+        JX_CUDA(cudaMemcpyAsync(z, out_buf.get(), bytes, cudaMemcpyDeviceToDevice, s));
+    }
+
+    void apply_direct(const double *r, double *z, cudaStream_t s) {
+        FastLevel<TX> &L0 = *lv[0];
+        fk::restrict_p<TX><<<div_up(nb, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get());
+        JX_LAUNCH_CHECK();
+        vcycle_tx(L0.f.get(), L0.u.get(), s);
+        for (int it = 1; it < cfg.stage1_maxit; ++it) {
+            // further AMG iterations as residual corrections: u += V(f - A u)
+            residual(L0, L0.f.get(), L0.u.get(), L0.r.get(), s);
+            vcycle_tx(L0.r.get(), L0.c.get(), s);
+            add_kernel<TX><<<div_up(L0.n, kThreads), kThreads, 0, s>>>(L0.n, L0.u.get(), L0.c.get());
+            JX_LAUNCH_CHECK();
+        }
+        fk::prolong_p<TX><<<div_up((long long)nb * bs, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index,
+                                                                                   L0.u.get(), z);
+        JX_LAUNCH_CHECK();
+        if (cfg.stage2_solver_type == 2)
+            for (int it = 0; it < cfg.stage2_maxit; ++it) stage2_sweep(r, z, s);
+    }
+
+    void vcycle(const double *fp, double *up, cudaStream_t s) override {
+        FastLevel<TX> &L0 = *lv[0];
+        const int n = L0.n;
+        fk::convert<double, TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, fp, L0.f.get());
+        JX_LAUNCH_CHECK();
+        vcycle_tx(L0.f.get(), L0.u.get(), s);
+        fk::convert<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, L0.u.get(), up);
+        JX_LAUNCH_CHECK();
+    }
+
+    double vcycle_factor(int cycles, cudaStream_t s) override {
+        const int n = A0.nrows;
+        if (n == 0 || cycles <= 0) return 0.0;
+        pe.alloc(n);
+        pr.alloc(n);
+        pc.alloc(n);
+        partials.alloc(reduce_partials() + 8);
+        nrm.alloc(2);
+        probe_kernel<<<div_up(n, kThreads), kThreads, 0, s>>>(n, pe.get());
+        JX_LAUNCH_CHECK();
+        auto norm = [&](const double *v) {
+            double h = 0.0;
+            dot_dev(n, v, v, partials.get(), nrm.get(), s);
+            JX_CUDA(cudaMemcpyAsync(&h, nrm.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+            JX_CUDA(cudaStreamSynchronize(s));
+            return sqrt(h);
+        };
+        double prev = norm(pe.get()), rho = 0.0;
+        for (int k = 0; k < cycles; ++k) {
+            csr_spmv(A0, -1.0, pe.get(), 0.0, pr.get(), s);  // r = -A e (f = 0)
+            vcycle(pr.get(), pc.get(), s);
+            axpy_dev(n, 1.0, pc.get(), pe.get(), s);         // e <- e + B r
+            const double cur = norm(pe.get());
+            rho = prev > 0.0 ? cur / prev : 0.0;
+            if (!(cur > 0.0) || !(cur == cur)) break;
+            prev = cur;
+        }
+        return rho;
+    }
+};
+
+template <typename TX>
+static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig &cfg, const FastOptions &opt,
+                               cudaStream_t s) {
+    std::unique_ptr<FastCpr<TX>> F(new FastCpr<TX>());
+    F->cfg = cfg;
+    F->opt = opt;
+    F->nb = A.nb;
+    F->bs = A.bs;
+    F->A0 = H.levels[0]->A.view();
+    const int L = H.num_levels();
+    const bool fp64 = std::is_same<TX, double>::value;
+    for (int l = 0; l < L; ++l) {
+        AmgLevel &HL = *H.levels[l];
+        std::unique_ptr<FastLevel<TX>> lev(new FastLevel<TX>());
+        FastLevel<TX> &Lv = *lev;
+        const int n = HL.A.nrows;
+        Lv.n = n;
+        alloc_vec(Lv.f, n);
+        alloc_vec(Lv.u, n);
+        if (l < L - 1) {
+            const int kind = fp64 ? VAL_F64 : ((opt.precision == 2 && l >= opt.bf16_level) ? VAL_BF16 : VAL_F32);
+            int sm = HL.smoother == SMOOTH_COLOR_GS ? FS_COLOR_GS : FS_L1_JACOBI;
+            if (opt.smoother == 2 || (opt.smoother == 1 && sm == FS_L1_JACOBI)) sm = FS_CHEB;
+            Lv.smoother = sm;
+            const CsrView<double> Av = HL.A.view();
+            const std::string nm = "A" + std::to_string(l);
+            if (sm == FS_COLOR_GS) {
+                std::vector<int> order = download_ints(HL.fwd.perm.get(), n, s);
+                build_tuned<TX>(nm.c_str(), n, n, Av.nnz, Av.ia, Av.ja, Av.a, kind, order, HL.fwd.h_group_ptr,
+                                HL.fwd.perm.get(), opt, Lv.A, F->tune_log, s);
+            } else {
+                build_tuned<TX>(nm.c_str(), n, n, Av.nnz, Av.ia, Av.ja, Av.a, kind, {}, {}, nullptr, opt, Lv.A,
+                                F->tune_log, s);
+            }
+            alloc_vec(Lv.dinv, n);
+            if (n) {
+                if (sm == FS_L1_JACOBI)
+                    fk::dinv_l1<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.a, Lv.dinv.get());
+                else
+                    fk::dinv_diag<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.ja, Av.a, Lv.dinv.get());
+                JX_LAUNCH_CHECK();
+            }
+            if (sm == FS_CHEB) {
+                Lv.lambda_max = estimate_lambda_max(Av, 12, s);
+                const double lo = (size_t)l < opt.level_lower.size() ? opt.level_lower[l] : opt.cheb_lower;
+                const double hi = (size_t)l < opt.level_upper.size() ? opt.level_upper[l] : opt.cheb_upper;
+                Lv.cheb_lo = lo * Lv.lambda_max;
+                Lv.cheb_hi = hi * Lv.lambda_max;
+                chebyshev3_coefficients(Lv.cheb_lo, Lv.cheb_hi, Lv.cheb);
+                alloc_vec(Lv.y1, n);
+                alloc_vec(Lv.y2, n);
+            }
+            alloc_vec(Lv.r, n);
+            alloc_vec(Lv.z, n);
+            if (l == 0) alloc_vec(Lv.c, n);
+            const int pk = fp64 ? VAL_F64 : VAL_F32;  // transfer operators: FP32 in the mixed path
+            const CsrView<double> Pv = HL.P.view(), Rv = HL.R.view();
+            build_tuned<TX>(("P" + std::to_string(l)).c_str(), Pv.nrows, Pv.ncols, Pv.nnz, Pv.ia, Pv.ja, Pv.a, pk, {},
+                            {}, nullptr, opt, Lv.P, F->tune_log, s);
+            build_tuned<TX>(("R" + std::to_string(l)).c_str(), Rv.nrows, Rv.ncols, Rv.nnz, Rv.ia, Rv.ja, Rv.a, pk, {},
+                            {}, nullptr, opt, Lv.R, F->tune_log, s);
+        }
+        F->lv.push_back(std::move(lev));
+    }
+    F->nc = H.nc;
+    F->Ainv = H.Ainv.get();
+    if (F->nc > 0 && !F->Ainv) {
+        set_error("fast CPR path needs the explicit coarse inverse");
+        throw CudaError{cudaErrorInvalidValue, "coarse inverse"};
+    }
+    // stage 2: block rows in the level-0 colour order
+    AmgLevel &H0 = *H.levels[0];
+    F->vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+    if (H0.fwd.ngroups > 0 && A.nb > 0) {
+        std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
+        const int kind = fp64 ? VAL_F64 : VAL_F32;
+        if (!opt.autotune) {
+            build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, A.nb >= opt.sell_min_rows, order,
+                            H0.fwd.h_group_ptr, H0.fwd.perm.get(), F->st2, s);
+        } else {
+            // time one stage-2 sweep per layout (CSR with 1..8 lanes per block row, sliced ELL)
+            build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, false, order, H0.fwd.h_group_ptr,
+                            H0.fwd.perm.get(), F->st2, s);
+            DevBuf<double> rb((size_t)A.nb * A.bs), zb((size_t)A.nb * A.bs);
+            rb.zero(s);
+            zb.zero(s);
+            auto time_sweep = [&]() {
+                F->stage2_sweep(rb.get(), zb.get(), s);
+                cudaEvent_t e0, e1;
+                JX_CUDA(cudaEventCreate(&e0));
+                JX_CUDA(cudaEventCreate(&e1));
+                JX_CUDA(cudaEventRecord(e0, s));
+                for (int k = 0; k < 3; ++k) F->stage2_sweep(rb.get(), zb.get(), s);
+                JX_CUDA(cudaEventRecord(e1, s));
+                JX_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                JX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return 1e3 * ms / 3;
+            };
+            double best = 1e30;
+            int best_lanes = 4;
+            for (int V = 1; V <= 8; V *= 2) {
+                F->opt.stage2_lanes = V;
+                const double t = time_sweep();
+                if (t < best) {
+                    best = t;
+                    best_lanes = V;
+                }
+            }
+            F->opt.stage2_lanes = best_lanes;
+            if (A.nb >= 2048) {
+                LevelMat S;
+                build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, true, order,
+                                H0.fwd.h_group_ptr, H0.fwd.perm.get(), S, s);
+                std::swap(F->st2, S);
+                const double t = time_sweep();
+                if (t < best) best = t;
+                else std::swap(F->st2, S);
+            }
+            char line[200];
+            snprintf(line, sizeof line, "stage2 rows %d blocks/row %.1f layout %s %.2f us", A.nb,
+                     (double)A.nnzb / A.nb,
+                     F->st2.sell ? "sell" : ("csr/" + std::to_string(F->opt.stage2_lanes)).c_str(), best);
+            F->tune_log.emplace_back(line);
+        }
+    }
+    JX_CUDA(cudaStreamSynchronize(s));
+    return F.release();
+}
+
+FastCprBase *make_fast_cpr(Amg &H, const BsrView<double> &A, const CprConfig &cfg, const FastOptions &opt,
+                           cudaStream_t s) {
+    if (opt.precision == 0) return build_fast<double>(H, A, cfg, opt, s);
+    return build_fast<float>(H, A, cfg, opt, s);
+}
+
+}  // namespace jxcpr

@@ -1,0 +1,509 @@
+// Device kernels of the fast (throughput / mixed-precision) CPR path.
+//
+// Every kernel is templated on the value storage type TV (double, float or
+// __nv_bfloat16 with a per-row scale) and the vector type TX (double or float;
+// arithmetic is done in TX).  Rows are reduced by V lanes of a warp (V a power
+// of two <= 32): lane l takes entries kb+l, kb+l+V, ... and the V partial sums
+// are combined with xor-shuffles, so every lane of a group must reach the
+// shuffles (out-of-range groups reduce an empty row).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace jxcpr {
+namespace fk {
+
+__device__ __forceinline__ double ldv(const double *p, long long k) { return __ldg(p + k); }
+__device__ __forceinline__ float ldv(const float *p, long long k) { return __ldg(p + k); }
+__device__ __forceinline__ float ldv(const __nv_bfloat16 *p, long long k) { return __bfloat162float(__ldg(p + k)); }
+
+template <int V, typename TA>
+__device__ __forceinline__ TA group_sum(TA v) {
+#pragma unroll
+    for (int o = V / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, V);
+    return v;
+}
+
+// sum_{k in [kb, ke)} a_k x_{ja_k}, reduced over the V lanes of the group.
+// Two entries per lane per trip keep more loads in flight.
+template <int V, typename TA, typename TV, typename TX>
+__device__ __forceinline__ TA row_sum(const int *__restrict__ ja, const TV *__restrict__ a, int kb, int ke,
+                                      const TX *x, int lane) {
+    TA s0 = 0, s1 = 0;
+    int k = kb + lane;
+    for (; k + V < ke; k += 2 * V) {
+        const int j0 = __ldg(ja + k), j1 = __ldg(ja + k + V);
+        const TA a0 = (TA)ldv(a, k), a1 = (TA)ldv(a, k + V);
+        s0 += a0 * (TA)x[j0];
+        s1 += a1 * (TA)x[j1];
+    }
+    if (k < ke) s0 += (TA)ldv(a, k) * (TA)x[__ldg(ja + k)];
+    return group_sum<V, TA>(s0 + s1);
+}
+
+// ---- matrix formats -----------------------------------------------------------
+// CSR with V lanes per row.  Stored row t maps to vector row perm[t] (perm ==
+// nullptr: identity); rscale (BF16 storage) is per stored row.
+template <int V_, typename TV>
+struct CsrFmt {
+    static constexpr int V = V_;
+    const int *ia, *ja;
+    const TV *a;
+    const float *rscale;
+    const int *perm;
+    __device__ __forceinline__ int row(int t) const { return perm ? __ldg(perm + t) : t; }
+    template <typename TA, typename TX>
+    __device__ __forceinline__ TA sum(int t, bool live, int lane, const TX *x, int kstart) const {
+        const int e = live ? __ldg(ia + t + 1) : 0;
+        int d = live ? __ldg(ia + t) + kstart : 0;
+        if (d > e) d = e;
+        return row_sum<V, TA>(ja, a, d, e, x, lane);
+    }
+    __device__ __forceinline__ float scale(int t) const { return rscale ? __ldg(rscale + t) : 1.0f; }
+};
+
+// Sliced ELL: 32-row slices stored slot-major, entry k of stored row t at
+// sp[t/32] + 32 k + t%32 (padding: value 0, column 0).  rows[t] is the vector
+// row of stored row t (-1: padding row).  One thread per row: the 32 rows of a
+// warp read each slot with one coalesced access.
+template <typename TV>
+struct SellFmt {
+    static constexpr int V = 1;
+    const long long *sp;
+    const int *col;
+    const TV *a;
+    const float *rscale;
+    const int *rows;
+    __device__ __forceinline__ int row(int t) const { return __ldg(rows + t); }
+    template <typename TA, typename TX>
+    __device__ __forceinline__ TA sum(int t, bool live, int, const TX *x, int kstart) const {
+        if (!live) return 0;
+        const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
+        const int w = (int)((b1 - b0) >> 5);
+        const long long o = b0 + (t & 31);
+        TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int k = kstart;
+        for (; k + 3 < w; k += 4) {
+            const long long p = o + (long long)k * 32;
+            const int j0 = __ldg(col + p), j1 = __ldg(col + p + 32), j2 = __ldg(col + p + 64),
+                      j3 = __ldg(col + p + 96);
+            const TA a0 = (TA)ldv(a, p), a1 = (TA)ldv(a, p + 32), a2 = (TA)ldv(a, p + 64), a3 = (TA)ldv(a, p + 96);
+            s0 += a0 * (TA)x[j0];
+            s1 += a1 * (TA)x[j1];
+            s2 += a2 * (TA)x[j2];
+            s3 += a3 * (TA)x[j3];
+        }
+        for (; k < w; ++k) {
+            const long long p = o + (long long)k * 32;
+            s0 += (TA)ldv(a, p) * (TA)x[__ldg(col + p)];
+        }
+        return (s0 + s1) + (s2 + s3);
+    }
+    __device__ __forceinline__ float scale(int t) const { return rscale ? __ldg(rscale + t) : 1.0f; }
+};
+
+// ---- row operations (prologue loads issued before the row sum) -----------------
+// Gauss-Seidel on one colour class: u_i = (f_i - sum_{j != i} a_ij u_j) dinv_i
+// (the diagonal is the first stored entry; dinv_i == 0 leaves the row).
+template <typename TX>
+struct OpGs {
+    static constexpr int kstart = 1;
+    const TX *f, *dinv;
+    TX *u;
+    int zero;  // every neighbour is 0 (first class after u = 0)
+    struct Pre { TX f, d; };
+    __device__ __forceinline__ const TX *x() const { return u; }
+    __device__ __forceinline__ bool need_sum() const { return !zero; }
+    __device__ __forceinline__ void load(int i, Pre &p) const { p.f = f[i]; p.d = dinv[i]; }
+    __device__ __forceinline__ void store(int i, TX s, const Pre &p) const {
+        if (p.d != (TX)0) u[i] = (p.f - s) * p.d;
+    }
+};
+// unew_i = u_i + (f_i - (A u)_i) dinv_i
+template <typename TX>
+struct OpJacobi {
+    static constexpr int kstart = 0;
+    const TX *f, *dinv, *u;
+    TX *unew;
+    int zero;  // u == 0
+    struct Pre { TX f, d, u; };
+    __device__ __forceinline__ const TX *x() const { return u; }
+    __device__ __forceinline__ bool need_sum() const { return !zero; }
+    __device__ __forceinline__ void load(int i, Pre &p) const {
+        p.f = f[i];
+        p.d = dinv[i];
+        p.u = zero ? (TX)0 : u[i];
+    }
+    __device__ __forceinline__ void store(int i, TX s, const Pre &p) const { unew[i] = p.u + (p.f - s) * p.d; }
+};
+// r_i = f_i - (A u)_i
+template <typename TX>
+struct OpResid {
+    static constexpr int kstart = 0;
+    const TX *f, *u;
+    TX *r;
+    struct Pre { TX f; };
+    __device__ __forceinline__ const TX *x() const { return u; }
+    __device__ __forceinline__ bool need_sum() const { return true; }
+    __device__ __forceinline__ void load(int i, Pre &p) const { p.f = f[i]; }
+    __device__ __forceinline__ void store(int i, TX s, const Pre &p) const { r[i] = p.f - s; }
+};
+// y = A x (+ y)
+template <typename TX>
+struct OpSpmv {
+    static constexpr int kstart = 0;
+    const TX *xin;
+    TX *y;
+    int beta_one;
+    struct Pre { TX y; };
+    __device__ __forceinline__ const TX *x() const { return xin; }
+    __device__ __forceinline__ bool need_sum() const { return true; }
+    __device__ __forceinline__ void load(int i, Pre &p) const { p.y = beta_one ? y[i] : (TX)0; }
+    __device__ __forceinline__ void store(int i, TX s, const Pre &p) const { y[i] = beta_one ? p.y + s : s; }
+};
+// Degree-3 polynomial smoother, Horner form of u += p(M) z, M = D^-1 A,
+// z = D^-1 (f - A u), p(t) = c0 + c1 t + c2 t^2:
+//   mode 0: z = D^-1 (f - A u), yout = c z          (c = c2; zero: u == 0)
+//   mode 1: yout = c z + D^-1 A yin                  (c = c1)
+//   mode 2: u = (zero ? 0 : u) + c z + D^-1 A yin    (c = c0)
+template <typename TX>
+struct OpCheb {
+    static constexpr int kstart = 0;
+    int mode, zero;
+    TX c;
+    const TX *f, *dinv, *yin;
+    TX *u, *z, *yout;
+    struct Pre { TX d, a, b; };
+    __device__ __forceinline__ const TX *x() const { return mode == 0 ? u : yin; }
+    __device__ __forceinline__ bool need_sum() const { return !(mode == 0 && zero); }
+    __device__ __forceinline__ void load(int i, Pre &p) const {
+        p.d = dinv[i];
+        if (mode == 0) {
+            p.a = f[i];
+        } else {
+            p.a = z[i];
+            p.b = (mode == 2 && !zero) ? u[i] : (TX)0;
+        }
+    }
+    __device__ __forceinline__ void store(int i, TX s, const Pre &p) const {
+        if (mode == 0) {
+            const TX zi = (p.a - s) * p.d;
+            z[i] = zi;
+            yout[i] = c * zi;
+        } else if (mode == 1) {
+            yout[i] = c * p.a + p.d * s;
+        } else {
+            u[i] = p.b + c * p.a + p.d * s;
+        }
+    }
+};
+
+// One launch of `op` over stored rows [r0, r1) of a matrix in format Fmt.
+template <class Fmt, class Op, typename TX>
+__global__ void __launch_bounds__(256) row_kernel(Fmt fmt, Op op, int r0, int r1) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = r0 + (int)(gt / Fmt::V);
+    const int lane = (int)(gt % Fmt::V);
+    const bool live = t < r1;
+    const int i = live ? fmt.row(t) : -1;
+    const bool own = i >= 0 && lane == 0;
+    typename Op::Pre pre;
+    if (own) op.load(i, pre);
+    TX s = 0;
+    if (op.need_sum()) s = fmt.template sum<TX, TX>(t, i >= 0, lane, op.x(), Op::kstart);
+    if (own) {
+        if (fmt.rscale) s *= (TX)fmt.scale(t);
+        op.store(i, s, pre);
+    }
+}
+
+template <typename TX>
+__global__ void restrict_p(int nb, int bs, int p, const double *__restrict__ r, TX *__restrict__ rp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) rp[i] = (TX)r[(long long)i * bs + p];
+}
+
+template <typename TX>
+__global__ void prolong_p(int nb, int bs, int p, const TX *__restrict__ up, double *__restrict__ z) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * bs) return;
+    const int i = (int)(t / bs), k = (int)(t % bs);
+    z[t] = k == p ? (double)up[i] : 0.0;
+}
+
+// u = Ainv f (FP64 inverse of the coarsest operator), one warp per row.
+template <typename TX>
+__global__ void dense_gemv(int n, const double *__restrict__ Ainv, const TX *__restrict__ f, TX *__restrict__ u) {
+    const int row = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0.0;
+    for (int c = lane; c < n; c += 32) s += Ainv[(long long)row * n + c] * (double)f[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) u[row] = (TX)s;
+}
+
+// ---- stage 2: hybrid block Gauss-Seidel, one colour class -------------------
+template <int BS, typename TV, typename TA>
+__device__ __forceinline__ void load_block(const TV *__restrict__ a, long long k, TA out[BS * BS]) {
+#pragma unroll
+    for (int q = 0; q < BS * BS; ++q) out[q] = (TA)ldv(a, k * BS * BS + q);
+}
+template <>
+__device__ __forceinline__ void load_block<2, double, double>(const double *__restrict__ a, long long k,
+                                                              double out[4]) {
+    const double2 *p = reinterpret_cast<const double2 *>(a + k * 4);
+    const double2 v0 = __ldg(p), v1 = __ldg(p + 1);
+    out[0] = v0.x;
+    out[1] = v0.y;
+    out[2] = v1.x;
+    out[3] = v1.y;
+}
+template <>
+__device__ __forceinline__ void load_block<2, float, float>(const float *__restrict__ a, long long k,
+                                                            float out[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(a + k * 4));
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+    out[3] = v.w;
+}
+
+template <int BS, typename TA>
+__device__ __forceinline__ void block_solve(const TA D[BS * BS], const TA rhs[BS], TA out[BS]) {
+    if (BS == 2) {
+        const TA det = D[0] * D[3] - D[1] * D[2];
+        const TA inv = det != (TA)0 ? (TA)1 / det : (TA)0;
+        out[0] = (D[3] * rhs[0] - D[1] * rhs[1]) * inv;
+        out[1] = (D[0] * rhs[1] - D[2] * rhs[0]) * inv;
+    } else {
+        // adjugate / determinant of a 3x3 block
+        const TA c00 = D[4] * D[8] - D[5] * D[7], c01 = D[5] * D[6] - D[3] * D[8], c02 = D[3] * D[7] - D[4] * D[6];
+        const TA det = D[0] * c00 + D[1] * c01 + D[2] * c02;
+        const TA inv = det != (TA)0 ? (TA)1 / det : (TA)0;
+        const TA c10 = D[2] * D[7] - D[1] * D[8], c11 = D[0] * D[8] - D[2] * D[6], c12 = D[1] * D[6] - D[0] * D[7];
+        const TA c20 = D[1] * D[5] - D[2] * D[4], c21 = D[2] * D[3] - D[0] * D[5], c22 = D[0] * D[4] - D[1] * D[3];
+        out[0] = (c00 * rhs[0] + c10 * rhs[1] + c20 * rhs[2]) * inv;
+        out[1] = (c01 * rhs[0] + c11 * rhs[1] + c21 * rhs[2]) * inv;
+        out[2] = (c02 * rhs[0] + c12 * rhs[1] + c22 * rhs[2]) * inv;
+    }
+}
+
+// x_i <- (1 - w omega) x_i + w D_i^-1 (omega b_i - sum_{j != i} A_ij (x_j - (1 - omega) vt_j))
+// (jxf_ParBSRHGSRelax's update with res = b, res0 = -sum A x, res2 = sum A vt);
+// plain (w = omega = 1): x_i <- D_i^-1 (b_i - sum A_ij x_j).  vt = x at sweep start.
+template <int BS, int V, typename TV, typename TA>
+__global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
+                          const int *__restrict__ ja, const TV *__restrict__ a, const double *__restrict__ b,
+                          double *x, const double *__restrict__ vt, TA w, TA omega, int plain) {
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = r0 + (int)(gt / V);
+    const int lane = (int)(gt % V);
+    const bool live = t < r1;
+    const int d = live ? ia[t] : 0, e = live ? ia[t + 1] : 0;
+    const TA omo = (TA)1 - omega;
+    TA acc[BS];
+#pragma unroll
+    for (int q = 0; q < BS; ++q) acc[q] = 0;
+    for (int k = d + 1 + lane; k < e; k += V) {
+        const int j = __ldg(ja + k);
+        TA blk[BS * BS], c[BS];
+        load_block<BS, TV, TA>(a, k, blk);
+#pragma unroll
+        for (int m = 0; m < BS; ++m) {
+            const TA xj = (TA)x[(long long)j * BS + m];
+            c[m] = plain ? xj : xj - omo * (TA)__ldg(vt + (long long)j * BS + m);
+        }
+#pragma unroll
+        for (int q = 0; q < BS; ++q)
+#pragma unroll
+            for (int m = 0; m < BS; ++m) acc[q] += blk[q * BS + m] * c[m];
+    }
+#pragma unroll
+    for (int q = 0; q < BS; ++q) acc[q] = group_sum<V, TA>(acc[q]);
+    if (!live || lane != 0) return;
+    const int i = perm[t];
+    TA D[BS * BS], rhs[BS], out[BS];
+    load_block<BS, TV, TA>(a, d, D);
+#pragma unroll
+    for (int q = 0; q < BS; ++q) rhs[q] = (plain ? (TA)1 : omega) * (TA)b[(long long)i * BS + q] - acc[q];
+    block_solve<BS, TA>(D, rhs, out);
+    const TA prod = (TA)1 - w * omega;
+#pragma unroll
+    for (int q = 0; q < BS; ++q) {
+        const long long o = (long long)i * BS + q;
+        x[o] = plain ? (double)out[q] : (double)(prod * (TA)vt[o] + w * out[q]);
+    }
+}
+
+// Stage 2 on a sliced-ELL block copy (one thread per block row, slot 0 = the
+// diagonal block, padding blocks are zero): same update as hgs_color.
+template <int BS, typename TV, typename TA>
+__global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long *__restrict__ sp,
+                                                const int *__restrict__ col, const TV *__restrict__ a,
+                                                const int *__restrict__ rows, const double *__restrict__ b,
+                                                double *x, const double *__restrict__ vt, TA w, TA omega,
+                                                int plain) {
+    const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= r1) return;
+    const int i = __ldg(rows + t);
+    if (i < 0) return;
+    const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
+    const int wd = (int)((b1 - b0) >> 5);
+    const long long o = b0 + (t & 31);
+    const TA omo = (TA)1 - omega;
+    TA rhs[BS], xv[BS], D[BS * BS], acc[BS];
+#pragma unroll
+    for (int q = 0; q < BS; ++q) {
+        rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
+        xv[q] = plain ? (TA)0 : (TA)vt[(long long)i * BS + q];
+        acc[q] = 0;
+    }
+    load_block<BS, TV, TA>(a, o, D);
+    int k = 1;
+    for (; k + 1 < wd; k += 2) {
+        const long long p0 = o + (long long)k * 32, p1 = p0 + 32;
+        const int j0 = __ldg(col + p0), j1 = __ldg(col + p1);
+        TA B0[BS * BS], B1[BS * BS], c0[BS], c1[BS];
+        load_block<BS, TV, TA>(a, p0, B0);
+        load_block<BS, TV, TA>(a, p1, B1);
+#pragma unroll
+        for (int m = 0; m < BS; ++m) {
+            const TA x0 = (TA)x[(long long)j0 * BS + m], x1 = (TA)x[(long long)j1 * BS + m];
+            c0[m] = plain ? x0 : x0 - omo * (TA)__ldg(vt + (long long)j0 * BS + m);
+            c1[m] = plain ? x1 : x1 - omo * (TA)__ldg(vt + (long long)j1 * BS + m);
+        }
+#pragma unroll
+        for (int q = 0; q < BS; ++q)
+#pragma unroll
+            for (int m = 0; m < BS; ++m) acc[q] += B0[q * BS + m] * c0[m] + B1[q * BS + m] * c1[m];
+    }
+    if (k < wd) {
+        const long long p0 = o + (long long)k * 32;
+        const int j0 = __ldg(col + p0);
+        TA B0[BS * BS], c0[BS];
+        load_block<BS, TV, TA>(a, p0, B0);
+#pragma unroll
+        for (int m = 0; m < BS; ++m) {
+            const TA x0 = (TA)x[(long long)j0 * BS + m];
+            c0[m] = plain ? x0 : x0 - omo * (TA)__ldg(vt + (long long)j0 * BS + m);
+        }
+#pragma unroll
+        for (int q = 0; q < BS; ++q)
+#pragma unroll
+            for (int m = 0; m < BS; ++m) acc[q] += B0[q * BS + m] * c0[m];
+    }
+    TA r2[BS], out[BS];
+#pragma unroll
+    for (int q = 0; q < BS; ++q) r2[q] = (plain ? (TA)1 : omega) * rhs[q] - acc[q];
+    block_solve<BS, TA>(D, r2, out);
+    const TA prod = (TA)1 - w * omega;
+#pragma unroll
+    for (int q = 0; q < BS; ++q)
+        x[(long long)i * BS + q] = plain ? (double)out[q] : (double)(prod * xv[q] + w * out[q]);
+}
+
+// ---- sliced-ELL fill ----------------------------------------------------------
+template <typename TV>
+__device__ __forceinline__ TV cvt_val(double v, double sc);
+template <>
+__device__ __forceinline__ double cvt_val<double>(double v, double) { return v; }
+template <>
+__device__ __forceinline__ float cvt_val<float>(double v, double) { return (float)v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 cvt_val<__nv_bfloat16>(double v, double sc) {
+    return __float2bfloat16_rn((float)(v / sc));
+}
+
+// Stored row t receives the entries of CSR/BSR row rows[t] (E values per
+// entry, E = 1 or bs*bs) in slot-major order; rscale != nullptr: BF16 row scale.
+template <typename TV>
+__global__ void sell_fill(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
+                          const int *__restrict__ ia, const int *__restrict__ ja, const double *__restrict__ a,
+                          int E, int *__restrict__ col, TV *__restrict__ val, float *__restrict__ rscale) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nstored) return;
+    const int i = rows[t];
+    const long long b0 = sp[t >> 5], b1 = sp[(t >> 5) + 1];
+    const int w = (int)((b1 - b0) >> 5);
+    const long long o = b0 + (t & 31);
+    const int d = i >= 0 ? ia[i] : 0;
+    const int len = i >= 0 ? ia[i + 1] - d : 0;
+    double sc = 1.0;
+    if (rscale) {
+        double m = 0.0;
+        for (long long q = (long long)d * E; q < (long long)(d + len) * E; ++q) m = fmax(m, fabs(a[q]));
+        sc = m > 0.0 ? m : 1.0;
+        rscale[t] = (float)sc;
+    }
+    for (int k = 0; k < w; ++k) {
+        const long long p = o + (long long)k * 32;
+        if (k < len) {
+            col[p] = ja[d + k];
+            for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(a[(long long)(d + k) * E + q], sc);
+        } else {
+            col[p] = 0;
+            for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(0.0, 1.0);
+        }
+    }
+}
+
+// ---- setup helpers ----------------------------------------------------------
+__global__ void to_f32(long long n, const double *__restrict__ in, float *__restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+// BF16 values scaled per row by max |a_ij| (kept in FP32).
+__global__ void to_bf16_rows(int n, const int *__restrict__ ia, const double *__restrict__ a,
+                             float *__restrict__ rscale, __nv_bfloat16 *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double m = 0.0;
+    for (int k = ia[i]; k < ia[i + 1]; ++k) m = fmax(m, fabs(a[k]));
+    const double sc = m > 0.0 ? m : 1.0;
+    rscale[i] = (float)sc;
+    for (int k = ia[i]; k < ia[i + 1]; ++k) out[k] = __float2bfloat16_rn((float)(a[k] / sc));
+}
+
+// 1 / a_ii where the diagonal is the first stored entry, else 0 (row skipped).
+template <typename TX>
+__global__ void dinv_diag(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                          const double *__restrict__ a, TX *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d = ia[i];
+    const bool has = d < ia[i + 1] && ja[d] == i && a[d] != 0.0;
+    out[i] = has ? (TX)(1.0 / a[d]) : (TX)0;
+}
+
+template <typename TX>
+__global__ void dinv_l1(int n, const int *__restrict__ ia, const double *__restrict__ a, TX *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int k = ia[i]; k < ia[i + 1]; ++k) s += fabs(a[k]);
+    out[i] = s > 0.0 ? (TX)(1.0 / s) : (TX)0;
+}
+
+// y = D^-1 A x in FP64 (power iteration); dinv from dinv_diag<double>.
+__global__ void dinv_a_x(int n, const int *__restrict__ ia, const int *__restrict__ ja, const double *__restrict__ a,
+                         const double *__restrict__ dinv, const double *__restrict__ x, double *__restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int k = ia[i]; k < ia[i + 1]; ++k) s += a[k] * x[ja[k]];
+    y[i] = dinv[i] * s;
+}
+
+template <typename TA, typename TB>
+__global__ void convert(long long n, const TA *__restrict__ in, TB *__restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (TB)in[i];
+}
+
+}  // namespace fk
+}  // namespace jxcpr

@@ -297,116 +297,6 @@ __global__ void hgs_sweep_block_kernel(int ngroups, const int *__restrict__ gptr
     }
 }
 
-// One colour class per launch (multicolour mode: classes are independent sets).
-template <int BS>
-__global__ void hgs_group_kernel(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
-                                 const int *__restrict__ ja, const double *__restrict__ a,
-                                 const int *__restrict__ rank, const double *__restrict__ b, double *x,
-                                 const double *__restrict__ vt, double w, double omega, int plain) {
-    const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < r1) hgs_row<BS>(perm[t], ia, ja, a, rank, b, x, vt, w, omega, plain);
-}
-
-void hgs_sweep_groups(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
-                      double *vt, double w, double omega, cudaStream_t s) {
-    const int nb = A.nb;
-    if (nb == 0 || sch.ngroups == 0) return;
-    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * A.bs, cudaMemcpyDeviceToDevice, s));
-    const double eps = 2.220446049250313e-16;
-    const int plain = (fabs(w - 1) < eps && fabs(omega - 1) < eps) ? 1 : 0;
-    for (int g = 0; g < sch.ngroups; ++g) {
-        const int r0 = sch.h_group_ptr[g], r1 = sch.h_group_ptr[g + 1];
-        if (r1 <= r0) continue;
-        if (A.bs == 2)
-            hgs_group_kernel<2><<<div_up(r1 - r0, 128), 128, 0, s>>>(r0, r1, sch.perm.get(), A.ia, A.ja, A.a, rank, b,
-                                                                    x, vt, w, omega, plain);
-        else
-            hgs_group_kernel<3><<<div_up(r1 - r0, 128), 128, 0, s>>>(r0, r1, sch.perm.get(), A.ia, A.ja, A.a, rank, b,
-                                                                    x, vt, w, omega, plain);
-        JX_LAUNCH_CHECK();
-    }
-}
-
-// Multicolour HGS on the colour-ordered copy: row t of the copy is row perm[t];
-// neighbours of earlier classes are read updated from x (previous launches),
-// later classes equal their start-of-sweep values, so x is read directly.
-template <int BS>
-__global__ void __launch_bounds__(128) hgs_color_kernel(int r0, int r1, const int *__restrict__ perm,
-                                                        const int *__restrict__ ia, const int *__restrict__ ja,
-                                                        const double *__restrict__ a, const double *__restrict__ b,
-                                                        double *x, const double *__restrict__ vt, double w,
-                                                        double omega, int plain) {
-    constexpr int B2 = BS * BS;
-    const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= r1) return;
-    const int i = perm[t];
-    const long long d = ia[t], e = ia[t + 1];
-    double res[BS], out[BS];
-#pragma unroll
-    for (int k = 0; k < BS; ++k) res[k] = b[(long long)i * BS + k];
-    if (plain) {
-        for (long long jj = d + 1; jj < e; ++jj) {
-            const int j = __ldg(ja + jj);
-            double xj[BS];
-#pragma unroll
-            for (int k = 0; k < BS; ++k) xj[k] = x[(long long)j * BS + k];
-            blk_matvec_stable<BS>(-1.0, a + jj * B2, xj, res);
-        }
-        blk_inv_matvec<BS>(a + d * B2, res, out);
-#pragma unroll
-        for (int k = 0; k < BS; ++k) x[(long long)i * BS + k] = out[k];
-        return;
-    }
-    double res0[BS], res2[BS], tmp[BS];
-#pragma unroll
-    for (int k = 0; k < BS; ++k) {
-        res0[k] = 0.0;
-        res2[k] = 0.0;
-    }
-    for (long long jj = d + 1; jj < e; ++jj) {
-        const int j = __ldg(ja + jj);
-        double xj[BS], vj[BS];
-#pragma unroll
-        for (int k = 0; k < BS; ++k) {
-            xj[k] = x[(long long)j * BS + k];
-            vj[k] = __ldg(vt + (long long)j * BS + k);
-        }
-        blk_matvec_stable<BS>(-1.0, a + jj * B2, xj, res0);
-        blk_matvec_stable<BS>(1.0, a + jj * B2, vj, res2);
-    }
-    const double prod = 1.0 - w * omega, omo = 1.0 - omega;
-#pragma unroll
-    for (int k = 0; k < BS; ++k) tmp[k] = omega * res[k] + res0[k] + omo * res2[k];
-    blk_inv_matvec<BS>(a + d * B2, tmp, out);
-#pragma unroll
-    for (int k = 0; k < BS; ++k) {
-        double xv = vt[(long long)i * BS + k];  // row i is updated only here: its x equals vt
-        xv *= prod;
-        xv += w * out[k];
-        x[(long long)i * BS + k] = xv;
-    }
-}
-
-void hgs_sweep_colors_perm(const BsrView<double> &Aperm, const Schedule &fwd, const double *b, double *x,
-                           double *vt, double w, double omega, cudaStream_t s) {
-    const int nb = Aperm.nb;
-    if (nb == 0 || fwd.ngroups == 0) return;
-    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * Aperm.bs, cudaMemcpyDeviceToDevice, s));
-    const double eps = 2.220446049250313e-16;
-    const int plain = (fabs(w - 1) < eps && fabs(omega - 1) < eps) ? 1 : 0;
-    for (int g = 0; g < fwd.ngroups; ++g) {
-        const int r0 = fwd.h_group_ptr[g], r1 = fwd.h_group_ptr[g + 1];
-        if (r1 <= r0) continue;
-        if (Aperm.bs == 2)
-            hgs_color_kernel<2><<<div_up(r1 - r0, 128), 128, 0, s>>>(r0, r1, fwd.perm.get(), Aperm.ia, Aperm.ja,
-                                                                    Aperm.a, b, x, vt, w, omega, plain);
-        else
-            hgs_color_kernel<3><<<div_up(r1 - r0, 128), 128, 0, s>>>(r0, r1, fwd.perm.get(), Aperm.ia, Aperm.ja,
-                                                                    Aperm.a, b, x, vt, w, omega, plain);
-        JX_LAUNCH_CHECK();
-    }
-}
-
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------

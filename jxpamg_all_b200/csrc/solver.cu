@@ -23,13 +23,65 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     A = A_;
     Timer t;
     t.start(s);
+    const bool fast_path = prm.smoother_order != ORDER_EXACT;
     amg.prm.order = prm.smoother_order;
-    amg.prm.coarse_exact = prm.coarse_exact;
+    amg.prm.coarse_exact = fast_path ? 0 : prm.coarse_exact;
     amg.prm.max_colors = prm.max_colors;
+    amg.prm.strong_threshold = prm.strong_threshold;
+    amg.prm.theta_for_level = nullptr;
+    fast.reset();
+    learned_used = 0;
+    plan = LearnedPlan();
+    if (fast_path && (prm.fast_smoother == 2 || prm.record_features)) {
+        plan.active = prm.fast_smoother == 2;
+        plan.record = true;
+        const double th = prm.strong_threshold;
+        amg.prm.theta_for_level = [this, th, s](int level, const CsrView<double> &Al) {
+            return learned_predict_level(plan, level, Al, th, s);
+        };
+    }
     DeviceCsr Ap;
     bsr_pressure_csr(A, prm.pressure_index, Ap, s);
     amg_setup(amg, std::move(Ap), s);
-    if (prm.smoother_order != ORDER_EXACT) permute_rows_bsr(A, amg.levels[0]->fwd.perm.get(), Aperm, s);
+    amg.prm.theta_for_level = nullptr;
+    if (fast_path) {
+        CprConfig cfg;
+        cfg.pressure_index = prm.pressure_index;
+        cfg.stage1_maxit = prm.stage1_maxit;
+        cfg.stage2_maxit = prm.stage2_maxit;
+        cfg.stage2_solver_type = prm.stage2_solver_type;
+        cfg.stage2_w = prm.stage2_relax_weight;
+        cfg.stage2_omega = prm.stage2_omega;
+        FastOptions opt;
+        opt.precision = prm.precision;
+        opt.bf16_level = prm.bf16_level;
+        opt.smoother = prm.fast_smoother == 0 ? 0 : (prm.fast_smoother == 3 ? 2 : 1);
+        opt.cheb_lower = prm.cheb_lower;
+        opt.cheb_upper = prm.cheb_upper;
+        opt.stage2_lanes = prm.stage2_lanes;
+        opt.autotune = prm.autotune;
+        opt.graphs = prm.graphs;
+        if (plan.active) {
+            opt.level_lower = plan.lower;
+            opt.level_upper = plan.upper;
+        }
+        fast.reset(make_fast_cpr(amg, A, cfg, opt, s));
+        if (plan.active) {
+            learned_used = 1;
+            if (prm.learned_fallback) {
+                // the plain smoother settings stay whenever the learned ones converge worse
+                FastOptions plain = opt;
+                plain.smoother = 0;
+                std::unique_ptr<FastCprBase> alt(make_fast_cpr(amg, A, cfg, plain, s));
+                factor_fast = fast->vcycle_factor(6, s);
+                factor_plain = alt->vcycle_factor(6, s);
+                if (!(factor_fast <= factor_plain * 1.02)) {
+                    fast = std::move(alt);
+                    learned_used = 0;
+                }
+            }
+        }
+    }
     rp.alloc(A.nb > 0 ? A.nb : 1);
     xp.alloc(A.nb > 0 ? A.nb : 1);
     vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
@@ -39,24 +91,41 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
 }
 
 void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
+    if (fast) {
+        fast->apply(r, z, s);
+        return;
+    }
     const int nb = A.nb, bs = A.bs;
     restrict_pressure(nb, bs, prm.pressure_index, r, rp.get(), s);
     JX_CUDA(cudaMemsetAsync(xp.get(), 0, sizeof(double) * nb, s));
     for (int it = 0; it < prm.stage1_maxit; ++it) amg_vcycle(amg, rp.get(), xp.get(), s);
     prolong_pressure(nb, bs, prm.pressure_index, xp.get(), z, s);
-    const AmgLevel &L0 = *amg.levels[0];
-    (void)L0;
     if (prm.stage2_solver_type == 2)
         for (int it = 0; it < prm.stage2_maxit; ++it) stage2_sweep(r, z, s);
 }
 
 void CprPrecond::stage2_sweep(const double *r, double *z, cudaStream_t s) {
+    if (fast) {
+        fast->stage2_sweep(r, z, s);
+        return;
+    }
     const AmgLevel &L0 = *amg.levels[0];
-    if (prm.smoother_order == ORDER_EXACT)
-        hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
-                  amg.err.get(), s);
-    else
-        hgs_sweep_colors_perm(Aperm.view(), L0.fwd, r, z, vt.get(), prm.stage2_relax_weight, prm.stage2_omega, s);
+    hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
+              amg.err.get(), s);
+}
+
+void CprPrecond::vcycle(const double *f, double *u, cudaStream_t s) {
+    if (!fast) {
+        amg_vcycle(amg, f, u, s);
+        return;
+    }
+    // fast path cycles start from zero: u += V(f - A_p u)
+    const CsrView<double> Ap = amg.levels[0]->A.view();
+    double *res = vt.get(), *cor = vt.get() + Ap.nrows;
+    copy_dev(Ap.nrows, f, res, s);
+    csr_spmv(Ap, -1.0, u, 1.0, res, s);
+    fast->vcycle(res, cor, s);
+    axpy_dev(Ap.nrows, 1.0, cor, u, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -116,6 +185,9 @@ void Gmres::setup(int n_, cudaStream_t s) {
     n = n_;
     p.clear();
     for (int i = 0; i <= prm.k_dim; ++i) p.emplace_back((size_t)(n > 0 ? n : 1));
+    zf.clear();
+    if (prm.flexible)
+        for (int i = 0; i < prm.k_dim; ++i) zf.emplace_back((size_t)(n > 0 ? n : 1));
     r.alloc(n > 0 ? n : 1);
     w.alloc(n > 0 ? n : 1);
     partials.alloc(reduce_partials() + 8);
@@ -158,6 +230,7 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
         else copy_dev(nl, in, out, s);
     };
     const int np = ops.np;
+    const bool flexible = prm.flexible && (int)zf.size() >= k_dim;
 
     copy_dev(nl, b, p[0].get(), s);
     spmv(-1.0, x, 1.0, p[0].get());
@@ -208,9 +281,10 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
         while (i < k_dim && iter < prm.max_iter) {
             ++i;
             ++iter;
-            JX_CUDA(cudaMemsetAsync(r.get(), 0, sizeof(double) * nl, s));
-            precond(p[i - 1].get(), r.get());
-            spmv(1.0, r.get(), 0.0, p[i].get());
+            double *zi = flexible ? zf[i - 1].get() : r.get();
+            JX_CUDA(cudaMemsetAsync(zi, 0, sizeof(double) * nl, s));
+            precond(p[i - 1].get(), zi);
+            spmv(1.0, zi, 0.0, p[i].get());
             // modified Gram-Schmidt, fused passes
             for (int j = 0; j <= i; ++j) {
                 const double *pprev = j > 0 ? p[j - 1].get() : nullptr;
@@ -262,12 +336,17 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
             t += rs[k];
             rs[k] = t / hh[k][k];
         }
-        copy_dev(nl, p[i - 1].get(), w.get(), s);
-        scale_dev(nl, rs[i - 1], w.get(), s);
-        for (int j = i - 2; j >= 0; --j) axpy_dev(nl, rs[j], p[j].get(), w.get(), s);
-        JX_CUDA(cudaMemsetAsync(r.get(), 0, sizeof(double) * nl, s));
-        precond(w.get(), r.get());
-        axpy_dev(nl, 1.0, r.get(), x, s);
+        if (flexible) {
+            // x += Z y (the preconditioned directions were kept)
+            for (int j = i - 1; j >= 0; --j) axpy_dev(nl, rs[j], zf[j].get(), x, s);
+        } else {
+            copy_dev(nl, p[i - 1].get(), w.get(), s);
+            scale_dev(nl, rs[i - 1], w.get(), s);
+            for (int j = i - 2; j >= 0; --j) axpy_dev(nl, rs[j], p[j].get(), w.get(), s);
+            JX_CUDA(cudaMemsetAsync(r.get(), 0, sizeof(double) * nl, s));
+            precond(w.get(), r.get());
+            axpy_dev(nl, 1.0, r.get(), x, s);
+        }
         if (r_norm <= epsilon && iter >= prm.min_iter) {
             copy_dev(nl, b, r.get(), s);
             spmv(-1.0, x, 1.0, r.get());

@@ -4,9 +4,13 @@
 #include <string>
 #include <vector>
 
+#include <memory>
+
 #include "amg.cuh"
 #include "common.cuh"
+#include "fast.cuh"
 #include "kernels.cuh"
+#include "learned.cuh"
 
 namespace jxcpr {
 
@@ -34,11 +38,26 @@ struct SolverParams {
     // decoupling applied by the solver object (0 none, 1 ABF, 5 True-IMPES)
     int decouple = 0;
     int consistent_rhs = 0;
+    // AMG strength threshold (jxf_cpr.c:331 sets 0.25)
+    double strong_threshold = 0.25;
     // device execution choices
-    int smoother_order = ORDER_EXACT;
+    int smoother_order = ORDER_EXACT;  // 0 exact order (bit-identical), 1 throughput / mixed path
     int coarse_exact = 1;
     int max_colors = 8;
     int use_tma_spmv = 0;
+    // fast path (smoother_order 1)
+    int precision = 0;       // 0 FP64, 1 FP32 preconditioner, 2 FP32 + BF16 coarse levels
+    int bf16_level = 1;      // precision 2: first BF16 level
+    int fast_smoother = 0;   // 0 colour GS / l1-Jacobi; 1 Chebyshev-3 on the levels without a GS colouring;
+                             // 2 as 1 with learned thresholds and intervals; 3 Chebyshev-3 on every level
+    int autotune = 1;        // fast path: time the operator layouts at setup and keep the fastest
+    int graphs = 1;          // fast path: each CPR application replays one captured CUDA graph
+    int flexible = 0;        // 1: flexible GMRES (stores M^-1 v_j; for inexact / low-precision preconditioners)
+    double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
+    double cheb_upper = 1.1;
+    int stage2_lanes = 4;
+    int learned_fallback = 1;  // learned mode: keep the plain smoothers when their V-cycle factor is lower
+    int record_features = 0;   // fast path: record the per-level features (training data)
 };
 
 struct Timer {
@@ -65,8 +84,11 @@ struct Timer {
 struct CprPrecond {
     SolverParams prm;
     BsrView<double> A;  // decoupled system matrix (owned by the solver)
-    DeviceBsr Aperm;    // throughput mode: rows of A in level-0 colour order (stage 2)
     Amg amg;
+    std::unique_ptr<FastCprBase> fast;  // smoother_order 1: throughput / mixed-precision preconditioner
+    double factor_fast = 0.0, factor_plain = 0.0;  // learned mode: measured V-cycle factors
+    int learned_used = 0;
+    LearnedPlan plan;  // per-level features and learned settings of the last setup
     DevBuf<double> rp, xp, vt;
     double stats[4] = {0, 0, 0, 0};  // stage1 setup, stage1 solve, stage2 setup, stage2 solve (seconds)
     bool ready = false;
@@ -74,6 +96,8 @@ struct CprPrecond {
     void apply(const double *r, double *z, cudaStream_t s);
     // one stage-2 block hybrid Gauss-Seidel sweep on A z = r (z in/out)
     void stage2_sweep(const double *r, double *z, cudaStream_t s);
+    // one pressure V-cycle on A_p u = f, u in/out (FP64)
+    void vcycle(const double *f, double *u, cudaStream_t s);
     int *err() { return amg.err.get(); }
 };
 
@@ -91,6 +115,7 @@ struct Gmres {
     SolverParams prm;
     int n = 0;
     std::vector<DevBuf<double>> p;
+    std::vector<DevBuf<double>> zf;       // flexible GMRES: z_j = M^-1 p_j
     DevBuf<double> r, w, partials, scal;  // scal: device scalars (dots)
     int *kerr = nullptr;
     void setup(int n_, cudaStream_t s);

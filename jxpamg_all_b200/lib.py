@@ -31,6 +31,8 @@ def _declare(lib):
     lib.jxcpr_bsr_matvec_dev_f32.argtypes = lib.jxcpr_bsr_matvec_dev.argtypes
     lib.jxcpr_dot_dev.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.jxcpr_dot_dev_noalloc.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
+    _declare_solver(lib)
+    _declare_mlp(lib)
 
 
 def load():
@@ -70,11 +72,17 @@ def _declare_solver(lib):
     lib.jxcpr_solver_cpr_apply.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_vcycle.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_stage2_sweep.argtypes = [P, P, P, c_int]
+    lib.jxcpr_solver_level_info.argtypes = [P, c_int, P, P, P, P]
+    lib.jxcpr_solver_level_features.argtypes = [P, c_int, P]
+    lib.jxcpr_solver_learned_status.argtypes = [P, P]
 
 
-_orig_declare = _declare
-
-
-def _declare(lib):  # noqa: F811
-    _orig_declare(lib)
-    _declare_solver(lib)
+def _declare_mlp(lib):
+    P = c_void_p
+    lib.jxcpr_mlp_set_weights.argtypes = [P]
+    lib.jxcpr_mlp_get_weights.argtypes = [P]
+    lib.jxcpr_mlp_forward_host.argtypes = [P, P, P]
+    lib.jxcpr_mlp_forward.argtypes = [P, P, c_int, P, P, P]
+    lib.jxcpr_mlp_loss_grad.argtypes = [P, P, P, c_int, P, P, P, P]
+    lib.jxcpr_mlp_adam.argtypes = [P, P, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   c_int, P]

@@ -27,8 +27,15 @@ class CprGmres:
     Integer options: k_dim, max_iter, min_iter, is_check_restarted,
     pressure_index, stage1_maxit, stage2_maxit, stage1_solver_type,
     stage2_solver_type, decouple, consistent_rhs, smoother_order, coarse_exact,
-    use_tma_spmv.  Real options: tol, a_tol, threshold, convfac_threshold,
-    stage2_relax_weight, stage2_omega.
+    use_tma_spmv, precision, bf16_level, fast_smoother, stage2_lanes,
+    learned_fallback, record_features.  Real options: tol, a_tol, threshold,
+    convfac_threshold, stage2_relax_weight, stage2_omega, strong_threshold,
+    cheb_lower, cheb_upper.
+
+    smoother_order 0 is the exact-order path (preconditioner bit-identical to
+    the reference); 1 the throughput path, whose precision (0 FP64, 1 FP32,
+    2 FP32 + BF16 coarse levels) and fast_smoother (0 multicolour GS /
+    l1-Jacobi, 1 Chebyshev-3, 2 learned) select the mixed and learned forms.
     """
 
     def __init__(self, **options):
@@ -132,6 +139,24 @@ class CprGmres:
         xp = np.zeros(self.nb) if xp is None else np.array(xp, dtype=np.float64)
         _lib.check(self._so.jxcpr_solver_vcycle(self.h, _ptr(np.ascontiguousarray(rp, np.float64)), _ptr(xp), 0))
         return xp
+
+    def level_info(self, lev):
+        sm, st = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        th, ch = np.zeros(1), np.zeros(6)
+        if self._so.jxcpr_solver_level_info(self.h, lev, _ptr(sm), _ptr(st), _ptr(th), _ptr(ch)) < 0:
+            return None
+        return dict(smoother=int(sm[0]), storage=int(st[0]), theta=float(th[0]), cheb=ch[:3].copy(),
+                    interval=(float(ch[3]), float(ch[4])), lambda_max=float(ch[5]))
+
+    def level_features(self, lev):
+        f = np.zeros(16, np.float32)
+        n = self._so.jxcpr_solver_level_features(self.h, lev, _ptr(f))
+        return None if n < 0 else f[:n].copy()
+
+    def learned_status(self):
+        o = np.zeros(3)
+        _lib.check(self._so.jxcpr_solver_learned_status(self.h, _ptr(o)))
+        return dict(learned_used=bool(o[0]), factor_learned=float(o[1]), factor_plain=float(o[2]))
 
     def close(self):
         if getattr(self, "h", None):
