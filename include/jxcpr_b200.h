@@ -155,7 +155,10 @@ JXCPR_API int jxcpr_solver_level_info(jxcpr_solver *solver, int level, int *smoo
 /* Features (16 floats) recorded for `level` by a setup with fast_smoother 2 or record_features 1;
  * returns the count or -1. */
 JXCPR_API int jxcpr_solver_level_features(jxcpr_solver *solver, int level, float *features);
-/* out[3] = {learned settings in use (1/0), V-cycle factor with them, with the plain smoothers}. */
+/* out[5] = {learned settings in use (1/0), GMRES residual reduction per iteration over an 8-iteration
+ * probe (tol 0, b = A 1) with the learned settings, the same with the plain smoothers on the same
+ * hierarchy, modelled bytes per GMRES iteration with each}.  The setup keeps the learned settings
+ * unless their residual reduction per byte is worse. */
 JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
 
 /* ---- learned settings: 16 -> 64 (tanh) -> 3 MLP, FP32; no reference counterpart -----------------

@@ -61,7 +61,8 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"record_features", &p.record_features},
                {"flexible", &p.flexible},
                {"autotune", &p.autotune},
-               {"graphs", &p.graphs}};
+               {"graphs", &p.graphs},
+               {"orthog", &p.orthog}};
     if (!key) return JXCPR_ERROR_ARG;
     if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
     for (auto &e : tab)
@@ -84,6 +85,7 @@ int set_real_param(SolverParams &p, const char *key, double v) {
                {"stage2_relax_weight", &p.stage2_relax_weight},
                {"stage2_omega", &p.stage2_omega},
                {"strong_threshold", &p.strong_threshold},
+               {"strong_threshold_coarse", &p.strong_threshold_coarse},
                {"cheb_lower", &p.cheb_lower},
                {"cheb_upper", &p.cheb_upper}};
     if (!key) return JXCPR_ERROR_ARG;
@@ -251,6 +253,8 @@ int jxcpr_solver_learned_status(jxcpr_solver *h, double *out) {
     out[0] = h->s.cpr.learned_used;
     out[1] = h->s.cpr.factor_fast;
     out[2] = h->s.cpr.factor_plain;
+    out[3] = h->s.cpr.probe_bytes[0];
+    out[4] = h->s.cpr.probe_bytes[1];
     return JXCPR_SUCCESS;
 }
 

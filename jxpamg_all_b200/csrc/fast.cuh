@@ -103,6 +103,9 @@ struct FastCprBase {
     virtual void level_info(int l, int *smoother, int *kind, double *cheb) const = 0;
     // Asymptotic convergence factor of the V-cycle on A_0 e = 0 (power method, `cycles` cycles)
     virtual double vcycle_factor(int cycles, cudaStream_t s) = 0;
+    // Modelled bytes one application moves (operator and vector traffic of
+    // every smoother pass, residual, transfer and stage-2 sweep).
+    virtual double apply_bytes() const = 0;
     // One line per tuned operator: "name rows mean_row layout time_us".
     std::vector<std::string> tune_log;
 };

@@ -347,6 +347,7 @@ struct FastCpr final : FastCprBase {
     int nc = 0;
     LevelMat st2;  // decoupled block matrix, level-0 colour classes as segments
     DevBuf<double> vt;
+    DevBuf<float> r32, z32, vt32;  // mixed path: stage-2 vectors in FP32
     CsrView<double> A0;  // FP64 level-0 operator (convergence-factor probe)
     DevBuf<double> pe, pr, pc, partials, nrm;
 
@@ -439,18 +440,18 @@ struct FastCpr final : FastCprBase {
         }
     }
 
-    template <typename TV>
-    void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const double *r, double *z, TA w,
-                        TA om, int plain, cudaStream_t s) {
+    template <typename TV, typename TXV>
+    void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp,
+                        TA w, TA om, int plain, cudaStream_t s) {
         const int grid = div_up((long long)(r1 - r0) * V, 128);
 #define JX_HGS_CSR(VV)                                                                                        \
     do {                                                                                                      \
         if (bs == 2)                                                                                          \
-            fk::hgs_color<2, VV, TV, TA><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, z, \
-                                                               vt.get(), w, om, plain);                       \
+            fk::hgs_color<2, VV, TV, TA, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, \
+                                                                    z, vtp, w, om, plain);                     \
         else                                                                                                  \
-            fk::hgs_color<3, VV, TV, TA><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, z, \
-                                                               vt.get(), w, om, plain);                       \
+            fk::hgs_color<3, VV, TV, TA, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, \
+                                                                    z, vtp, w, om, plain);                     \
     } while (0)
         switch (V) {
             case 1: JX_HGS_CSR(1); break;
@@ -463,37 +464,55 @@ struct FastCpr final : FastCprBase {
 #undef JX_HGS_CSR
     }
 
-    void stage2_sweep(const double *r, double *z, cudaStream_t s) override {
+    // One stage-2 sweep on vectors of type TXV (FP64 path: the caller's r, z;
+    // mixed path: FP32 copies), vtp = start-of-sweep copy of z.
+    template <typename TXV>
+    void sweep_typed(const TXV *r, TXV *z, TXV *vtp, cudaStream_t s) {
         const LevelMat &M = st2;
         if (M.n == 0) return;
-        JX_CUDA(cudaMemcpyAsync(vt.get(), z, sizeof(double) * M.n * bs, cudaMemcpyDeviceToDevice, s));
+        JX_CUDA(cudaMemcpyAsync(vtp, z, sizeof(TXV) * M.n * bs, cudaMemcpyDeviceToDevice, s));
         const double eps = 2.220446049250313e-16;
         const int plain = (fabs(cfg.stage2_w - 1) < eps && fabs(cfg.stage2_omega - 1) < eps) ? 1 : 0;
         const TA w = (TA)cfg.stage2_w, om = (TA)cfg.stage2_omega;
         for (size_t c = 0; c + 1 < M.seg.size(); ++c) {
             const int r0 = M.seg[c], r1 = M.seg[c + 1];
             if (r1 <= r0) continue;
-            if constexpr (std::is_same<TX, double>::value) {
-                launch_stage2<double>(M, M.a64.get(), r0, r1, r, z, w, om, plain, s);
-            } else {
-                launch_stage2<float>(M, M.a32.get(), r0, r1, r, z, w, om, plain, s);
-            }
+            if constexpr (std::is_same<TX, double>::value)
+                launch_stage2<double, TXV>(M, M.a64.get(), r0, r1, r, z, vtp, w, om, plain, s);
+            else
+                launch_stage2<float, TXV>(M, M.a32.get(), r0, r1, r, z, vtp, w, om, plain, s);
             JX_LAUNCH_CHECK();
         }
     }
-    template <typename TV>
-    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const double *r, double *z, TA w, TA om,
-                       int plain, cudaStream_t s) {
+    // FP64 interface (C ABI / tests): the mixed path converts in and out.
+    void stage2_sweep(const double *r, double *z, cudaStream_t s) override {
+        if constexpr (std::is_same<TX, double>::value) {
+            sweep_typed<double>(r, z, vt.get(), s);
+        } else {
+            const long long n = (long long)nb * bs;
+            if (!n) return;
+            fk::convert<double, float><<<div_up(n, kThreads), kThreads, 0, s>>>(n, r, r32.get());
+            JX_LAUNCH_CHECK();
+            fk::convert<double, float><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z, z32.get());
+            JX_LAUNCH_CHECK();
+            sweep_typed<float>(r32.get(), z32.get(), vt32.get(), s);
+            fk::convert<float, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z32.get(), z);
+            JX_LAUNCH_CHECK();
+        }
+    }
+    template <typename TV, typename TXV>
+    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp, TA w,
+                       TA om, int plain, cudaStream_t s) {
         if (M.sell) {
             const int grid = div_up(r1 - r0, kThreads);
             if (bs == 2)
-                fk::hgs_sell<2, TV, TA><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a, M.rows.get(), r,
-                                                                  z, vt.get(), w, om, plain);
+                fk::hgs_sell<2, TV, TA, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                                                                       M.rows.get(), r, z, vtp, w, om, plain);
             else
-                fk::hgs_sell<3, TV, TA><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a, M.rows.get(), r,
-                                                                  z, vt.get(), w, om, plain);
+                fk::hgs_sell<3, TV, TA, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                                                                       M.rows.get(), r, z, vtp, w, om, plain);
         } else {
-            launch_hgs_csr<TV>(opt.stage2_lanes, M, a, r0, r1, r, z, w, om, plain, s);
+            launch_hgs_csr<TV, TXV>(opt.stage2_lanes, M, a, r0, r1, r, z, vtp, w, om, plain, s);
         }
     }
 
@@ -546,7 +565,14 @@ struct FastCpr final : FastCprBase {
 
     void apply_direct(const double *r, double *z, cudaStream_t s) {
         FastLevel<TX> &L0 = *lv[0];
-        fk::restrict_p<TX><<<div_up(nb, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get());
+        constexpr bool fp64 = std::is_same<TX, double>::value;
+        const long long n = (long long)nb * bs;
+        if (fp64) {
+            fk::restrict_p<TX><<<div_up(nb, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get());
+        } else {
+            fk::restrict_cvt<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get(),
+                                                                        r32.get());
+        }
         JX_LAUNCH_CHECK();
         vcycle_tx(L0.f.get(), L0.u.get(), s);
         for (int it = 1; it < cfg.stage1_maxit; ++it) {
@@ -556,11 +582,22 @@ struct FastCpr final : FastCprBase {
             add_kernel<TX><<<div_up(L0.n, kThreads), kThreads, 0, s>>>(L0.n, L0.u.get(), L0.c.get());
             JX_LAUNCH_CHECK();
         }
-        fk::prolong_p<TX><<<div_up((long long)nb * bs, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index,
-                                                                                   L0.u.get(), z);
+        const bool st2_on = cfg.stage2_solver_type == 2 && cfg.stage2_maxit > 0;
+        if (fp64 || !st2_on) {
+            fk::prolong_p<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index,
+                                                                              L0.u.get(), z);
+            JX_LAUNCH_CHECK();
+            if (st2_on)
+                for (int it = 0; it < cfg.stage2_maxit; ++it) sweep_typed<double>(r, z, vt.get(), s);
+            return;
+        }
+        // mixed path: stage 2 on FP32 copies of r and z, result converted to FP64
+        fk::prolong_p<TX, float><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, L0.u.get(),
+                                                                         z32.get());
         JX_LAUNCH_CHECK();
-        if (cfg.stage2_solver_type == 2)
-            for (int it = 0; it < cfg.stage2_maxit; ++it) stage2_sweep(r, z, s);
+        for (int it = 0; it < cfg.stage2_maxit; ++it) sweep_typed<float>(r32.get(), z32.get(), vt32.get(), s);
+        fk::convert<float, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z32.get(), z);
+        JX_LAUNCH_CHECK();
     }
 
     void vcycle(const double *fp, double *up, cudaStream_t s) override {
@@ -571,6 +608,25 @@ struct FastCpr final : FastCprBase {
         vcycle_tx(L0.f.get(), L0.u.get(), s);
         fk::convert<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, L0.u.get(), up);
         JX_LAUNCH_CHECK();
+    }
+
+    double apply_bytes() const override {
+        auto vb = [](int kind) { return kind == VAL_F64 ? 8.0 : (kind == VAL_F32 ? 4.0 : 2.0); };
+        const double xb = sizeof(TX);
+        double total = 0.0;
+        for (size_t l = 0; l + 1 < lv.size(); ++l) {
+            const FastLevel<TX> &L = *lv[l];
+            // matrix passes per V-cycle incl. the residual: GS 2 x 1.5 + 2 x 2.5 sweeps -> 6, l1-Jacobi 7 + 1,
+            // Chebyshev 2 + 3 + 1
+            const double passes = L.smoother == FS_L1_JACOBI ? 8.0 : 6.0;
+            total += passes * ((double)L.A.nnz * (vb(L.A.kind) + 4.0) + 3.0 * L.n * xb);
+            total += (double)L.P.nnz * (vb(L.P.kind) + 4.0) + (double)L.R.nnz * (vb(L.R.kind) + 4.0) +
+                     2.0 * (L.P.n + L.P.m) * xb;
+        }
+        total += (double)nc * nc * 8.0;
+        const double bsz = bs * bs;
+        total += cfg.stage2_maxit * ((double)st2.nnz * (bsz * vb(st2.kind) + 4.0) + 4.0 * nb * bs * xb);
+        return total;
     }
 
     double vcycle_factor(int cycles, cudaStream_t s) override {
@@ -677,6 +733,12 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
     // stage 2: block rows in the level-0 colour order
     AmgLevel &H0 = *H.levels[0];
     F->vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+    if (!fp64) {
+        const size_t nv = (size_t)(A.nb > 0 ? A.nb : 1) * A.bs;
+        F->r32.alloc(nv);
+        F->z32.alloc(nv);
+        F->vt32.alloc(nv);
+    }
     if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
         const int kind = fp64 ? VAL_F64 : VAL_F32;

@@ -225,12 +225,23 @@ __global__ void restrict_p(int nb, int bs, int p, const double *__restrict__ r, 
     if (i < nb) rp[i] = (TX)r[(long long)i * bs + p];
 }
 
-template <typename TX>
-__global__ void prolong_p(int nb, int bs, int p, const TX *__restrict__ up, double *__restrict__ z) {
+template <typename TX, typename TZ>
+__global__ void prolong_p(int nb, int bs, int p, const TX *__restrict__ up, TZ *__restrict__ z) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nb * bs) return;
     const int i = (int)(t / bs), k = (int)(t % bs);
-    z[t] = k == p ? (double)up[i] : 0.0;
+    z[t] = k == p ? (TZ)up[i] : (TZ)0;
+}
+
+// rp = r[p-th component] and r32 = r converted (mixed path: stage 2 works in FP32)
+template <typename TX>
+__global__ void restrict_cvt(int nb, int bs, int p, const double *__restrict__ r, TX *__restrict__ rp,
+                             float *__restrict__ r32) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * bs) return;
+    const double v = r[t];
+    r32[t] = (float)v;
+    if ((int)(t % bs) == p) rp[t / bs] = (TX)v;
 }
 
 // u = Ainv f (FP64 inverse of the coarsest operator), one warp per row.
@@ -295,10 +306,10 @@ __device__ __forceinline__ void block_solve(const TA D[BS * BS], const TA rhs[BS
 // x_i <- (1 - w omega) x_i + w D_i^-1 (omega b_i - sum_{j != i} A_ij (x_j - (1 - omega) vt_j))
 // (jxf_ParBSRHGSRelax's update with res = b, res0 = -sum A x, res2 = sum A vt);
 // plain (w = omega = 1): x_i <- D_i^-1 (b_i - sum A_ij x_j).  vt = x at sweep start.
-template <int BS, int V, typename TV, typename TA>
+template <int BS, int V, typename TV, typename TA, typename TXV>
 __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
-                          const int *__restrict__ ja, const TV *__restrict__ a, const double *__restrict__ b,
-                          double *x, const double *__restrict__ vt, TA w, TA omega, int plain) {
+                          const int *__restrict__ ja, const TV *__restrict__ a, const TXV *__restrict__ b,
+                          TXV *x, const TXV *__restrict__ vt, TA w, TA omega, int plain) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int t = r0 + (int)(gt / V);
     const int lane = (int)(gt % V);
@@ -335,17 +346,17 @@ __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const in
 #pragma unroll
     for (int q = 0; q < BS; ++q) {
         const long long o = (long long)i * BS + q;
-        x[o] = plain ? (double)out[q] : (double)(prod * (TA)vt[o] + w * out[q]);
+        x[o] = plain ? (TXV)out[q] : (TXV)(prod * (TA)vt[o] + w * out[q]);
     }
 }
 
 // Stage 2 on a sliced-ELL block copy (one thread per block row, slot 0 = the
 // diagonal block, padding blocks are zero): same update as hgs_color.
-template <int BS, typename TV, typename TA>
+template <int BS, typename TV, typename TA, typename TXV>
 __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long *__restrict__ sp,
                                                 const int *__restrict__ col, const TV *__restrict__ a,
-                                                const int *__restrict__ rows, const double *__restrict__ b,
-                                                double *x, const double *__restrict__ vt, TA w, TA omega,
+                                                const int *__restrict__ rows, const TXV *__restrict__ b,
+                                                TXV *x, const TXV *__restrict__ vt, TA w, TA omega,
                                                 int plain) {
     const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= r1) return;
@@ -403,7 +414,7 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
     const TA prod = (TA)1 - w * omega;
 #pragma unroll
     for (int q = 0; q < BS; ++q)
-        x[(long long)i * BS + q] = plain ? (double)out[q] : (double)(prod * xv[q] + w * out[q]);
+        x[(long long)i * BS + q] = plain ? (TXV)out[q] : (TXV)(prod * xv[q] + w * out[q]);
 }
 
 // ---- sliced-ELL fill ----------------------------------------------------------

@@ -282,7 +282,29 @@ double learned_predict_level(LearnedPlan &plan, int level, const CsrView<double>
     }
     float y[kMlpOut];
     mlp_forward_host(w.data(), f.data(), y);
-    const double th = mlp_theta(y[0]), lo = mlp_lower(y[1]), hi = mlp_upper(y[2]);
+    // The network is trained on a grid of settings; predictions are snapped to
+    // the nearest trained value so that no untrained combination is used.
+    const double th_raw = mlp_theta(y[0]), lo_raw = mlp_lower(y[1]), hi_raw = mlp_upper(y[2]);
+    static const double kTheta0[] = {0.25, 0.5}, kThetaC[] = {0.25, 0.5, 0.7};
+    static const double kLo[] = {0.1, 0.3, 0.5}, kHi[] = {1.2, 1.1, 1.2};
+    double th = 0.25, best = 1e30;
+    const double *tg = level == 0 ? kTheta0 : kThetaC;
+    const int ng = level == 0 ? 2 : 3;
+    for (int q = 0; q < ng; ++q)
+        if (fabs(tg[q] - th_raw) < best) {
+            best = fabs(tg[q] - th_raw);
+            th = tg[q];
+        }
+    double lo = 0.3, hi = 1.1;
+    best = 1e30;
+    for (int q = 0; q < 3; ++q) {
+        const double d = fabs(kLo[q] - lo_raw) / 0.4 + fabs(kHi[q] - hi_raw) / 0.1;
+        if (d < best) {
+            best = d;
+            lo = kLo[q];
+            hi = kHi[q];
+        }
+    }
     if ((int)plan.theta.size() <= level) {
         plan.theta.resize(level + 1, default_theta);
         plan.lower.resize(level + 1, 0.3);

@@ -30,15 +30,20 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     amg.prm.strong_threshold = prm.strong_threshold;
     amg.prm.theta_for_level = nullptr;
     fast.reset();
+    fast_alt.reset();
     learned_used = 0;
+    factor_fast = factor_plain = 0.0;
     plan = LearnedPlan();
+    const double th0 = prm.strong_threshold;
+    const double thc = (fast_path && prm.strong_threshold_coarse >= 0.0) ? prm.strong_threshold_coarse : th0;
     if (fast_path && (prm.fast_smoother == 2 || prm.record_features)) {
         plan.active = prm.fast_smoother == 2;
         plan.record = true;
-        const double th = prm.strong_threshold;
-        amg.prm.theta_for_level = [this, th, s](int level, const CsrView<double> &Al) {
-            return learned_predict_level(plan, level, Al, th, s);
+        amg.prm.theta_for_level = [this, th0, thc, s](int level, const CsrView<double> &Al) {
+            return learned_predict_level(plan, level, Al, level == 0 ? th0 : thc, s);
         };
+    } else if (thc != th0) {
+        amg.prm.theta_for_level = [th0, thc](int level, const CsrView<double> &) { return level == 0 ? th0 : thc; };
     }
     DeviceCsr Ap;
     bsr_pressure_csr(A, prm.pressure_index, Ap, s);
@@ -69,16 +74,11 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         if (plan.active) {
             learned_used = 1;
             if (prm.learned_fallback) {
-                // the plain smoother settings stay whenever the learned ones converge worse
+                // plain smoother settings on the same hierarchy; Solver::setup keeps
+                // whichever preconditioner reduces the GMRES residual faster
                 FastOptions plain = opt;
                 plain.smoother = 0;
-                std::unique_ptr<FastCprBase> alt(make_fast_cpr(amg, A, cfg, plain, s));
-                factor_fast = fast->vcycle_factor(6, s);
-                factor_plain = alt->vcycle_factor(6, s);
-                if (!(factor_fast <= factor_plain * 1.02)) {
-                    fast = std::move(alt);
-                    learned_used = 0;
-                }
+                fast_alt.reset(make_fast_cpr(amg, A, cfg, plain, s));
             }
         }
     }
@@ -181,6 +181,87 @@ __global__ void sum_partials_kernel(int np, const double *__restrict__ partials,
     }
 }
 
+// ---------------------------------------------------------------------------
+// classical Gram-Schmidt (one pass): h = V^T w in one sweep over the basis,
+// then w -= V h with ||w||^2 in a second sweep.  V is an array of m device
+// pointers (m <= kCgsMax).
+// ---------------------------------------------------------------------------
+static constexpr int kCgsMax = 32;
+static constexpr int kCgsThreads = 256;
+
+__global__ void __launch_bounds__(kCgsThreads) cgs_dots_kernel(long long n, int m, const double *const *__restrict__ V,
+                                                               const double *__restrict__ w,
+                                                               double *__restrict__ partials) {
+    double acc[kCgsMax];
+#pragma unroll
+    for (int k = 0; k < kCgsMax; ++k) acc[k] = 0.0;
+    for (long long i = (long long)blockIdx.x * kCgsThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kCgsThreads) {
+        const double wi = w[i];
+#pragma unroll
+        for (int k = 0; k < kCgsMax; ++k)
+            if (k < m) acc[k] += V[k][i] * wi;
+    }
+    __shared__ double sh[kCgsThreads / 32][kCgsMax];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kCgsMax; ++k) {
+        if (k >= m) break;
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < m) {
+        double v = 0.0;
+        for (int q = 0; q < kCgsThreads / 32; ++q) v += sh[q][threadIdx.x];
+        partials[(long long)blockIdx.x * kCgsMax + threadIdx.x] = v;
+    }
+}
+
+// out[k] = sum over blocks of partials[b][k], k < m (one warp per k)
+__global__ void cgs_sum_kernel(int nblocks, int m, const double *__restrict__ partials, double *__restrict__ out) {
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= m) return;
+    double v = 0.0;
+    for (int b = lane; b < nblocks; b += 32) v += partials[(long long)b * kCgsMax + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) out[k] = v;
+}
+
+// w -= sum_k h_k V_k, partial ||w||^2 per block
+__global__ void __launch_bounds__(kCgsThreads) cgs_update_kernel(long long n, int m,
+                                                                 const double *const *__restrict__ V,
+                                                                 const double *__restrict__ h, double *__restrict__ w,
+                                                                 double *__restrict__ partials) {
+    __shared__ double hs[kCgsMax];
+    if (threadIdx.x < kCgsMax) hs[threadIdx.x] = threadIdx.x < m ? h[threadIdx.x] : 0.0;
+    __syncthreads();
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * kCgsThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kCgsThreads) {
+        double s = w[i];
+#pragma unroll
+        for (int k = 0; k < kCgsMax; ++k)
+            if (k < m) s -= hs[k] * V[k][i];
+        w[i] = s;
+        acc += s * s;
+    }
+    __shared__ double ws[kCgsThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r = threadIdx.x < kCgsThreads / 32 ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        if (threadIdx.x == 0) partials[blockIdx.x] = r;
+    }
+}
+
 void Gmres::setup(int n_, cudaStream_t s) {
     n = n_;
     p.clear();
@@ -190,9 +271,14 @@ void Gmres::setup(int n_, cudaStream_t s) {
         for (int i = 0; i < prm.k_dim; ++i) zf.emplace_back((size_t)(n > 0 ? n : 1));
     r.alloc(n > 0 ? n : 1);
     w.alloc(n > 0 ? n : 1);
-    partials.alloc(reduce_partials() + 8);
+    cgs_blocks = std::max(1, std::min(4 * sm_count(), div_up(n > 0 ? n : 1, kCgsThreads)));
+    partials.alloc(std::max<size_t>(reduce_partials() + 8, (size_t)cgs_blocks * kCgsMax));
     scal.alloc(prm.k_dim + 8);
-    (void)s;
+    std::vector<const double *> ptrs;
+    for (auto &v : p) ptrs.push_back(v.get());
+    vptrs.alloc(ptrs.size());
+    vptrs.upload(reinterpret_cast<const double **>(ptrs.data()), ptrs.size(), s);
+    JX_CUDA(cudaStreamSynchronize(s));
 }
 
 namespace {
@@ -285,6 +371,18 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
             JX_CUDA(cudaMemsetAsync(zi, 0, sizeof(double) * nl, s));
             precond(p[i - 1].get(), zi);
             spmv(1.0, zi, 0.0, p[i].get());
+            if (prm.orthog == 1 && i <= kCgsMax) {
+                // classical Gram-Schmidt: h = V_i^T w, w -= V_i h, ||w||^2 -> scal[i]
+                const double *const *V = vptrs.get();
+                cgs_dots_kernel<<<cgs_blocks, kCgsThreads, 0, s>>>(nl, i, V, p[i].get(), ops.partials);
+                JX_LAUNCH_CHECK();
+                cgs_sum_kernel<<<1, 32 * kCgsMax, 0, s>>>(cgs_blocks, i, ops.partials, ops.scal);
+                JX_LAUNCH_CHECK();
+                cgs_update_kernel<<<cgs_blocks, kCgsThreads, 0, s>>>(nl, i, V, ops.scal, p[i].get(), ops.partials);
+                JX_LAUNCH_CHECK();
+                sum_partials_kernel<<<1, 512, 0, s>>>(cgs_blocks, ops.partials, ops.scal + i);
+                JX_LAUNCH_CHECK();
+            } else
             // modified Gram-Schmidt, fused passes
             for (int j = 0; j <= i; ++j) {
                 const double *pprev = j > 0 ? p[j - 1].get() : nullptr;
@@ -414,8 +512,53 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     gmres.setup(nb * bs, s);
     b.alloc((size_t)(nb > 0 ? nb : 1) * bs);
     x.alloc((size_t)(nb > 0 ? nb : 1) * bs);
+    if (cpr.fast_alt) learned_probe(s);
     JX_CUDA(cudaStreamSynchronize(s));
     setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Learned settings against the plain smoothers: a few GMRES iterations (tol 0)
+// on A x = A 1 with each preconditioner.  GMRES's own residual reduction per
+// iteration, weighted by the bytes one iteration moves (the preconditioner's
+// modelled traffic plus the SpMV and orthogonalisation common to both), is
+// compared: the learned settings stay unless their residual reduction per
+// byte is worse.
+void Solver::learned_probe(cudaStream_t s) {
+    const int m = 8;
+    const long long n = (long long)A.nb * A.bs;
+    SolverParams saved = gmres.prm;
+    gmres.prm.max_iter = m;
+    gmres.prm.min_iter = 0;
+    gmres.prm.tol = 0.0;
+    gmres.prm.a_tol = 0.0;
+    gmres.prm.is_check_restarted = 0;
+    fill_dev(n, 1.0, x.get(), s);
+    bsr_spmv<double, double>(A.view(), 1.0, x.get(), 0.0, b.get(), kerr.get(), s, false);
+    auto probe = [&]() {
+        JX_CUDA(cudaMemsetAsync(x.get(), 0, sizeof(double) * n, s));
+        GmresResult r = gmres.solve(A.view(), &cpr, b.get(), x.get(), s);
+        return r.rel_residual;
+    };
+    const double bl = cpr.fast->apply_bytes();
+    const double rl = probe();
+    std::swap(cpr.fast, cpr.fast_alt);
+    const double bp = cpr.fast->apply_bytes();
+    const double rp = probe();
+    cpr.factor_fast = pow(rl, 1.0 / m);
+    cpr.factor_plain = pow(rp, 1.0 / m);
+    // common per-iteration traffic: BSR SpMV (FP64) and about k/2 orthogonalisation passes
+    const double common = (double)A.nnzb * (A.bs * A.bs * 8.0 + 4.0) + 2.0 * n * 8.0 + 15.0 * 4.0 * n * 8.0;
+    const double el = rl > 0.0 ? -log(rl) / (bl + common) : 1e300;
+    const double ep = rp > 0.0 ? -log(rp) / (bp + common) : 1e300;
+    cpr.probe_bytes[0] = bl + common;
+    cpr.probe_bytes[1] = bp + common;
+    if (el >= ep) {
+        std::swap(cpr.fast, cpr.fast_alt);  // learned settings stay
+    } else {
+        cpr.learned_used = 0;
+    }
+    cpr.fast_alt.reset();
+    gmres.prm = saved;
 }
 
 GmresResult Solver::solve(const double *b_in, double *x_io, int device) {

@@ -40,6 +40,7 @@ struct SolverParams {
     int consistent_rhs = 0;
     // AMG strength threshold (jxf_cpr.c:331 sets 0.25)
     double strong_threshold = 0.25;
+    double strong_threshold_coarse = -1.0;  // levels >= 1 (fast path); < 0: strong_threshold
     // device execution choices
     int smoother_order = ORDER_EXACT;  // 0 exact order (bit-identical), 1 throughput / mixed path
     int coarse_exact = 1;
@@ -52,6 +53,7 @@ struct SolverParams {
                              // 2 as 1 with learned thresholds and intervals; 3 Chebyshev-3 on every level
     int autotune = 1;        // fast path: time the operator layouts at setup and keep the fastest
     int graphs = 1;          // fast path: each CPR application replays one captured CUDA graph
+    int orthog = 0;          // 0 modified Gram-Schmidt (the reference's), 1 classical Gram-Schmidt (one pass)
     int flexible = 0;        // 1: flexible GMRES (stores M^-1 v_j; for inexact / low-precision preconditioners)
     double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
     double cheb_upper = 1.1;
@@ -86,7 +88,9 @@ struct CprPrecond {
     BsrView<double> A;  // decoupled system matrix (owned by the solver)
     Amg amg;
     std::unique_ptr<FastCprBase> fast;  // smoother_order 1: throughput / mixed-precision preconditioner
-    double factor_fast = 0.0, factor_plain = 0.0;  // learned mode: measured V-cycle factors
+    std::unique_ptr<FastCprBase> fast_alt;  // learned mode: plain-smoother variant until the probe decides
+    double factor_fast = 0.0, factor_plain = 0.0;  // learned mode: GMRES residual reduction per iteration
+    double probe_bytes[2] = {0, 0};                 // modelled bytes per GMRES iteration (learned, plain)
     int learned_used = 0;
     LearnedPlan plan;  // per-level features and learned settings of the last setup
     DevBuf<double> rp, xp, vt;
@@ -117,6 +121,8 @@ struct Gmres {
     std::vector<DevBuf<double>> p;
     std::vector<DevBuf<double>> zf;       // flexible GMRES: z_j = M^-1 p_j
     DevBuf<double> r, w, partials, scal;  // scal: device scalars (dots)
+    DevBuf<const double *> vptrs;         // device array of the basis pointers (classical Gram-Schmidt)
+    int cgs_blocks = 1;
     int *kerr = nullptr;
     void setup(int n_, cudaStream_t s);
     GmresResult solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s);
@@ -140,6 +146,7 @@ struct Solver {
     void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);
     // b, x host or device; x holds the initial guess on entry.
     GmresResult solve(const double *b_in, double *x_io, int device);
+    void learned_probe(cudaStream_t s);
 };
 
 }  // namespace jxcpr

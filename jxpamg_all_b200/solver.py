@@ -107,6 +107,13 @@ class CprGmres:
     def num_levels(self):
         return int(self._so.jxcpr_solver_num_levels(self.h))
 
+    def level_sizes(self, lev, what=0):
+        """(rows, cols, nnz) of level lev's operator (what 0), P (1) or R (2)."""
+        sz = np.zeros(3, np.int32)
+        if self._so.jxcpr_solver_level_sizes(self.h, lev, what, _ptr(sz)) < 0:
+            return None
+        return tuple(int(v) for v in sz)
+
     def level_matrix(self, lev, what=0):
         sz = np.zeros(3, np.int32)
         if self._so.jxcpr_solver_level_sizes(self.h, lev, what, _ptr(sz)) < 0:
@@ -154,9 +161,10 @@ class CprGmres:
         return None if n < 0 else f[:n].copy()
 
     def learned_status(self):
-        o = np.zeros(3)
+        o = np.zeros(5)
         _lib.check(self._so.jxcpr_solver_learned_status(self.h, _ptr(o)))
-        return dict(learned_used=bool(o[0]), factor_learned=float(o[1]), factor_plain=float(o[2]))
+        return dict(learned_used=bool(o[0]), factor_learned=float(o[1]), factor_plain=float(o[2]),
+                    bytes_learned=float(o[3]), bytes_plain=float(o[4]))
 
     def close(self):
         if getattr(self, "h", None):
