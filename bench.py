@@ -1,16 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark: CPR-GMRES time to FP64 relative residual 1e-6 on one B200.
+"""Benchmark: CPR-GMRES time to FP64 relative residual 1e-6 on one B200,
+mixed precision + learned settings against the plain FP64 GPU path.
 
 Workload (the configuration the headline metric is quoted on): the 1.12M-cell
 channelised two-phase reservoir Jacobian -- 60x220x85 grid, 2x2 BSR blocks,
 7.78M stored blocks, seed 1 -- decoupled by ABF and solved by CPR-GMRES(30)
-(AMG V(1,1) on pressure + 3 block-Gauss-Seidel sweeps) in FP64.  The data are
-the seeded synthetic system of jxpamg_all_b200.synth (the reference's SPE10
-inputs are not available).
+(AMG V(1,1) on pressure + 3 block-Gauss-Seidel sweeps).  The data are the
+seeded synthetic system of jxpamg_all_b200.synth (the reference's SPE10 inputs
+are not available).
 
-One step = one solve from x0 = 0 to rel-res <= 1e-6.
-  value : device-resident solve (matrix, hierarchy and b in HBM), seconds.
-  e2e   : the same solve through the public C ABI from pinned host buffers,
+One step = one solve from x0 = 0 to FP64 rel-res <= 1e-6 (GMRES confirms the
+true residual b - A x in FP64 before it reports convergence).
+  value : device-resident solve with the measured path (FP32 preconditioner,
+          learned per-level strength thresholds and Chebyshev intervals,
+          flexible FP64 GMRES), seconds; config.plain_fp64_s is the same
+          measurement for the plain FP64 path and config.speedup_vs_plain_fp64
+          their ratio.
+  e2e   : the measured path through the public C ABI from pinned host buffers,
           timed per step from the host->device upload of the matrix and b,
           through decoupling, CPR setup and solve, to the device->host read
           of x (the whole call a user makes).
@@ -19,8 +25,8 @@ explicit flush is needed between steps.
 
 --impl reference times the reference library (compiled from its own sources
 into oracle/_ref) on the host cores, on a bounded sample: decoupling + CPR
-setup + 2 GMRES iterations, scaled to the reference's iteration count on this
-system.
+setup + GMRES runs of 2 and 4 iterations, scaled to the reference's iteration
+count on this system.
 
 Multi-GPU (torchrun): replicas -- every rank solves its own copy of the
 system; value is the max over ranks of the mean solve time (weak scaling).
@@ -53,7 +59,11 @@ WORKLOADS = {
     "c0": "config-0 system: 20x40x10 two-phase Jacobian, 8,000 cells, 2x2 BSR, 53,200 blocks, seed 0",
     "slab45": "60x220x45 slab of the channelised geometry, 594,000 cells, 2x2 BSR, seed 5 (profiling case)",
 }
-SOLVER_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0)
+# plain FP64 GPU path (the comparison): the reference's method in the throughput ordering
+PLAIN_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0,
+                  precision=0, fast_smoother=0)
+# measured path: FP32 preconditioner + learned settings, flexible FP64 GMRES
+SOLVER_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=2, flexible=1)
 
 
 def solver_opts(args):
@@ -221,56 +231,79 @@ def run_ours(args):
     d_ia, d_ja, d_a, d_b = dev(s.ia), dev(s.ja), dev(s.a), dev(s.b)
     d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
 
-    G = CprGmres(**solver_opts(args))
-    G.set_stream(stream.cuda_stream)
-    G.setup(d_ia.data_ptr(), d_ja.data_ptr(), d_a.data_ptr(), s.block_size, nb=s.num_block_rows, nnzb=s.nnzb,
-            device=True)
-    setup_stats = G.stats()
+    def make(opts):
+        G = CprGmres(**opts)
+        G.set_stream(stream.cuda_stream)
+        G.setup(d_ia.data_ptr(), d_ja.data_ptr(), d_a.data_ptr(), s.block_size, nb=s.num_block_rows, nnzb=s.nnzb,
+                device=True)
+        return G
 
-    def solve_device():
+    def solve_device(G):
         d_x.zero_()
         return G.solve(d_b.data_ptr(), d_x.data_ptr(), device=True)
 
-    for _ in range(args.warmup):
-        _, it, rel, conv = solve_device()
-    torch.cuda.synchronize()
+    measured_opts = solver_opts(args)
     if args.profile_solve:
         # one solve inside a profiler range (ncu --profile-from-start off), nothing else
+        G = make(PLAIN_OPTS if args.path == "plain" else measured_opts)
+        for _ in range(args.warmup):
+            solve_device(G)
+        torch.cuda.synchronize()
         torch.cuda.profiler.start()
-        _, it, rel, conv = solve_device()
+        _, it, rel, conv = solve_device(G)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-        print(json.dumps({"profile_solve": args.config, "iterations": it, "rel": rel, "converged": conv}))
+        print(json.dumps({"profile_solve": args.config, "path": args.path, "iterations": it, "rel": rel,
+                          "converged": conv}))
         G.close()
         return 0 if conv else 1
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = so.jxcpr_launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    iters = []
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            _, it, rel, conv = solve_device()
-            iters.append(it)
-            if not conv:
-                raise RuntimeError(f"solve did not converge (rel {rel})")
-        e1.record(stream)
-        torch.cuda.synchronize()
-    launches = so.jxcpr_launch_count() - launches0
-    clocks = clk.summary()
-    if ws > 1:
-        dist.barrier()
-    elapsed = e0.elapsed_time(e1) / 1e3
-    t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed = float(t.item())
-    per_solve = elapsed / args.steps
 
-    # GMRES reports convergence only after recomputing the true residual b - A x
-    rel_true = rel
+    def timed(G, clk_name):
+        """Device-resident solves: W warm-up, K timed between barriers (CUDA events, max over ranks)."""
+        for _ in range(args.warmup):
+            solve_device(G)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = so.jxcpr_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iters, rels = [], []
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                _, it, rel, conv = solve_device(G)
+                iters.append(it)
+                rels.append(rel)
+                if not conv:
+                    raise RuntimeError(f"{clk_name}: solve did not converge (rel {rel})")
+            e1.record(stream)
+            torch.cuda.synchronize()
+        launches = so.jxcpr_launch_count() - l0
+        t = torch.tensor([e0.elapsed_time(e1) / 1e3], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / args.steps, int(np.median(iters)), float(rels[-1]), launches, clk.summary()
+
+    # ---- plain FP64 path (the comparison) ----------------------------------------
+    P = make(PLAIN_OPTS)
+    plain_setup = P.stats()
+    plain_t, plain_it, plain_rel, _, clk_p = timed(P, "plain FP64")
+    x_plain = d_x.cpu().numpy().copy()
+    roof_plain = roofline_stage2(P, s, stream, 8)
+    P.close()
+
+    # ---- measured path: mixed precision + learned settings ------------------------
+    G = make(measured_opts)
+    setup_stats = G.stats()
+    learned = G.learned_status()
+    per_solve, it_m, rel_m, launches, clocks = timed(G, "mixed+learned")
+    x_mixed = d_x.cpu().numpy().copy()
+    err_vs_fp64 = float(np.linalg.norm(x_mixed - x_plain) / np.linalg.norm(x_plain))
+    roof = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) == 0 else 4)
+    G.close()
+    if clk_p.get("reasons"):
+        clocks["reasons"] = sorted(set(clocks.get("reasons", [])) | set(clk_p["reasons"]))
 
     # ---- e2e: public C ABI with pinned host buffers, setup included --------------
     pin = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()  # noqa: E731
@@ -280,7 +313,7 @@ def run_ours(args):
     d2h = h_x.numel() * 8
 
     def e2e_step():
-        E = CprGmres(**solver_opts(args))
+        E = CprGmres(**measured_opts)
         E.set_stream(stream.cuda_stream)
         E.nb, E.bs = s.num_block_rows, s.block_size
         lib.check(E._so.jxcpr_solver_setup(E.h, s.num_block_rows, s.block_size, s.nnzb,
@@ -309,9 +342,6 @@ def run_ours(args):
     if ws > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
 
-    # ---- roofline of the dominant kernel -------------------------------------------
-    roof = roofline_stage2(G, s, stream)
-
     line = None
     if rank == 0:
         cpu = None
@@ -321,33 +351,45 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": per_solve, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.config], "method": "plain FP64 CPR-GMRES(30), ABF decoupling, "
-                       "AMG V(1,1) (HMIS, ext+i) + 3 block-GS stage-2 sweeps",
-                       "smoother": "multicolour Gauss-Seidel / l1-Jacobi (throughput mode)",
-                       "iterations": int(np.median(iters)), "final_true_rel_res": rel_true,
-                       "setup_s": setup_stats["setup_ms"] / 1e3, "amg_levels": setup_stats["levels"],
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.config],
+                       "method": "CPR-GMRES(30) to FP64 true rel-res 1e-6, ABF decoupling, AMG V(1,1) (HMIS, ext+i) "
+                                 "+ 3 block-GS stage-2 sweeps",
+                       "measured_path": "mixed+learned: FP32 preconditioner storage/arithmetic (AMG levels, transfers, "
+                                        "stage 2), FP64 flexible GMRES / SpMV / true residual / coarsest solve; learned "
+                                        "per-level strength thresholds and Chebyshev-3 intervals (" +
+                                        ("kept" if learned["learned_used"] else "rejected by the probe: plain smoothers")
+                                        + ")",
+                       "options": measured_opts,
+                       "iterations": it_m, "final_rel_res": rel_m,
+                       "plain_fp64_s": plain_t, "plain_fp64_iterations": plain_it, "plain_fp64_rel_res": plain_rel,
+                       "speedup_vs_plain_fp64": plain_t / per_solve,
+                       "x_rel_diff_vs_plain_fp64": err_vs_fp64,
+                       "learned": learned,
+                       "setup_s": setup_stats["setup_ms"] / 1e3, "plain_setup_s": plain_setup["setup_ms"] / 1e3,
+                       "amg_levels": setup_stats["levels"],
+                       "roofline_plain_fp64_stage2": roof_plain,
                        "l2_flush": "not needed: matrix + hierarchy + Krylov basis > 126 MB L2",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": float(e2e_t.item()), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
-                    "note": "public C ABI from pinned host memory: upload + decoupling + CPR setup + solve + x download"},
+                    "note": "public C ABI from pinned host memory, mixed+learned path: upload + decoupling + CPR setup "
+                            "(incl. the learned-settings probe) + solve + x download"},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    G.close()
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def roofline_stage2(G, s, stream):
-    """The dominant kernel of the solve is the stage-2 block Gauss-Seidel sweep
-    (one launch per colour class).  Achieved = algorithmic bytes of one sweep /
+def roofline_stage2(G, s, stream, value_bytes):
+    """Roofline of the stage-2 block Gauss-Seidel sweep (one launch per colour
+    class) in the path's own storage precision: algorithmic bytes of one sweep /
     mean sweep time (CUDA events on the solver's stream)."""
     import torch
 
@@ -361,27 +403,23 @@ def roofline_stage2(G, s, stream):
     peak = peaks.get("hbm_gbs")
     src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    n = s.n
-    dev = lambda arr: torch.from_numpy(np.ascontiguousarray(arr)).cuda()  # noqa: E731
-    r = dev(np.random.default_rng(0).standard_normal(n))
-    z = torch.zeros(n, dtype=torch.float64, device="cuda")
     reps = 20
-    for _ in range(3):
-        lib.check(so.jxcpr_solver_stage2_sweep(G.h, ctypes.c_void_p(r.data_ptr()), ctypes.c_void_p(z.data_ptr()), 1))
+    lib.check(so.jxcpr_solver_stage2_native(G.h, 3))
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(reps):
-        lib.check(so.jxcpr_solver_stage2_sweep(G.h, ctypes.c_void_p(r.data_ptr()), ctypes.c_void_p(z.data_ptr()), 1))
+    lib.check(so.jxcpr_solver_stage2_native(G.h, reps))
     e1.record(stream)
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3 / reps
-    bs, nb, nnzb = s.block_size, s.num_block_rows, s.nnzb
-    # values + column indices + row pointers, x/vt/b read once, x written once, start-of-sweep copy (read+write)
-    alg = nnzb * (bs * bs * 8 + 4) + (nb + 1) * 4 + n * 8 * 3 + n * 8 + n * 8 * 2
+    bs, nb, nnzb, n = s.block_size, s.num_block_rows, s.nnzb, s.n
+    xb = value_bytes  # the mixed path keeps the stage-2 vectors in FP32 too
+    # values + column indices + row pointers, b/x/vt read once, x written once, start-of-sweep copy (read+write)
+    alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * xb * 6
     achieved = alg / sec / 1e9
-    return {"bound": "hbm", "kernel": "stage-2 block hybrid Gauss-Seidel sweep (hgs_group_kernel, 2 colour launches + "
-            "start copy)", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+    return {"bound": "hbm", "kernel": f"stage-2 block hybrid Gauss-Seidel sweep (hgs_sell<{bs}>, "
+            f"{'FP64' if value_bytes == 8 else 'FP32'} values, one launch per colour class + start copy)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": src, "traffic": None, "algorithmic_bytes": int(alg), "sweep_ms": sec * 1e3}
 
 
@@ -395,6 +433,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override a solver option of the measured path (repeatable)")
+    ap.add_argument("--path", default="mixed", choices=["mixed", "plain"], help="path --profile-solve runs")
     ap.add_argument("--profile-solve", action="store_true",
                     help="set up, run --warmup solves, then one solve inside a profiler range, and exit")
     args = ap.parse_args()

@@ -146,6 +146,11 @@ JXCPR_API int jxcpr_solver_vcycle(jxcpr_solver *solver, const double *rp, double
  * relax_weight / omega from the stage2_* options). */
 JXCPR_API int jxcpr_solver_stage2_sweep(jxcpr_solver *solver, const double *b, double *x, int device);
 
+/* Queues `sweeps` stage-2 sweeps in the fast path's own storage precision (FP64, or FP32 in the mixed
+ * path) on internal vectors, asynchronously on the solver's stream (no reference counterpart): the
+ * kernel a roofline measurement times with events on that stream. */
+JXCPR_API int jxcpr_solver_stage2_native(jxcpr_solver *solver, int sweeps);
+
 /* ---- fast path (smoother_order 1) inspection: no reference counterpart ---------------------
  * level_info: smoother (1 multicolour GS, 2 l1-Jacobi, 3 Chebyshev-3; 0 exact path), storage
  * (0 FP64, 1 FP32, 2 BF16 + row scale), the strength threshold the level was coarsened with and

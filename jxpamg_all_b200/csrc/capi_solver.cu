@@ -320,6 +320,18 @@ int jxcpr_solver_stage2_sweep(jxcpr_solver *h, const double *b, double *x, int d
     });
 }
 
+int jxcpr_solver_stage2_native(jxcpr_solver *h, int sweeps) {
+    if (!h || sweeps < 0 || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    if (!h->s.cpr.fast) {
+        set_error("stage2_native needs the fast path (smoother_order 1)");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        h->s.cpr.fast->stage2_native(sweeps, h->s.stream);
+        return JXCPR_SUCCESS;
+    });
+}
+
 int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int device) {
     if (!h || !rp || !xp || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
     return guarded([&] {

@@ -106,6 +106,9 @@ struct FastCprBase {
     // Modelled bytes one application moves (operator and vector traffic of
     // every smoother pass, residual, transfer and stage-2 sweep).
     virtual double apply_bytes() const = 0;
+    // `sweeps` stage-2 sweeps in the preconditioner's own precision on internal
+    // vectors (no conversions), queued on s: the kernel the roofline times.
+    virtual void stage2_native(int sweeps, cudaStream_t s) = 0;
     // One line per tuned operator: "name rows mean_row layout time_us".
     std::vector<std::string> tune_log;
 };

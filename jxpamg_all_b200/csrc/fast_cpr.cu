@@ -610,6 +610,24 @@ struct FastCpr final : FastCprBase {
         JX_LAUNCH_CHECK();
     }
 
+    DevBuf<TX> nat_r, nat_z;
+    void stage2_native(int sweeps, cudaStream_t s) override {
+        const long long n = (long long)nb * bs;
+        if (!n) return;
+        if (!nat_r.get()) {
+            nat_r.alloc(n);
+            nat_z.alloc(n);
+            nat_r.zero(s);
+            nat_z.zero(s);
+        }
+        for (int k = 0; k < sweeps; ++k) {
+            if constexpr (std::is_same<TX, double>::value)
+                sweep_typed<double>(nat_r.get(), nat_z.get(), vt.get(), s);
+            else
+                sweep_typed<float>(nat_r.get(), nat_z.get(), vt32.get(), s);
+        }
+    }
+
     double apply_bytes() const override {
         auto vb = [](int kind) { return kind == VAL_F64 ? 8.0 : (kind == VAL_F32 ? 4.0 : 2.0); };
         const double xb = sizeof(TX);
