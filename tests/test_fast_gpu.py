@@ -1,0 +1,111 @@
+"""The throughput / mixed-precision path (smoother_order 1) on the GPU.
+
+Its orderings differ from the reference (multicolour Gauss-Seidel, l1-Jacobi or
+Chebyshev on dense levels, FP32/BF16 storage), so parity is checked through
+what the method guarantees: GMRES reaches the tolerance on the TRUE residual
+of the decoupled system (recomputed here on the CPU with the oracle), the
+hierarchy is the exact path's one for the default thresholds, and options that
+must not change results (CUDA-graph replay) do not.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from jxpamg_all_b200.solver import CprGmres
+from jxpamg_all_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(decouple=1, max_iter=400, smoother_order=1, coarse_exact=0)
+
+
+def true_rel(s, x, decouple=1):
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, decouple)
+    r = b - synth.bsr_matvec_np(s.ia, s.ja, a, s.block_size, x)
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+def solve(s, **opt):
+    G = CprGmres(**dict(BASE, **opt)).setup(s.ia, s.ja, s.a, s.block_size)
+    x, it, rel, conv = G.solve(s.b)
+    return G, x, it, rel, conv
+
+
+VARIANTS = [
+    dict(precision=0, fast_smoother=0),
+    dict(precision=0, fast_smoother=1),
+    dict(precision=0, fast_smoother=3),
+    dict(precision=1, fast_smoother=0, flexible=1),
+    dict(precision=1, fast_smoother=1, flexible=1),
+    dict(precision=2, fast_smoother=1, flexible=1),
+    dict(precision=1, fast_smoother=2, flexible=1),
+    dict(precision=2, fast_smoother=2, flexible=1),
+    dict(precision=0, fast_smoother=0, orthog=1),
+    dict(precision=1, fast_smoother=1, flexible=1, autotune=0, graphs=0),
+    dict(precision=0, fast_smoother=1, strong_threshold=0.5, strong_threshold_coarse=0.7),
+]
+
+
+@pytest.mark.parametrize("name", ["small", "c0", "tiny3", "slab_small"])
+@pytest.mark.parametrize("opt", VARIANTS, ids=lambda o: "-".join(f"{k}{v}" for k, v in o.items()))
+def test_variants_reach_true_residual(systems, name, opt):
+    s = systems(name) if name != "slab_small" else synth.reservoir_system(30, 110, 12, seed=21, phases=2,
+                                                                         channelised_layers=7)
+    G, x, it, rel, conv = solve(s, **opt)
+    assert conv, (it, rel)
+    assert true_rel(s, x) <= 1.05e-6
+    G.close()
+
+
+def test_graph_replay_is_identical(systems):
+    s = systems("c0")
+    _, x1, it1, _, _ = solve(s, precision=1, fast_smoother=1, flexible=1, graphs=1, autotune=0)
+    _, x2, it2, _, _ = solve(s, precision=1, fast_smoother=1, flexible=1, graphs=0, autotune=0)
+    assert it1 == it2 and np.array_equal(x1, x2)
+
+
+def test_mixed_solution_close_to_fp64(systems):
+    s = systems("c0")
+    _, x64, _, _, _ = solve(s, precision=0, fast_smoother=0)
+    for p in (1, 2):
+        _, xm, _, _, _ = solve(s, precision=p, fast_smoother=1, flexible=1)
+        assert np.linalg.norm(xm - x64) <= 1e-3 * np.linalg.norm(x64)
+
+
+def test_level_storage_and_smoothers(systems):
+    s = systems("c0")
+    G, *_ = solve(s, precision=2, fast_smoother=1, flexible=1, bf16_level=1)
+    L = G.num_levels()
+    for lev in range(L - 1):
+        info = G.level_info(lev)
+        assert info["storage"] == (1 if lev == 0 else 2)
+        assert info["smoother"] in (1, 3)
+        if info["smoother"] == 3:
+            lo, hi = info["interval"]
+            c0, c1, c2 = info["cheb"]
+            t = np.linspace(lo, hi, 101)
+            q = 1 - t * (c0 + c1 * t + c2 * t * t)  # error polynomial of one application
+            sg = (hi + lo) / (hi - lo)
+            assert np.max(np.abs(q)) <= 1.0 / (4 * sg ** 3 - 3 * sg) * (1 + 1e-9)
+    assert G.level_info(L - 1)["smoother"] == 0
+
+
+def test_default_threshold_hierarchy_matches_exact_path(systems):
+    """The fast path coarsens with the reference's rules: same hierarchy as the exact path."""
+    s = systems("small")
+    E = CprGmres(decouple=1).setup(s.ia, s.ja, s.a, s.block_size)
+    F, *_ = solve(s, precision=1, fast_smoother=1, flexible=1)
+    assert E.num_levels() == F.num_levels()
+    for lev in range(E.num_levels()):
+        for u, v in zip(E.level_matrix(lev)[:3], F.level_matrix(lev)[:3]):
+            assert np.array_equal(u, v)
+
+
+def test_stage2_native_and_autotune_report(systems):
+    from jxpamg_all_b200 import lib
+
+    s = systems("c0")
+    G, *_ = solve(s, precision=1, fast_smoother=1, flexible=1)
+    lib.check(lib.load().jxcpr_solver_stage2_native(G.h, 2))
+    rep = G.setup_report()
+    assert "tuned stage2" in rep and "tuned A0" in rep
