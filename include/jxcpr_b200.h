@@ -102,7 +102,9 @@ JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *
  * JXF_CPRSetParameter does, jxf_cpr.c:226-262):
  *   int : k_dim (30), max_iter (100), min_iter (0), is_check_restarted (1),
  *         pressure_index (0), stage1_maxit (1), stage2_maxit (3),
- *         stage1_solver_type (1 AMG; 0 none), stage2_solver_type (2 HGS),
+ *         stage1_solver_type (1 AMG; 0 none), stage2_solver_type (2 HGS; 5 block ILU(0)
+ *         correction z += BILU^-1 (r - A z) after CPR without sweeps; bilu_sweeps (3),
+ *         bilu_ir_iters (5), bilu_lower_iters (5), bilu_upper_iters (5)),
  *         decouple (0 none, 1 ABF, 5 True-IMPES), consistent_rhs (0: the
  *         reference's right-hand-side arithmetic, 1: solution-preserving),
  *         smoother_order (0 exact sequential order, 1 multicolour),
@@ -145,6 +147,15 @@ JXCPR_API int jxcpr_solver_vcycle(jxcpr_solver *solver, const double *rp, double
  * (jxf_ParBSRHGSRelax, jxfpamg-0220/csrc/amg/par_relax_bsr.c:193-573,
  * relax_weight / omega from the stage2_* options). */
 JXCPR_API int jxcpr_solver_stage2_sweep(jxcpr_solver *solver, const double *b, double *x, int device);
+
+/* Block ILU(0) stage 2 (stage2_solver_type 5): the factors jxf_BILUSetup builds with type 3
+ * (jxf_ILUSetupFGPBILU_v3, jxfpamg-0220/csrc/ilu/par_bilu_setup.c:4996) and one jxf_BILUSolve with
+ * tri-solve 14 (par_bilu_solve.c:360, 2893) on the decoupled matrix.  sizes = {L blocks, U blocks};
+ * factors: L (strictly lower, A's entry order), U (strictly upper), D^-1 (nb blocks), host arrays;
+ * apply: u = BILU^-1 f (u starts at 0). */
+JXCPR_API int jxcpr_solver_bilu_sizes(jxcpr_solver *solver, long long *sizes);
+JXCPR_API int jxcpr_solver_bilu_factors(jxcpr_solver *solver, double *la, double *ua, double *dinv);
+JXCPR_API int jxcpr_solver_bilu_apply(jxcpr_solver *solver, const double *f, double *u, int device);
 
 /* Queues `sweeps` stage-2 sweeps in the fast path's own storage precision (FP64, or FP32 in the mixed
  * path) on internal vectors, asynchronously on the solver's stream (no reference counterpart): the

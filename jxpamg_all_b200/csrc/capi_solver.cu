@@ -62,7 +62,11 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"flexible", &p.flexible},
                {"autotune", &p.autotune},
                {"graphs", &p.graphs},
-               {"orthog", &p.orthog}};
+               {"orthog", &p.orthog},
+               {"bilu_sweeps", &p.bilu_sweeps},
+               {"bilu_ir_iters", &p.bilu_ir_iters},
+               {"bilu_lower_iters", &p.bilu_lower_iters},
+               {"bilu_upper_iters", &p.bilu_upper_iters}};
     if (!key) return JXCPR_ERROR_ARG;
     if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
     for (auto &e : tab)
@@ -316,6 +320,42 @@ int jxcpr_solver_stage2_sweep(jxcpr_solver *h, const double *b, double *x, int d
             JX_CUDA(cudaMemcpyAsync(x, S.x.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
             JX_CUDA(cudaStreamSynchronize(st));
         }
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_bilu_sizes(jxcpr_solver *h, long long *sizes) {
+    if (!h || !sizes || !h->s.cpr.bilu) return JXCPR_ERROR_ARG;
+    sizes[0] = h->s.cpr.bilu->L.nnzb;
+    sizes[1] = h->s.cpr.bilu->U.nnzb;
+    return JXCPR_SUCCESS;
+}
+
+int jxcpr_solver_bilu_factors(jxcpr_solver *h, double *la, double *ua, double *dinv) {
+    if (!h || !h->s.cpr.bilu) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        const Bilu &B = *h->s.cpr.bilu;
+        const size_t bn = (size_t)B.bs * B.bs;
+        if (la && B.L.nnzb) JX_CUDA(cudaMemcpy(la, B.L.a.get(), sizeof(double) * B.L.nnzb * bn, cudaMemcpyDeviceToHost));
+        if (ua && B.U.nnzb) JX_CUDA(cudaMemcpy(ua, B.U.a.get(), sizeof(double) * B.U.nnzb * bn, cudaMemcpyDeviceToHost));
+        if (dinv && B.nb) JX_CUDA(cudaMemcpy(dinv, B.Dinv.get(), sizeof(double) * B.nb * bn, cudaMemcpyDeviceToHost));
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_bilu_apply(jxcpr_solver *h, const double *f, double *u, int device) {
+    if (!h || !f || !u || !h->s.cpr.bilu) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        Solver &S = h->s;
+        const long long n = (long long)S.A.nb * S.A.bs;
+        cudaStream_t st = S.stream;
+        const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        JX_CUDA(cudaMemcpyAsync(S.b.get(), f, sizeof(double) * n, in, st));
+        JX_CUDA(cudaMemsetAsync(S.x.get(), 0, sizeof(double) * n, st));
+        S.cpr.bilu->solve(S.A.view(), S.b.get(), S.x.get(), st);
+        const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        JX_CUDA(cudaMemcpyAsync(u, S.x.get(), sizeof(double) * n, out, st));
+        JX_CUDA(cudaStreamSynchronize(st));
         return JXCPR_SUCCESS;
     });
 }

@@ -87,12 +87,27 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
     stats[0] = t.stop_ms(s) * 1e-3;
     stats[2] = 0.0;  // stage 2 (HGS) needs no setup beyond the level-0 schedule
+    bilu.reset();
+    if (prm.stage2_solver_type == 5) {
+        Timer t2;
+        t2.start(s);
+        bilu.reset(new Bilu());
+        bilu->sweeps = prm.bilu_sweeps;
+        bilu->ir_iters = prm.bilu_ir_iters;
+        bilu->lower_iters = prm.bilu_lower_iters;
+        bilu->upper_iters = prm.bilu_upper_iters;
+        bilu->setup(A, s);
+        bres.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+        bdelta.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+        stats[2] = t2.stop_ms(s) * 1e-3;
+    }
     ready = true;
 }
 
 void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
     if (fast) {
         fast->apply(r, z, s);
+        bilu_stage(r, z, s);
         return;
     }
     const int nb = A.nb, bs = A.bs;
@@ -102,6 +117,20 @@ void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
     prolong_pressure(nb, bs, prm.pressure_index, xp.get(), z, s);
     if (prm.stage2_solver_type == 2)
         for (int it = 0; it < prm.stage2_maxit; ++it) stage2_sweep(r, z, s);
+    bilu_stage(r, z, s);
+}
+
+// Stage 2 as a block-ILU(0) correction: r' = r - A z, z += BILU^-1 r'
+// (the composition of JXF_CPRPrecond without stage-2 sweeps, jxf_ParBSRMatrixMatvec
+// and jxf_BILUSolve that the reference's drivers use).
+void CprPrecond::bilu_stage(const double *r, double *z, cudaStream_t s) {
+    if (!bilu) return;
+    const long long n = (long long)A.nb * A.bs;
+    copy_dev(n, r, bres.get(), s);
+    bsr_spmv<double, double>(A, -1.0, z, 1.0, bres.get(), nullptr, s, false);
+    JX_CUDA(cudaMemsetAsync(bdelta.get(), 0, sizeof(double) * n, s));
+    bilu->solve(A, bres.get(), bdelta.get(), s);
+    axpy_dev(n, 1.0, bdelta.get(), z, s);
 }
 
 void CprPrecond::stage2_sweep(const double *r, double *z, cudaStream_t s) {

@@ -7,6 +7,7 @@
 #include <memory>
 
 #include "amg.cuh"
+#include "bilu.cuh"
 #include "common.cuh"
 #include "fast.cuh"
 #include "kernels.cuh"
@@ -31,7 +32,12 @@ struct SolverParams {
     int stage1_maxit = 1;
     int stage2_maxit = 3;
     int stage1_solver_type = 1;  // 1: AMG
-    int stage2_solver_type = 2;  // 2: block hybrid Gauss-Seidel (HGS)
+    int stage2_solver_type = 2;  // 2: block hybrid Gauss-Seidel (HGS); 5: block ILU(0) correction (BILU)
+    // BILU stage 2 (jxf_BILUSetup type 3 / jxf_BILUSolve tri-solve 14 parameters)
+    int bilu_sweeps = 3;
+    int bilu_ir_iters = 5;
+    int bilu_lower_iters = 5;
+    int bilu_upper_iters = 5;
     double threshold = 1e-15;    // accepted and ignored, as in the reference
     double stage2_relax_weight = 0.7;
     double stage2_omega = 0.9;
@@ -88,7 +94,9 @@ struct CprPrecond {
     BsrView<double> A;  // decoupled system matrix (owned by the solver)
     Amg amg;
     std::unique_ptr<FastCprBase> fast;  // smoother_order 1: throughput / mixed-precision preconditioner
-    std::unique_ptr<FastCprBase> fast_alt;  // learned mode: plain-smoother variant until the probe decides
+    std::unique_ptr<FastCprBase> fast_alt;
+    std::unique_ptr<Bilu> bilu;         // stage2_solver_type 5
+    DevBuf<double> bres, bdelta;        // BILU stage: r - A z and its correction  // learned mode: plain-smoother variant until the probe decides
     double factor_fast = 0.0, factor_plain = 0.0;  // learned mode: GMRES residual reduction per iteration
     double probe_bytes[2] = {0, 0};                 // modelled bytes per GMRES iteration (learned, plain)
     int learned_used = 0;
@@ -100,6 +108,7 @@ struct CprPrecond {
     void apply(const double *r, double *z, cudaStream_t s);
     // one stage-2 block hybrid Gauss-Seidel sweep on A z = r (z in/out)
     void stage2_sweep(const double *r, double *z, cudaStream_t s);
+    void bilu_stage(const double *r, double *z, cudaStream_t s);
     // one pressure V-cycle on A_p u = f, u in/out (FP64)
     void vcycle(const double *f, double *u, cudaStream_t s);
     int *err() { return amg.err.get(); }

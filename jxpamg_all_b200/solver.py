@@ -166,6 +166,20 @@ class CprGmres:
         return dict(learned_used=bool(o[0]), factor_learned=float(o[1]), factor_plain=float(o[2]),
                     bytes_learned=float(o[3]), bytes_plain=float(o[4]))
 
+    def bilu_factors(self):
+        """Block ILU(0) factors of stage2_solver_type 5: (la, ua, dinv) as flat host arrays."""
+        sz = np.zeros(2, np.int64)
+        _lib.check(self._so.jxcpr_solver_bilu_sizes(self.h, _ptr(sz)))
+        bn = self.bs * self.bs
+        la, ua, dinv = np.zeros(max(int(sz[0]), 1) * bn), np.zeros(max(int(sz[1]), 1) * bn), np.zeros(self.nb * bn)
+        _lib.check(self._so.jxcpr_solver_bilu_factors(self.h, _ptr(la), _ptr(ua), _ptr(dinv)))
+        return la[:int(sz[0]) * bn], ua[:int(sz[1]) * bn], dinv
+
+    def bilu_apply(self, f):
+        u = np.zeros(self.nb * self.bs)
+        _lib.check(self._so.jxcpr_solver_bilu_apply(self.h, _ptr(np.ascontiguousarray(f, np.float64)), _ptr(u), 0))
+        return u
+
     def close(self):
         if getattr(self, "h", None):
             self._so.jxcpr_solver_destroy(self.h)

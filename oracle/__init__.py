@@ -249,3 +249,60 @@ def ref_hgs_relax(ia, ja, a, bs, x, b, w=0.7, omega=0.9, direction=1, sweeps=1):
     ref().ref_hgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), c_double(w),
                         c_double(omega), c_int(direction), c_int(sweeps))
     return x
+
+
+# ---- block ILU(0) (orc_bilu.c restatement; ref_bilu = the reference library) ---------
+def bilu_pattern(ia, ja):
+    """Strictly lower / upper block patterns of A in A's entry order: (lia, lja, uia, uja)."""
+    nb = len(ia) - 1
+    ia, ja = _i32(ia), _i32(ja)
+    lia, uia = np.zeros(nb + 1, np.int32), np.zeros(nb + 1, np.int32)
+    lja, uja = np.zeros(max(len(ja), 1), np.int32), np.zeros(max(len(ja), 1), np.int32)
+    orc().orc_bilu_pattern(c_int(nb), _p(ia), _p(ja), _p(lia), _p(lja), _p(uia), _p(uja))
+    return lia, lja[:lia[-1]].copy(), uia, uja[:uia[-1]].copy()
+
+
+def bilu_setup(ia, ja, a, bs, sweeps=3):
+    """Factors of jxf_ILUSetupFGPBILU_v3: dict(lia, lja, la, uia, uja, ua, dinv)."""
+    nb = len(ia) - 1
+    lia, lja, uia, uja = bilu_pattern(ia, ja)
+    bn = bs * bs
+    la = np.zeros(max(len(lja), 1) * bn)
+    ua = np.zeros(max(len(uja), 1) * bn)
+    dinv = np.zeros(nb * bn)
+    orc().orc_bilu_setup(c_int(nb), c_int(bs), _p(_i32(ia)), _p(_i32(ja)), _p(_f64(a)), c_int(sweeps), _p(lia),
+                         _p(lja), _p(la), _p(uia), _p(uja), _p(ua), _p(dinv))
+    return dict(lia=lia, lja=lja, la=la[:len(lja) * bn], uia=uia, uja=uja, ua=ua[:len(uja) * bn], dinv=dinv)
+
+
+def bilu_solve(ia, ja, a, bs, F, f, ir=5, lower=5, upper=5, u0=None):
+    """u = BILU(f) with tri-solve 14 (u0 = 0 unless given)."""
+    nb = len(ia) - 1
+    u = np.zeros(nb * bs) if u0 is None else _f64(u0).copy()
+    orc().orc_bilu_solve(c_int(nb), c_int(bs), _p(_i32(ia)), _p(_i32(ja)), _p(_f64(a)), _p(F["lia"]),
+                         _p(F["lja"]), _p(F["la"]), _p(F["uia"]), _p(F["uja"]), _p(F["ua"]), _p(F["dinv"]),
+                         c_int(ir), c_int(lower), c_int(upper), _p(_f64(f)), _p(u))
+    return u
+
+
+def ref_bilu(ia, ja, a, bs, f, sweeps=3, ir=5, lower=5, upper=5):
+    """The reference's jxf_BILUSetup + jxf_BILUSolve: (u, la, ua, dinv)."""
+    nb = len(ia) - 1
+    lia, lja, uia, uja = bilu_pattern(ia, ja)
+    bn = bs * bs
+    la = np.zeros(max(len(lja), 1) * bn)
+    ua = np.zeros(max(len(uja), 1) * bn)
+    dinv = np.zeros(nb * bn)
+    u = np.zeros(nb * bs)
+    st = ref().ref_bilu(c_int(nb), c_int(bs), _p(_i32(ia)), _p(_i32(ja)), _p(_f64(a)), c_int(sweeps), c_int(ir),
+                        c_int(lower), c_int(upper), _p(_f64(f)), _p(u), _p(la), _p(ua), _p(dinv), c_int(1))
+    if st:
+        raise RuntimeError(f"ref_bilu returned {st}")
+    return u, la[:len(lja) * bn], ua[:len(uja) * bn], dinv
+
+
+def cpr_bilu_apply(cpr, ia, ja, a, bs, F, r, ir=5, lower=5, upper=5):
+    """Stage-2 BILU composition: z = CPR(r) without stage-2 sweeps, r' = r - A z, z += BILU(r')."""
+    z = cpr.apply(r)
+    rr = bsr_matvec(ia, ja, a, bs, z, alpha=-1.0, y=_f64(r).copy(), beta=1.0)
+    return z + 1.0 * bilu_solve(ia, ja, a, bs, F, rr, ir, lower, upper)

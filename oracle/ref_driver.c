@@ -24,6 +24,7 @@
 #include "jxf_mv.h"
 #include "jxf_pamg.h"
 #include "jxf_parbsr_mv.h"
+#include "jxf_parbilu.h"
 
 int ref_driver_version(void) { return 2; }
 
@@ -334,4 +335,47 @@ int ref_cpr_gmres_solve(int nb, int bs, const int *ia, const int *ja, const doub
     }
     quiet_end(quiet);
     return 0;
+}
+
+/* ---- block ILU(0): jxf_BILUSetup / jxf_BILUSolve ------------------------------
+ * Type 3 (jxf_ILUSetupFGPBILU_v3, par_bilu_setup.c:4996) with `sweeps` sweeps,
+ * solve with tri_solve 14 (par_bilu_solve.c:360, 2893), max_iter 1, tol 0,
+ * the given IR / lower / upper Jacobi iteration counts; u = 0 on entry.  The
+ * lower-case entry points are called directly: the upper-case JXF_BILUSetup /
+ * JXF_BILUSolve wrappers forward to the CSR ILU (parbsr_bilu.c:36-66).
+ * Outputs the factors (L, U strictly lower / upper blocks in A's order, D^-1
+ * blocks) and u. */
+int ref_bilu(int nb, int bs, const int *ia, const int *ja, const double *a, int sweeps, int ir, int lower, int upper,
+             const double *f, double *u, double *la, double *ua, double *dinv, int quiet)
+{
+    jxf_BSRMatrix *A = make_bsr(nb, bs, ia, ja, a);
+    jxf_ParBSRMatrix *Ap = to_par(A);
+    jxf_Vector *vf = make_vec(nb * bs, f), *vu = make_vec(nb * bs, NULL), *vt = make_vec(nb * bs, NULL);
+    jxf_ParVector *pf = to_par_vec(Ap, vf), *pu = to_par_vec(Ap, vu), *pt = to_par_vec(Ap, vt);
+    void *solver = jxf_BILUCreate();
+    jxf_ParBILUData *d = (jxf_ParBILUData *)solver;
+    jxf_ParILUDataIluType(d) = 3;
+    jxf_ParILUDataLfil(d) = 0;
+    jxf_ParILUDataMaxIter(d) = 1;
+    jxf_ParILUDataTol(d) = 0.0;
+    jxf_ParILUDataTriSolve(d) = 14;
+    jxf_ParILUDataLogging(d) = 0;
+    jxf_ParILUDataPrintLevel(d) = 0;
+    jxf_ParILUDatasweep(d) = sweeps;
+    jxf_ParILUDataIRIters(d) = ir;
+    jxf_ParILUDataLowerJacobiIters(d) = lower;
+    jxf_ParILUDataUpperJacobiIters(d) = upper;
+    quiet_begin(quiet);
+    int ierr = jxf_BILUSetup(solver, Ap, pt, pt);
+    if (!ierr) ierr = jxf_BILUSolve(solver, Ap, pf, pu);
+    quiet_end(quiet);
+    const int bn = bs * bs;
+    jxf_BSRMatrix *L = jxf_ParBSRMatrixDiag(jxf_ParILUDataMatL(d));
+    jxf_BSRMatrix *U = jxf_ParBSRMatrixDiag(jxf_ParILUDataMatU(d));
+    if (la) memcpy(la, jxf_BSRMatrixData(L), sizeof(double) * (size_t)jxf_BSRMatrixI(L)[nb] * bn);
+    if (ua) memcpy(ua, jxf_BSRMatrixData(U), sizeof(double) * (size_t)jxf_BSRMatrixI(U)[nb] * bn);
+    if (dinv) memcpy(dinv, pvec_data(jxf_ParILUDataD(d)), sizeof(double) * (size_t)nb * bn);
+    memcpy(u, pvec_data(pu), sizeof(double) * nb * bs);
+    jxf_BILUDestroy(solver);
+    return ierr;
 }
