@@ -329,7 +329,8 @@ struct DevOps {
 };
 }  // namespace
 
-GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s) {
+GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s,
+                         const std::function<void(const double *, double *)> *ext) {
     GmresResult res;
     const int k_dim = prm.k_dim;
     const long long nl = n;
@@ -341,7 +342,8 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
         bsr_spmv<double, double>(A, alpha, xx, beta, yy, kerr, s, prm.use_tma_spmv != 0 && kerr != nullptr);
     };
     auto precond = [&](const double *in, double *out) {
-        if (M) M->apply(in, out, s);
+        if (ext && *ext) (*ext)(in, out);
+        else if (M) M->apply(in, out, s);
         else copy_dev(nl, in, out, s);
     };
     const int np = ops.np;
@@ -535,7 +537,8 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     kerr.alloc(1);
     kerr.zero(s);
     cpr.prm = prm;
-    cpr.setup(A.view(), s);
+    cpr.ready = false;
+    if (prm.stage1_solver_type) cpr.setup(A.view(), s);  // 0: GMRES without CPR (identity or caller's preconditioner)
     gmres.prm = prm;
     gmres.kerr = kerr.get();
     gmres.setup(nb * bs, s);
@@ -601,7 +604,7 @@ GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
     gmres.prm = prm;
     cpr.prm.stage2_maxit = prm.stage2_maxit;
     cpr.prm.stage1_maxit = prm.stage1_maxit;
-    last = gmres.solve(A.view(), prm.stage1_solver_type ? &cpr : nullptr, b.get(), x.get(), s);
+    last = gmres.solve(A.view(), prm.stage1_solver_type ? &cpr : nullptr, b.get(), x.get(), s, &ext_precond);
     const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     JX_CUDA(cudaMemcpyAsync(x_io, x.get(), sizeof(double) * n, out, s));
     JX_CUDA(cudaStreamSynchronize(s));

@@ -4,6 +4,7 @@
 #include <string>
 #include <vector>
 
+#include <functional>
 #include <memory>
 
 #include "amg.cuh"
@@ -134,7 +135,9 @@ struct Gmres {
     int cgs_blocks = 1;
     int *kerr = nullptr;
     void setup(int n_, cudaStream_t s);
-    GmresResult solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s);
+    // ext (optional): any other right preconditioner z = M^-1 r on device vectors
+    GmresResult solve(const BsrView<double> &A, CprPrecond *M, const double *b, double *x, cudaStream_t s,
+                      const std::function<void(const double *, double *)> *ext = nullptr);
 };
 
 // Full solver object: owns the device matrix, decoupling coefficients, CPR, GMRES.
@@ -151,6 +154,8 @@ struct Solver {
     bool stream_set = false;  // the caller chose the stream (possibly the legacy default stream)
     double setup_ms = 0.0, solve_ms = 0.0, upload_ms = 0.0, decouple_ms = 0.0;
     GmresResult last;
+    // a preconditioner supplied by the caller instead of CPR (stage1_solver_type 0 then applies it)
+    std::function<void(const double *, double *)> ext_precond;
     // A on the host or the device (device = 1), copied into the solver.
     void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);
     // b, x host or device; x holds the initial guess on entry.
