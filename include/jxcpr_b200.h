@@ -42,6 +42,9 @@ JXCPR_API int jxcpr_version(void);
 JXCPR_API unsigned long long jxcpr_launch_count(void);
 /* Message describing the calling thread's last failure ("" if none). */
 JXCPR_API const char *jxcpr_last_error(void);
+/* The library keeps freed device blocks for reuse (a freed block is handed out again only after a
+ * device synchronisation); this returns every cached block to the driver. */
+JXCPR_API int jxcpr_release_cached_memory(void);
 
 /* ---- BSR SpMV ------------------------------------------------------------
  * y = alpha*A*x + beta*y for a block-CSR matrix with bs x bs row-major blocks

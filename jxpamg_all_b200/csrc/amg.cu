@@ -91,36 +91,38 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(int n, const double *__r
     for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = xs[i];
 }
 
-// Explicit inverse column by column (setup of the fast coarse solve).
-__global__ void lu_inverse_kernel(int n, const double *__restrict__ Lt, const double *__restrict__ Ut,
-                                  double *__restrict__ inv_t, double *__restrict__ work) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;  // unit vector e_c
-    if (c >= n) return;
-    double *x = work + (long long)c * n;
-    for (int i = 0; i < n; ++i) x[i] = (i == c) ? 1.0 : 0.0;
-    for (int k = 0; k < n - 1; ++k) {
-        const double xk = x[k];
-        for (int j = k + 1; j < n; ++j) {
-            const double l = Lt[(long long)k * n + j];
-            if (l != 0.0) x[j] -= l * xk;
-        }
-    }
-    for (int k = n - 1; k > 0; --k) {
-        x[k] /= Ut[(long long)k * n + k];
-        const double xk = x[k];
-        for (int j = 0; j < k; ++j) {
-            const double v = Ut[(long long)k * n + j];
-            if (v != 0.0) x[j] -= xk * v;
-        }
-    }
-    x[0] /= Ut[0];
-    for (int i = 0; i < n; ++i) inv_t[(long long)c * n + i] = x[i];  // column c of A^{-1}
+// Explicit inverse (setup of the fast coarse solve): X = I, then the forward
+// and back substitutions of the stored factors applied to every column at
+// once, one launch per elimination step (the same operations per column as a
+// column-by-column substitution).
+__global__ void eye_kernel(int n, double *__restrict__ X) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (long long)n * n) X[t] = (t / n == t % n) ? 1.0 : 0.0;
 }
 
-__global__ void transpose_sq_kernel(int n, const double *__restrict__ in, double *__restrict__ out) {
-    const int r = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < n && c < n) out[(long long)c * n + r] = in[(long long)r * n + c];
+// rows j > k: X[j][c] -= L[j][k] X[k][c]
+__global__ void inv_forward_kernel(int n, int k, const double *__restrict__ Lt, double *__restrict__ X) {
+    const int j = k + 1 + blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n || c >= n) return;
+    const double l = Lt[(long long)k * n + j];
+    if (l != 0.0) X[(long long)j * n + c] -= l * X[(long long)k * n + c];
 }
+
+// rows j < k: X[j][c] -= U[j][k] (X[k][c] / U[k][k]); row k itself is scaled by inv_scale_kernel afterwards
+__global__ void inv_backward_kernel(int n, int k, const double *__restrict__ Ut, double *__restrict__ X) {
+    const int j = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k || c >= n) return;
+    const double v = Ut[(long long)k * n + j];
+    if (v != 0.0) X[(long long)j * n + c] -= (X[(long long)k * n + c] / Ut[(long long)k * n + k]) * v;
+}
+
+__global__ void inv_scale_kernel(int n, int k, const double *__restrict__ Ut, double *__restrict__ X) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) X[(long long)k * n + c] /= Ut[(long long)k * n + k];
+}
+
 
 // u = Ainv f, one warp per row.
 __global__ void dense_gemv_kernel(int n, const double *__restrict__ Ainv, const double *__restrict__ f,
@@ -159,12 +161,22 @@ void coarse_setup(Amg &H, cudaStream_t s) {
     transpose_upper_kernel<<<dim3(div_up(n, 256), n), 256, 0, s>>>(n, M.get(), H.Ufac.get());
     JX_LAUNCH_CHECK();
     if (!H.prm.coarse_exact) {
-        DevBuf<double> inv_t((size_t)n * n), work((size_t)n * n);
-        lu_inverse_kernel<<<div_up(n, 64), 64, 0, s>>>(n, H.Lt.get(), H.Ufac.get(), inv_t.get(), work.get());
-        JX_LAUNCH_CHECK();
         H.Ainv.alloc((size_t)n * n);
-        transpose_sq_kernel<<<dim3(div_up(n, 256), n), 256, 0, s>>>(n, inv_t.get(), H.Ainv.get());
+        double *X = H.Ainv.get();
+        eye_kernel<<<div_up((long long)n * n, 256), 256, 0, s>>>(n, X);
         JX_LAUNCH_CHECK();
+        for (int k = 0; k < n - 1; ++k) {
+            inv_forward_kernel<<<dim3(div_up(n, 256), n - k - 1), 256, 0, s>>>(n, k, H.Lt.get(), X);
+            JX_LAUNCH_CHECK();
+        }
+        for (int k = n - 1; k >= 0; --k) {
+            if (k > 0) {
+                inv_backward_kernel<<<dim3(div_up(n, 256), k), 256, 0, s>>>(n, k, H.Ufac.get(), X);
+                JX_LAUNCH_CHECK();
+            }
+            inv_scale_kernel<<<div_up(n, 256), 256, 0, s>>>(n, k, H.Ufac.get(), X);
+            JX_LAUNCH_CHECK();
+        }
     }
     JX_CUDA(cudaStreamSynchronize(s));
 }
@@ -233,7 +245,12 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         AmgLevel &L = *H.levels[level];
         const int n = L.A.nrows;
         DevPattern S;
-        L.theta = H.prm.theta_for_level ? H.prm.theta_for_level(level, L.A.view()) : H.prm.strong_threshold;
+        if (H.prm.theta_for_level) {
+            L.theta = H.prm.theta_for_level(level, L.A.view());
+            H.log.mark("level_features", s);
+        } else {
+            L.theta = H.prm.strong_threshold;
+        }
         amg_strength(L.A.view(), L.theta, H.prm.max_row_sum, S, s);
         H.log.mark("strength", s);
         std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);

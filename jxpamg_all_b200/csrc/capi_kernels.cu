@@ -108,3 +108,12 @@ int jxcpr_dot_dev(long long n, const double *x, const double *y, double *out_hos
 }
 
 }  // extern "C"
+
+extern "C" int jxcpr_release_cached_memory(void) {
+    try {
+        jxcpr::pool_trim();
+    } catch (...) {
+        return JXCPR_ERROR_DEVICE;
+    }
+    return JXCPR_SUCCESS;
+}

@@ -57,8 +57,17 @@ void count_launches(unsigned long long n);  // kernels replayed by a CUDA graph 
         JX_CUDA(cudaGetLastError());          \
     } while (0)
 
-// Owning device buffer (cudaMalloc'd, 256-byte aligned, padded by 64 bytes so
-// that 16-byte-rounded bulk copies of the tail stay inside the allocation).
+// Device memory cache behind DevBuf.  A freed block is parked; it becomes
+// reusable only after a device synchronisation (the one cudaFree would have
+// done), so no work still queued on any stream can touch a block handed out
+// again.  Blocks are bucketed (powers of two up to 1 GiB, 256 MiB multiples
+// above); the cache is trimmed when it exceeds its limit or cudaMalloc fails.
+void *pool_alloc(size_t bytes);
+void pool_free(void *p);
+void pool_trim();
+
+// Owning device buffer (256-byte aligned, padded by 64 bytes so that
+// 16-byte-rounded bulk copies of the tail stay inside the allocation).
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -75,18 +84,12 @@ struct DevBuf {
     ~DevBuf() { release(); }
     void alloc(size_t count) {
         release();
+        const size_t bytes = count * sizeof(T) + 64;
+        p = static_cast<T *>(pool_alloc(bytes));
         n = count;
-        size_t bytes = count * sizeof(T) + 64;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            n = 0;
-            set_error("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
-            throw CudaError{e, "cudaMalloc"};
-        }
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) pool_free(p);
         p = nullptr;
         n = 0;
     }

@@ -68,11 +68,13 @@ struct LevelMat {
 template <typename TX>
 struct FastLevel {
     int n = 0;
-    int smoother = FS_L1_JACOBI;
+    int smoother = FS_L1_JACOBI;  // in use
+    int smoother_cfg = FS_L1_JACOBI, smoother_plain = FS_L1_JACOBI;  // configured / plain settings
     LevelMat A;          // colour classes as segments (FS_COLOR_GS) or one segment
     int last_color = -1;
     LevelMat P, R;       // interpolation from level+1 / restriction to it
-    DevBuf<TX> dinv;     // 1/a_ii (GS, Chebyshev) or 1/sum|a_ij| (l1-Jacobi); 0 skips the row
+    DevBuf<TX> dinv;     // 1/a_ii (GS, Chebyshev); 0 skips the row
+    DevBuf<TX> dinv_l1;  // 1/sum_j |a_ij| (l1-Jacobi)
     double cheb[3] = {0, 0, 0};  // p(t) = c0 + c1 t + c2 t^2
     double cheb_lo = 0, cheb_hi = 0, lambda_max = 0;
     DevBuf<TX> f, u, r, z, y1, y2;
@@ -103,6 +105,9 @@ struct FastCprBase {
     virtual void level_info(int l, int *smoother, int *kind, double *cheb) const = 0;
     // Asymptotic convergence factor of the V-cycle on A_0 e = 0 (power method, `cycles` cycles)
     virtual double vcycle_factor(int cycles, cudaStream_t s) = 0;
+    // plain = true: the plain smoothers (colour GS / l1-Jacobi) on every level, on
+    // the same storage; false: the configured ones (Chebyshev / learned)
+    virtual void set_plain_mode(bool plain) = 0;
     // Modelled bytes one application moves (operator and vector traffic of
     // every smoother pass, residual, transfer and stage-2 sweep).
     virtual double apply_bytes() const = 0;

@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <memory>
 #include <numeric>
+#include <map>
+#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -227,8 +229,26 @@ std::string layout_name(const LevelMat &M) {
     return M.sell ? std::string("sell") : ("csr/" + std::to_string(M.lanes));
 }
 
+// Layout choices of earlier setups, keyed by operator role, shape and storage:
+// a repeated setup of the same system skips the timing runs.
+struct TuneChoice {
+    int sell = 0, lanes = 1;
+    double us = 0.0;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> &tune_cache() {
+    static std::map<std::string, TuneChoice> *c = new std::map<std::string, TuneChoice>();
+    return *c;
+}
+std::string tune_key(const char *name, int n, long long nnz, int kind, int E) {
+    char k[160];
+    snprintf(k, sizeof k, "%s/%d/%lld/%d/%d", name, n, nnz, kind, E);
+    return k;
+}
+
 // Builds a scalar operator in the layout that runs fastest here: CSR with
-// 1..32 lanes per row, or sliced ELL (operators with >= 2048 rows).
+// 1..32 lanes per row (the candidates around the mean row length), or sliced
+// ELL (operators with >= 2048 rows).
 template <typename TX>
 void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, const int *ja, const double *a,
                  int kind, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
@@ -237,33 +257,53 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
         build_level_mat(n, m, nnz, 1, ia, ja, a, kind, use_sell(opt, n, nnz), order, seg, order_dev, M, s);
         return;
     }
-    build_level_mat(n, m, nnz, 1, ia, ja, a, kind, false, order, seg, order_dev, M, s);
-    DevBuf<TX> x(m > 0 ? m : 1), y(n > 0 ? n : 1);
-    x.zero(s);
-    y.zero(s);
-    double best = 1e30;
-    int best_lanes = M.lanes;
-    for (int V = 1; V <= 32; V *= 2) {
-        M.lanes = V;
-        const double t = time_pass<TX>(M, x.get(), y.get(), s);
-        if (t < best) {
-            best = t;
-            best_lanes = V;
+    const std::string key = tune_key(name, n, nnz, kind, 1);
+    TuneChoice best;
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = tune_cache().find(key);
+        if (it != tune_cache().end()) {
+            best = it->second;
+            cached = true;
         }
     }
-    M.lanes = best_lanes;
-    if (n >= 2048) {
-        LevelMat S;
-        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, true, order, seg, order_dev, S, s);
-        const double t = time_pass<TX>(S, x.get(), y.get(), s);
-        if (t < best) {
-            best = t;
-            M = std::move(S);
+    if (cached) {
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, best.sell != 0, order, seg, order_dev, M, s);
+        if (!best.sell) M.lanes = best.lanes;
+    } else {
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, false, order, seg, order_dev, M, s);
+        DevBuf<TX> x(m > 0 ? m : 1), y(n > 0 ? n : 1);
+        x.zero(s);
+        y.zero(s);
+        best.us = 1e30;
+        const int v0 = lanes_for(n ? (double)nnz / n : 1.0);
+        for (int V = 1; V <= 32; V *= 2) {
+            if (V * 4 < v0 || V > v0 * 4) continue;  // candidates within a factor 4 of the mean-based choice
+            M.lanes = V;
+            const double t = time_pass<TX>(M, x.get(), y.get(), s);
+            if (t < best.us) {
+                best.us = t;
+                best.lanes = V;
+            }
         }
+        M.lanes = best.lanes;
+        if (n >= 2048) {
+            LevelMat S;
+            build_level_mat(n, m, nnz, 1, ia, ja, a, kind, true, order, seg, order_dev, S, s);
+            const double t = time_pass<TX>(S, x.get(), y.get(), s);
+            if (t < best.us) {
+                best.us = t;
+                best.sell = 1;
+                M = std::move(S);
+            }
+        }
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_cache()[key] = best;
     }
     char line[200];
-    snprintf(line, sizeof line, "%s rows %d mean %.1f layout %s %.2f us", name, n, n ? (double)nnz / n : 0.0,
-             layout_name(M).c_str(), best);
+    snprintf(line, sizeof line, "%s rows %d mean %.1f layout %s %.2f us%s", name, n, n ? (double)nnz / n : 0.0,
+             layout_name(M).c_str(), best.us, cached ? " (cached)" : "");
     log.emplace_back(line);
 }
 
@@ -387,9 +427,9 @@ struct FastCpr final : FastCprBase {
             }
         } else if (L.smoother == FS_L1_JACOBI) {
             for (int rep = 0; rep < 2; ++rep) {  // 2 x (u -> tmp -> u)
-                fk::OpJacobi<TX> a{f, L.dinv.get(), u, L.z.get(), zero ? 1 : 0};
+                fk::OpJacobi<TX> a{f, L.dinv_l1.get(), u, L.z.get(), zero ? 1 : 0};
                 launch_rows<TX>(M, a, 0, M.nstored, s);
-                fk::OpJacobi<TX> b{f, L.dinv.get(), L.z.get(), u, 0};
+                fk::OpJacobi<TX> b{f, L.dinv_l1.get(), L.z.get(), u, 0};
                 launch_rows<TX>(M, b, 0, M.nstored, s);
                 zero = false;
             }
@@ -534,7 +574,7 @@ struct FastCpr final : FastCprBase {
         const size_t n = (size_t)nb * bs;
         in_buf.alloc(n > 0 ? n : 1);
         out_buf.alloc(n > 0 ? n : 1);
-        JX_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        if (!cap_stream) JX_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
         const unsigned long long k0 = launch_count();
         JX_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
         try {
@@ -608,6 +648,18 @@ struct FastCpr final : FastCprBase {
         vcycle_tx(L0.f.get(), L0.u.get(), s);
         fk::convert<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, L0.u.get(), up);
         JX_LAUNCH_CHECK();
+    }
+
+    void set_plain_mode(bool plain) override {
+        for (auto &lp : lv) lp->smoother = plain ? lp->smoother_plain : lp->smoother_cfg;
+        if (graph_exec) {  // the captured sequence depends on the smoothers
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+        if (graph) {
+            cudaGraphDestroy(graph);
+            graph = nullptr;
+        }
     }
 
     DevBuf<TX> nat_r, nat_z;
@@ -699,9 +751,11 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
         alloc_vec(Lv.u, n);
         if (l < L - 1) {
             const int kind = fp64 ? VAL_F64 : ((opt.precision == 2 && l >= opt.bf16_level) ? VAL_BF16 : VAL_F32);
-            int sm = HL.smoother == SMOOTH_COLOR_GS ? FS_COLOR_GS : FS_L1_JACOBI;
+            const int plain_sm = HL.smoother == SMOOTH_COLOR_GS ? FS_COLOR_GS : FS_L1_JACOBI;
+            int sm = plain_sm;
             if (opt.smoother == 2 || (opt.smoother == 1 && sm == FS_L1_JACOBI)) sm = FS_CHEB;
-            Lv.smoother = sm;
+            Lv.smoother = Lv.smoother_cfg = sm;
+            Lv.smoother_plain = (opt.smoother == 2) ? FS_CHEB : plain_sm;
             const CsrView<double> Av = HL.A.view();
             const std::string nm = "A" + std::to_string(l);
             if (sm == FS_COLOR_GS) {
@@ -714,11 +768,15 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
             }
             alloc_vec(Lv.dinv, n);
             if (n) {
-                if (sm == FS_L1_JACOBI)
-                    fk::dinv_l1<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.a, Lv.dinv.get());
-                else
-                    fk::dinv_diag<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.ja, Av.a, Lv.dinv.get());
+                fk::dinv_diag<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.ja, Av.a, Lv.dinv.get());
                 JX_LAUNCH_CHECK();
+            }
+            if (Lv.smoother_plain == FS_L1_JACOBI || sm == FS_L1_JACOBI) {
+                alloc_vec(Lv.dinv_l1, n);
+                if (n) {
+                    fk::dinv_l1<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.a, Lv.dinv_l1.get());
+                    JX_LAUNCH_CHECK();
+                }
             }
             if (sm == FS_CHEB) {
                 Lv.lambda_max = estimate_lambda_max(Av, 12, s);
@@ -760,9 +818,30 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
     if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
         const int kind = fp64 ? VAL_F64 : VAL_F32;
-        if (!opt.autotune) {
-            build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, A.nb >= opt.sell_min_rows, order,
-                            H0.fwd.h_group_ptr, H0.fwd.perm.get(), F->st2, s);
+        const std::string key = tune_key("stage2", A.nb, A.nnzb, kind, A.bs * A.bs);
+        TuneChoice cached_choice;
+        bool cached = false;
+        if (opt.autotune) {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = tune_cache().find(key);
+            if (it != tune_cache().end()) {
+                cached_choice = it->second;
+                cached = true;
+            }
+        }
+        if (!opt.autotune || cached) {
+            const bool sell = cached ? cached_choice.sell != 0 : A.nb >= opt.sell_min_rows;
+            build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, sell, order, H0.fwd.h_group_ptr,
+                            H0.fwd.perm.get(), F->st2, s);
+            if (cached) {
+                F->opt.stage2_lanes = cached_choice.lanes;
+                char line[200];
+                snprintf(line, sizeof line, "stage2 rows %d blocks/row %.1f layout %s %.2f us (cached)", A.nb,
+                         (double)A.nnzb / A.nb,
+                         F->st2.sell ? "sell" : ("csr/" + std::to_string(F->opt.stage2_lanes)).c_str(),
+                         cached_choice.us);
+                F->tune_log.emplace_back(line);
+            }
         } else {
             // time one stage-2 sweep per layout (CSR with 1..8 lanes per block row, sliced ELL)
             build_level_mat(A.nb, A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, false, order, H0.fwd.h_group_ptr,
@@ -810,6 +889,12 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
                      (double)A.nnzb / A.nb,
                      F->st2.sell ? "sell" : ("csr/" + std::to_string(F->opt.stage2_lanes)).c_str(), best);
             F->tune_log.emplace_back(line);
+            TuneChoice c;
+            c.sell = F->st2.sell;
+            c.lanes = F->opt.stage2_lanes;
+            c.us = best;
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            tune_cache()[key] = c;
         }
     }
     JX_CUDA(cudaStreamSynchronize(s));

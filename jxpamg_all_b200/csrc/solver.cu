@@ -30,7 +30,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     amg.prm.strong_threshold = prm.strong_threshold;
     amg.prm.theta_for_level = nullptr;
     fast.reset();
-    fast_alt.reset();
+    probe_pending = false;
     learned_used = 0;
     factor_fast = factor_plain = 0.0;
     plan = LearnedPlan();
@@ -71,15 +71,12 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
             opt.level_upper = plan.upper;
         }
         fast.reset(make_fast_cpr(amg, A, cfg, opt, s));
+        amg.log.mark("fast_build", s);
         if (plan.active) {
             learned_used = 1;
-            if (prm.learned_fallback) {
-                // plain smoother settings on the same hierarchy; Solver::setup keeps
-                // whichever preconditioner reduces the GMRES residual faster
-                FastOptions plain = opt;
-                plain.smoother = 0;
-                fast_alt.reset(make_fast_cpr(amg, A, cfg, plain, s));
-            }
+            // plain smoother settings on the same hierarchy and storage; Solver::setup keeps
+            // whichever reduces the GMRES residual faster per byte
+            probe_pending = prm.learned_fallback != 0;
         }
     }
     rp.alloc(A.nb > 0 ? A.nb : 1);
@@ -97,6 +94,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         bilu->lower_iters = prm.bilu_lower_iters;
         bilu->upper_iters = prm.bilu_upper_iters;
         bilu->setup(A, s);
+        amg.log.mark("bilu_setup", s);
         bres.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
         bdelta.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
         stats[2] = t2.stop_ms(s) * 1e-3;
@@ -544,7 +542,12 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     gmres.setup(nb * bs, s);
     b.alloc((size_t)(nb > 0 ? nb : 1) * bs);
     x.alloc((size_t)(nb > 0 ? nb : 1) * bs);
-    if (cpr.fast_alt) learned_probe(s);
+    cpr.amg.log.mark("gmres_vectors", s);
+    if (cpr.probe_pending) {
+        learned_probe(s);
+        cpr.probe_pending = false;
+        cpr.amg.log.mark("learned_probe", s);
+    }
     JX_CUDA(cudaStreamSynchronize(s));
     setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -573,7 +576,7 @@ void Solver::learned_probe(cudaStream_t s) {
     };
     const double bl = cpr.fast->apply_bytes();
     const double rl = probe();
-    std::swap(cpr.fast, cpr.fast_alt);
+    cpr.fast->set_plain_mode(true);
     const double bp = cpr.fast->apply_bytes();
     const double rp = probe();
     cpr.factor_fast = pow(rl, 1.0 / m);
@@ -584,12 +587,8 @@ void Solver::learned_probe(cudaStream_t s) {
     const double ep = rp > 0.0 ? -log(rp) / (bp + common) : 1e300;
     cpr.probe_bytes[0] = bl + common;
     cpr.probe_bytes[1] = bp + common;
-    if (el >= ep) {
-        std::swap(cpr.fast, cpr.fast_alt);  // learned settings stay
-    } else {
-        cpr.learned_used = 0;
-    }
-    cpr.fast_alt.reset();
+    if (el >= ep) cpr.fast->set_plain_mode(false);  // learned settings stay
+    else cpr.learned_used = 0;
     gmres.prm = saved;
 }
 

@@ -95,9 +95,9 @@ struct CprPrecond {
     BsrView<double> A;  // decoupled system matrix (owned by the solver)
     Amg amg;
     std::unique_ptr<FastCprBase> fast;  // smoother_order 1: throughput / mixed-precision preconditioner
-    std::unique_ptr<FastCprBase> fast_alt;
+    bool probe_pending = false;  // learned mode: the plain-vs-learned probe runs after GMRES setup
     std::unique_ptr<Bilu> bilu;         // stage2_solver_type 5
-    DevBuf<double> bres, bdelta;        // BILU stage: r - A z and its correction  // learned mode: plain-smoother variant until the probe decides
+    DevBuf<double> bres, bdelta;        // BILU stage: r - A z and its correction
     double factor_fast = 0.0, factor_plain = 0.0;  // learned mode: GMRES residual reduction per iteration
     double probe_bytes[2] = {0, 0};                 // modelled bytes per GMRES iteration (learned, plain)
     int learned_used = 0;
