@@ -180,6 +180,26 @@ JXCPR_API int jxcpr_solver_level_features(jxcpr_solver *solver, int level, float
  * unless their residual reduction per byte is worse. */
 JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
 
+/* ---- batched solves: many set-up solvers, one graph launch; no reference counterpart -------------
+ * create: records every solver's whole GMRES solve (option graph_gmres is switched on: flexible GMRES
+ * with two-pass classical Gram-Schmidt and true-residual restarts, run on the device with conditional
+ * graph nodes) as an independent branch of one CUDA graph.  The solvers must be set up with the fast
+ * CPR path (smoother_order 1, stage1_solver_type 1) and stay alive and unchanged while the batch exists.
+ * solve: b[k], x[k] (x = initial guess, overwritten) host arrays, or device arrays with device = 1; one
+ * graph launch for all systems.  Per system: iterations, FP64 relative residual, latency_ms = its own
+ * solve time on the device, finish_ms = completion time since the first system started, status
+ * (0, 256 not converged, 512 device error).  Returns 0, or the first error other than 256.
+ * last_ms: device time of the last launch (CUDA events).  launch: the graph alone on `stream` (NULL:
+ * the batch's own), with the inputs already in the solvers' buffers. */
+typedef struct jxcpr_batch jxcpr_batch;
+JXCPR_API int jxcpr_batch_create(jxcpr_batch **batch, int nsys, jxcpr_solver *const *solvers);
+JXCPR_API int jxcpr_batch_destroy(jxcpr_batch *batch);
+JXCPR_API int jxcpr_batch_solve(jxcpr_batch *batch, const double *const *b, double *const *x, int device,
+                                int *iterations, double *rel_residual, double *latency_ms, double *finish_ms,
+                                int *status);
+JXCPR_API int jxcpr_batch_last_ms(jxcpr_batch *batch, double *ms);
+JXCPR_API int jxcpr_batch_launch(jxcpr_batch *batch, void *stream);
+
 /* ---- learned settings: 16 -> 64 (tanh) -> 3 MLP, FP32; no reference counterpart -----------------
  * Weight blob (jxcpr_mlp_num_weights() floats): mu[16], sigma[16], W1[64][16], b1[64], W2[3][64], b2[3];
  * outputs y -> strength threshold 0.1 + 0.8 sigmoid(y0), Chebyshev interval

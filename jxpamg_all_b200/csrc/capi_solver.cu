@@ -4,17 +4,15 @@
 #include <string.h>
 
 #include <algorithm>
+#include <stdexcept>
 #include <new>
 #include <string>
 
 #include "jxcpr_b200.h"
-#include "solver.cuh"
+#include "handle.cuh"
 
 using namespace jxcpr;
 
-struct jxcpr_solver {
-    Solver s;
-};
 
 namespace {
 template <typename F>
@@ -23,6 +21,8 @@ int guarded(F &&f) {
         return f();
     } catch (const CudaError &) {
         return JXCPR_ERROR_DEVICE;
+    } catch (const std::invalid_argument &) {
+        return JXCPR_ERROR_ARG;
     } catch (const std::bad_alloc &) {
         set_error("host allocation failed");
         return JXCPR_ERROR_MEMORY;
@@ -63,6 +63,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"autotune", &p.autotune},
                {"graphs", &p.graphs},
                {"orthog", &p.orthog},
+               {"graph_gmres", &p.graph_gmres},
                {"bilu_sweeps", &p.bilu_sweeps},
                {"bilu_ir_iters", &p.bilu_ir_iters},
                {"bilu_lower_iters", &p.bilu_lower_iters},

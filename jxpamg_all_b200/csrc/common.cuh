@@ -28,6 +28,8 @@ namespace jxcpr {
 void set_error(const char *fmt, ...);
 const char *last_error();
 unsigned long long launch_count();
+// kernels recorded into a graph are counted when the graph runs, not when captured
+void uncount_launches(unsigned long long n);
 
 // Number of SMs of the current device (cached per device).
 int sm_count();

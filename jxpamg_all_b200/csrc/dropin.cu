@@ -13,13 +13,10 @@
 #include <vector>
 
 #include "jxcpr_dropin.h"
-#include "solver.cuh"
+#include "handle.cuh"
 
 using namespace jxcpr;
 
-struct jxcpr_solver {  // layout of capi_solver.cu's handle
-    Solver s;
-};
 
 struct jxf_CPRPrecond_dropin {
     jxcpr_solver *h = nullptr;

@@ -99,6 +99,9 @@ struct FastOptions {
 struct FastCprBase {
     virtual ~FastCprBase() = default;
     virtual void apply(const double *r, double *z, cudaStream_t s) = 0;
+    // The application's kernels queued on s, never through the private graph:
+    // for callers that capture the application into a graph of their own.
+    virtual void apply_enqueue(const double *r, double *z, cudaStream_t s) = 0;
     virtual void vcycle(const double *fp, double *up, cudaStream_t s) = 0;  // FP64 pressure in/out
     virtual void stage2_sweep(const double *r, double *z, cudaStream_t s) = 0;
     virtual int num_levels() const = 0;

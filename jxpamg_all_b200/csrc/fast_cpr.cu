@@ -587,6 +587,7 @@ struct FastCpr final : FastCprBase {
         }
         JX_CUDA(cudaStreamEndCapture(cap_stream, &graph));
         graph_kernels = launch_count() - k0;
+        uncount_launches(graph_kernels);
         JX_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
     }
 
@@ -602,6 +603,8 @@ struct FastCpr final : FastCprBase {
         count_launches(graph_kernels);
         JX_CUDA(cudaMemcpyAsync(z, out_buf.get(), bytes, cudaMemcpyDeviceToDevice, s));
     }
+
+    void apply_enqueue(const double *r, double *z, cudaStream_t s) override { apply_direct(r, z, s); }
 
     void apply_direct(const double *r, double *z, cudaStream_t s) {
         FastLevel<TX> &L0 = *lv[0];

@@ -1,0 +1,606 @@
+// Restarted flexible GMRES(k) with the whole solve on the device, recorded as
+// one CUDA graph with conditional WHILE nodes:
+//
+//   ||b||  ->  WHILE (not done) {                       restart cycle
+//                 r = b - A x, ||r||, convergence test, v_0 = r / ||r||
+//                 WHILE (cycle continues) {              Arnoldi step i
+//                    z_i = M^-1 v_i  (CPR kernels recorded in place)
+//                    w = A z_i
+//                    h1 = V^T w,  w -= V h1              two-pass classical
+//                    h2 = V^T w,  s = ||w||^2            Gram-Schmidt (CGS2)
+//                    Givens rotation of column i (one thread), test
+//                    v_{i+1} = (w - V h2) / sqrt(s - ||h2||^2)
+//                 }
+//                 x += Z y  (y from the triangular solve at the cycle end)
+//              }
+//
+// The host sees no per-iteration round trip: the Hessenberg matrix, rotations,
+// residual estimates and the loop conditions live in device memory.  The
+// scalar recurrence (rotations, estimate, convergence and restart rules,
+// back substitution) follows the host GMRES (jxfpamg-0220/csrc/krylov/
+// pgmres.c:1090-1560) step for step; two things differ by design: each cycle
+// restarts from the true residual b - A x instead of the rotated estimate,
+// and the orthogonalisation is CGS2 (three passes over the basis, a fixed
+// number of kernels per step, which a graph needs) instead of MGS (i + 1
+// passes).  The norm of the new vector comes from Pythagoras,
+// ||w - V h2||^2 = ||w||^2 - ||h2||^2, as in delayed CGS2 (Swirydowicz et al.,
+// 2020).  Flexible: the preconditioned directions z_i are kept and x += Z y.
+#include <cmath>
+#include <stdexcept>
+
+#include "solver.cuh"
+
+namespace jxcpr {
+namespace gg {
+
+constexpr int kThreads = 256;
+constexpr int kRedThreads = 1024;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// sum over the block; the result is valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+__device__ __forceinline__ double sum_row(const double *row, int G, double *sh) {
+    double v = 0.0;
+    for (int j = threadIdx.x; j < G; j += blockDim.x) v += row[j];
+    return block_sum(v, sh);
+}
+
+// partials[blockIdx.x] = sum of x^2 over the block's elements
+__global__ void __launch_bounds__(kThreads) sq_partials(long long n, const double *__restrict__ x,
+                                                        double *__restrict__ partials) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
+        acc = fma(x[e], x[e], acc);
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kRedThreads) init_kernel(GgState *st, const double *__restrict__ partials, int G) {
+    __shared__ double sh[32];
+    const double v = sum_row(partials, G, sh);
+    if (threadIdx.x == 0) {
+        GgState s{};
+        s.b_norm = sqrt(v);
+        s.first = 1;
+        s.t_start = global_ns();
+        *st = s;
+    }
+}
+
+// Start of a restart cycle: ||r|| of r = b - A x, the convergence and stop
+// rules, and the first basis vector's scale.  Sets both loop conditions.
+__global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const double *__restrict__ partials, int G,
+                                                              GgParams P, GgWork W, double *__restrict__ norms,
+                                                              cudaGraphConditionalHandle h_out,
+                                                              cudaGraphConditionalHandle h_in) {
+    __shared__ double sh[32];
+    const double rn2 = sum_row(partials, G, sh);
+    if (threadIdx.x != 0) return;
+    GgState &s = *st;
+    const double rn = sqrt(rn2);
+    bool done = false;
+    s.cycles += 1;
+    if (s.first) {
+        s.first = 0;
+        if (s.b_norm != 0.0 && !(s.b_norm / s.b_norm == s.b_norm / s.b_norm)) {
+            s.status = 1;  // NaN/Inf in b
+            done = true;
+        } else if (rn != 0.0 && !(rn / rn == rn / rn)) {
+            s.status = 1;  // NaN/Inf in A or x0
+            done = true;
+        }
+        s.r_norm0 = rn;
+        s.epsilon = fmax(P.a_tol, P.tol * (s.b_norm > 0.0 ? s.b_norm : rn));
+        s.normdown = rn;
+        norms[0] = rn;
+    }
+    s.r_norm = rn;
+    if (!done) {
+        if (rn == 0.0 || (rn <= s.epsilon && s.iter >= P.min_iter)) {
+            s.converged = 1;
+            done = true;
+        } else if (s.est_conv && !P.check_restarted) {
+            done = true;  // estimate below tolerance, true residual not, no restart allowed
+        } else if (s.conv_fail || s.iter >= P.max_iter || s.cycles > P.max_iter + 1) {
+            done = true;
+        }
+    }
+    s.est_conv = 0;
+    s.conv_fail = 0;
+    s.i = 0;
+    s.m = 0;
+    if (done) {
+        s.done = 1;
+        s.cont = 0;
+        s.rel = s.b_norm > 0.0 ? rn / s.b_norm : (s.r_norm0 > 0.0 ? rn / s.r_norm0 : 0.0);
+        s.t_end = global_ns();
+        cudaGraphSetConditional(h_in, 0);
+        cudaGraphSetConditional(h_out, 0);
+    } else {
+        W.rs[0] = rn;
+        s.scale = 1.0 / rn;
+        s.cont = 1;
+        cudaGraphSetConditional(h_in, 1);
+    }
+}
+
+// v_0 = r * scale (skipped once the solve is done)
+__global__ void __launch_bounds__(kThreads) scale0_kernel(long long n, const double *__restrict__ r,
+                                                          double *const *__restrict__ V, const GgState *st) {
+    if (st->done) return;
+    const double sc = st->scale;
+    double *v0 = V[0];
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
+        v0[e] = r[e] * sc;
+}
+
+// dst = V[i] (the preconditioner's input buffer)
+__global__ void __launch_bounds__(kThreads) gather_kernel(long long n, const double *const *__restrict__ V,
+                                                          const GgState *st, double *__restrict__ dst) {
+    const double *src = V[st->i];
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
+        dst[e] = src[e];
+}
+
+// Z[i] = src (the preconditioner's output, kept for the flexible update)
+__global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, const double *__restrict__ src,
+                                                           double *const *__restrict__ Z, const GgState *st) {
+    double *dst = Z[st->i];
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
+        dst[e] = src[e];
+}
+
+// Block (x, k): partial <V[k], w> over the x-th slice, k <= i (k = i + 1 with
+// self: <w, w>).  Blocks beyond the current basis size return at once.
+__global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const double *const *__restrict__ V,
+                                                        const GgState *st, const double *__restrict__ w, int self,
+                                                        double *__restrict__ partials) {
+    __shared__ double sh[32];
+    const int k = blockIdx.y, m = st->i + 1;
+    if (k > m || (k == m && !self)) return;
+    const double *v = k == m ? w : V[k];
+    double acc = 0.0;
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
+        acc = fma(v[e], w[e], acc);
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[(long long)k * gridDim.x + blockIdx.x] = acc;
+}
+
+// h[k] = sum of partials row k, k <= i (one warp per row)
+__global__ void __launch_bounds__(kRedThreads) reduce_h_kernel(const double *__restrict__ partials, int G,
+                                                               const GgState *st, double *__restrict__ h) {
+    const int m = st->i + 1, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x >> 5; k < m; k += kRedThreads / 32) {
+        double v = 0.0;
+        for (int j = lane; j < G; j += 32) v += partials[(long long)k * G + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) h[k] = v;
+    }
+}
+
+// w -= sum_{k <= i} h[k] V[k]
+__global__ void __launch_bounds__(kThreads) update_kernel(long long n, const double *const *__restrict__ V,
+                                                          const GgState *st, const double *__restrict__ h,
+                                                          double *__restrict__ w) {
+    __shared__ const double *vs[kGgMaxK + 2];
+    __shared__ double hs[kGgMaxK + 2];
+    const int m = st->i + 1;
+    for (int k = threadIdx.x; k < m; k += kThreads) {
+        vs[k] = V[k];
+        hs[k] = h[k];
+    }
+    __syncthreads();
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
+        double s = w[e];
+        for (int k = 0; k < m; ++k) s = fma(-hs[k], vs[k][e], s);
+        w[e] = s;
+    }
+}
+
+// One thread: the Hessenberg column of this step, its Givens rotation, the
+// residual estimate, the cycle-end rules and, at a cycle end, y = H^-1 rs.
+__global__ void __launch_bounds__(kRedThreads) arnoldi_kernel(const double *__restrict__ partials, int G, GgState *st,
+                                                              GgParams P, GgWork W, double *__restrict__ norms,
+                                                              cudaGraphConditionalHandle h_in) {
+    __shared__ double sig;
+    const int i0 = st->i, m = i0 + 1, lane = threadIdx.x & 31;
+    // second-pass coefficients h2[k], k < m, and ||w||^2 (row m)
+    for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
+        double v = 0.0;
+        for (int j = lane; j < G; j += 32) v += partials[(long long)k * G + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) {
+            if (k < m) W.h2[k] = v;
+            else sig = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    GgState &s = *st;
+    const int K = P.k;
+    double *hh = W.hh, *rs = W.rs, *c = W.c, *sn = W.sn;
+#define HH(r, q) hh[(long long)(r) * K + (q)]
+    double ss = 0.0;
+    for (int j = 0; j < m; ++j) {
+        HH(j, i0) = W.h1[j] + W.h2[j];
+        ss += W.h2[j] * W.h2[j];
+    }
+    const double t2 = sig - ss;
+    double t = t2 > 0.0 ? sqrt(t2) : 0.0;
+    HH(m, i0) = t;
+    s.scale = t != 0.0 ? 1.0 / t : 0.0;
+    const int i = m;  // steps in this cycle, 1-based as in the reference loop
+    for (int j = 1; j < i; ++j) {
+        t = HH(j - 1, i - 1);
+        HH(j - 1, i - 1) = sn[j - 1] * HH(j, i - 1) + c[j - 1] * t;
+        HH(j, i - 1) = -sn[j - 1] * t + c[j - 1] * HH(j, i - 1);
+    }
+    t = HH(i, i - 1) * HH(i, i - 1);
+    t += HH(i - 1, i - 1) * HH(i - 1, i - 1);
+    double gamma = sqrt(t);
+    if (gamma == 0.0) gamma = 1.e-16;
+    c[i - 1] = HH(i - 1, i - 1) / gamma;
+    sn[i - 1] = HH(i, i - 1) / gamma;
+    rs[i] = -HH(i, i - 1) * rs[i - 1];
+    rs[i] /= gamma;
+    rs[i - 1] = c[i - 1] * rs[i - 1];
+    HH(i - 1, i - 1) = sn[i - 1] * HH(i, i - 1) + c[i - 1] * HH(i - 1, i - 1);
+    const double r_norm = fabs(rs[i]);
+    const double conv = r_norm / s.normdown;
+    s.normdown = r_norm;
+    s.iter += 1;
+    norms[s.iter] = r_norm;
+    s.r_norm = r_norm;
+    s.i = i;
+    s.m = m;
+    bool end = i >= K || s.iter >= P.max_iter;
+    if (s.iter > 1 && conv > P.convfac) {
+        s.conv_fail = 1;
+        end = true;
+    }
+    if (r_norm <= s.epsilon && s.iter >= P.min_iter) {
+        s.est_conv = 1;
+        end = true;
+    }
+    if (end) {
+        rs[i - 1] = rs[i - 1] / HH(i - 1, i - 1);
+        for (int k = i - 2; k >= 0; --k) {
+            double a = 0.0;
+            for (int j = k + 1; j < i; ++j) a -= HH(k, j) * rs[j];
+            a += rs[k];
+            rs[k] = a / HH(k, k);
+        }
+        for (int j = 0; j < i; ++j) W.y[j] = rs[j];
+    }
+#undef HH
+    s.cont = end ? 0 : 1;
+    cudaGraphSetConditional(h_in, end ? 0u : 1u);
+}
+
+// v_{m} = (w - sum_{k < m} h2[k] V[k]) * scale, skipped at a cycle end
+__global__ void __launch_bounds__(kThreads) final_kernel(long long n, double *const *__restrict__ V,
+                                                         const GgState *st, const double *__restrict__ h,
+                                                         const double *__restrict__ w) {
+    __shared__ const double *vs[kGgMaxK + 2];
+    __shared__ double hs[kGgMaxK + 2];
+    if (!st->cont) return;
+    const int m = st->m;
+    const double sc = st->scale;
+    double *dst = V[m];
+    for (int k = threadIdx.x; k < m; k += kThreads) {
+        vs[k] = V[k];
+        hs[k] = h[k];
+    }
+    __syncthreads();
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
+        double s = w[e];
+        for (int k = 0; k < m; ++k) s = fma(-hs[k], vs[k][e], s);
+        dst[e] = s * sc;
+    }
+}
+
+// x += sum_{j < i} y[j] Z[j] (latest direction first, as the host update)
+__global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, double *const *__restrict__ Z,
+                                                            const GgState *st, const double *__restrict__ y,
+                                                            double *__restrict__ x) {
+    __shared__ const double *zs[kGgMaxK];
+    __shared__ double ys[kGgMaxK];
+    const int i = st->i;
+    if (i == 0) return;
+    for (int k = threadIdx.x; k < i; k += kThreads) {
+        zs[k] = Z[k];
+        ys[k] = y[k];
+    }
+    __syncthreads();
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
+        double xe = x[e];
+        for (int j = i - 1; j >= 0; --j) xe = fma(ys[j], zs[j][e], xe);
+        x[e] = xe;
+    }
+}
+
+__global__ void summary_kernel(const GgState *st, const int *kerr, const int *aerr, double *out) {
+    const GgState &s = *st;
+    out[0] = s.iter;
+    out[1] = s.converged;
+    out[2] = s.rel;
+    out[3] = s.status;
+    out[4] = (double)s.t_start;
+    out[5] = (double)s.t_end;
+    out[6] = s.cycles;
+    out[7] = (kerr ? *kerr : 0) + (aerr ? *aerr : 0);
+}
+
+// Adds a WHILE node after the nodes captured so far on s and continues the
+// capture after it; returns its body graph.
+cudaGraph_t add_while(cudaStream_t s, cudaGraphConditionalHandle h) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    JX_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) {
+        set_error("graph gmres: stream is not capturing");
+        throw CudaError{cudaErrorStreamCaptureInvalidated, "capture"};
+    }
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    JX_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    JX_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return body;
+}
+
+cudaGraph_t capture_graph(cudaStream_t s) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    JX_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive) {
+        set_error("graph gmres: stream is not capturing");
+        throw CudaError{cudaErrorStreamCaptureInvalidated, "capture"};
+    }
+    return g;
+}
+
+void end_capture_quietly(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!s || cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs == cudaStreamCaptureStatusNone) return;
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+}
+
+}  // namespace gg
+
+GraphGmres::~GraphGmres() {
+    reset_graph();
+    for (auto &a : aux)
+        if (a) cudaStreamDestroy(a);
+}
+
+void GraphGmres::reset_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+}
+
+void GraphGmres::prepare(Solver &S) {
+    const SolverParams &prm = S.prm;
+    if (prm.k_dim < 1 || prm.k_dim > kGgMaxK) {
+        set_error("graph gmres: k_dim must be in 1..%d", kGgMaxK);
+        throw std::invalid_argument("k_dim");
+    }
+    if (!S.cpr.fast || prm.stage1_solver_type != 1 || S.ext_precond) {
+        set_error("graph gmres needs the fast CPR preconditioner (smoother_order 1, stage1_solver_type 1)");
+        throw std::invalid_argument("graph gmres");
+    }
+    n = (long long)S.A.nb * S.A.bs;
+    k = prm.k_dim;
+    max_iter = prm.max_iter;
+    const long long nn = n > 0 ? n : 1;
+    G = std::max(1, std::min(2 * sm_count(), div_up(nn, gg::kThreads * 4)));
+    G1 = std::max(1, std::min(8 * sm_count(), div_up(nn, gg::kThreads)));
+    state.alloc(1);
+    // work: rs (k+1), c (k), sn (k), h1 (k+2), h2 (k+2), y (k), hh ((k+1) k)
+    const size_t wsz = (size_t)(k + 1) + 2 * k + 2 * (k + 2) + k + (size_t)(k + 1) * k;
+    work.alloc(wsz);
+    double *wp = work.get();
+    W.rs = wp;
+    W.c = W.rs + (k + 1);
+    W.sn = W.c + k;
+    W.h1 = W.sn + k;
+    W.h2 = W.h1 + (k + 2);
+    W.y = W.h2 + (k + 2);
+    W.hh = W.y + k;
+    partials.alloc((size_t)(k + 2) * G);
+    norms.alloc((size_t)max_iter + 2);
+    summary.alloc(8);
+    cin.alloc(nn);
+    cout.alloc(nn);
+    // basis: the host GMRES's vectors are reused (same sizes); flexible directions as well if present
+    Gmres &g = S.gmres;
+    if ((int)g.p.size() < k + 1) {
+        set_error("graph gmres: basis not allocated");
+        throw CudaError{cudaErrorInvalidValue, "basis"};
+    }
+    std::vector<double *> vp, zp;
+    for (int j = 0; j <= k; ++j) vp.push_back(g.p[j].get());
+    own_z.clear();
+    if ((int)g.zf.size() >= k) {
+        for (int j = 0; j < k; ++j) zp.push_back(g.zf[j].get());
+    } else {
+        for (int j = 0; j < k; ++j) {
+            own_z.emplace_back((size_t)nn);
+            zp.push_back(own_z.back().get());
+        }
+    }
+    cudaStream_t s = S.stream;
+    vptr.alloc(vp.size());
+    vptr.upload(vp.data(), vp.size(), s);
+    zptr.alloc(zp.size());
+    zptr.upload(zp.data(), zp.size(), s);
+    for (auto &a : aux)
+        if (!a) JX_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    P.k = k;
+    P.max_iter = prm.max_iter;
+    P.min_iter = prm.min_iter;
+    P.check_restarted = prm.is_check_restarted;
+    P.tol = prm.tol;
+    P.a_tol = prm.a_tol;
+    P.convfac = prm.convfac_threshold;
+    JX_CUDA(cudaStreamSynchronize(s));
+    reset_graph();
+}
+
+bool GraphGmres::matches(const SolverParams &prm) const {
+    return prm.k_dim == P.k && prm.max_iter == P.max_iter && prm.min_iter == P.min_iter &&
+           prm.is_check_restarted == P.check_restarted && prm.tol == P.tol && prm.a_tol == P.a_tol &&
+           prm.convfac_threshold == P.convfac;
+}
+
+void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
+    using namespace gg;
+    const long long nn = n;
+    const BsrView<double> A = S.A.view();
+    const bool staged = S.prm.use_tma_spmv != 0;
+    int *kerr = S.kerr.get();
+    double *b = S.b.get(), *x = S.x.get(), *r = S.gmres.r.get(), *w = S.gmres.w.get();
+    double *const *V = vptr.get();
+    double *const *Z = zptr.get();
+    GgState *st = state.get();
+    double *pt = partials.get();
+    const unsigned long long c0 = launch_count();
+    unsigned long long c1 = c0, c2 = c0, c3 = c0, c4 = c0;
+    try {
+        if (S.prm.decouple)
+            bsr_decouple_rhs(S.A.nb, S.A.bs, S.prm.decouple, S.dcoef.get(), b, S.prm.consistent_rhs, s);
+        sq_partials<<<G, kThreads, 0, s>>>(nn, b, pt);
+        JX_LAUNCH_CHECK();
+        init_kernel<<<1, kRedThreads, 0, s>>>(st, pt, G);
+        JX_LAUNCH_CHECK();
+        cudaGraphConditionalHandle h_out = 0, h_in = 0;
+        JX_CUDA(cudaGraphConditionalHandleCreate(&h_out, capture_graph(s), 1, cudaGraphCondAssignDefault));
+        cudaGraph_t body_out = add_while(s, h_out);
+        c1 = launch_count();
+        cudaStream_t s1 = aux[0], s2 = aux[1];
+        JX_CUDA(cudaStreamBeginCaptureToGraph(s1, body_out, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        JX_CUDA(cudaGraphConditionalHandleCreate(&h_in, body_out, 0, cudaGraphCondAssignDefault));
+        copy_dev(nn, b, r, s1);
+        bsr_spmv<double, double>(A, -1.0, x, 1.0, r, kerr, s1, staged);
+        sq_partials<<<G, kThreads, 0, s1>>>(nn, r, pt);
+        JX_LAUNCH_CHECK();
+        restart_kernel<<<1, kRedThreads, 0, s1>>>(st, pt, G, P, W, norms.get(), h_out, h_in);
+        JX_LAUNCH_CHECK();
+        scale0_kernel<<<G1, kThreads, 0, s1>>>(nn, r, V, st);
+        JX_LAUNCH_CHECK();
+        cudaGraph_t body_in = add_while(s1, h_in);
+        c2 = launch_count();
+        JX_CUDA(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        gather_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, cin.get());
+        JX_LAUNCH_CHECK();
+        S.cpr.apply_enqueue(cin.get(), cout.get(), s2);
+        scatter_kernel<<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st);
+        JX_LAUNCH_CHECK();
+        bsr_spmv<double, double>(A, 1.0, cout.get(), 0.0, w, kerr, s2, staged);
+        dots_kernel<<<dim3(G, k + 2), kThreads, 0, s2>>>(nn, V, st, w, 0, pt);
+        JX_LAUNCH_CHECK();
+        reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, W.h1);
+        JX_LAUNCH_CHECK();
+        update_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h1, w);
+        JX_LAUNCH_CHECK();
+        dots_kernel<<<dim3(G, k + 2), kThreads, 0, s2>>>(nn, V, st, w, 1, pt);
+        JX_LAUNCH_CHECK();
+        arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, P, W, norms.get(), h_in);
+        JX_LAUNCH_CHECK();
+        final_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h2, w);
+        JX_LAUNCH_CHECK();
+        cudaGraph_t gchk = nullptr;
+        JX_CUDA(cudaStreamEndCapture(s2, &gchk));
+        c3 = launch_count();
+        update_x_kernel<<<G1, kThreads, 0, s1>>>(nn, Z, st, W.y, x);
+        JX_LAUNCH_CHECK();
+        JX_CUDA(cudaStreamEndCapture(s1, &gchk));
+        c4 = launch_count();
+        summary_kernel<<<1, 1, 0, s>>>(st, kerr, S.cpr.amg.err.get(), out);
+        JX_LAUNCH_CHECK();
+    } catch (...) {
+        end_capture_quietly(aux[1]);
+        end_capture_quietly(aux[0]);
+        uncount_launches(launch_count() - c0);
+        throw;
+    }
+    const unsigned long long c5 = launch_count();
+    kernels_step = c3 - c2;
+    kernels_cycle = (c2 - c1) + (c4 - c3);
+    kernels_fixed = (c1 - c0) + (c5 - c4);
+    uncount_launches(c5 - c0);
+}
+
+void GraphGmres::build_single(Solver &S) {
+    reset_graph();
+    cudaStream_t cs = nullptr;
+    JX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    try {
+        JX_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        try {
+            record(S, cs, summary.get());
+        } catch (...) {
+            gg::end_capture_quietly(cs);
+            throw;
+        }
+        JX_CUDA(cudaStreamEndCapture(cs, &graph));
+        JX_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    } catch (...) {
+        cudaStreamDestroy(cs);
+        reset_graph();
+        throw;
+    }
+    cudaStreamDestroy(cs);
+}
+
+unsigned long long GraphGmres::kernels_run(int iterations, int cycles) const {
+    return kernels_fixed + (unsigned long long)cycles * kernels_cycle + (unsigned long long)iterations * kernels_step;
+}
+
+GmresResult GraphGmres::result_from(const double *sm, cudaStream_t s, bool with_norms) {
+    GmresResult res;
+    res.iterations = (int)sm[0];
+    res.converged = (int)sm[1];
+    res.rel_residual = sm[2];
+    res.status = sm[3] != 0.0 ? JXCPR_ERROR_GENERIC : 0;
+    if (with_norms) {
+        res.norms.assign((size_t)res.iterations + 1, 0.0);
+        JX_CUDA(cudaMemcpyAsync(res.norms.data(), norms.get(), sizeof(double) * (res.iterations + 1),
+                                cudaMemcpyDeviceToHost, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+    }
+    return res;
+}
+
+}  // namespace jxcpr

@@ -118,6 +118,15 @@ void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
     bilu_stage(r, z, s);
 }
 
+void CprPrecond::apply_enqueue(const double *r, double *z, cudaStream_t s) {
+    if (!fast) {
+        set_error("apply_enqueue: needs the fast CPR preconditioner");
+        throw CudaError{cudaErrorInvalidValue, "apply_enqueue"};
+    }
+    fast->apply_enqueue(r, z, s);
+    bilu_stage(r, z, s);
+}
+
 // Stage 2 as a block-ILU(0) correction: r' = r - A z, z += BILU^-1 r'
 // (the composition of JXF_CPRPrecond without stage-2 sweeps, jxf_ParBSRMatrixMatvec
 // and jxf_BILUSolve that the reference's drivers use).
@@ -520,6 +529,7 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     }
     cudaStream_t s = stream;
     auto t0 = std::chrono::steady_clock::now();
+    ggmres.reset();  // its graph holds the previous setup's buffers
     A.alloc(nb, bs, nnzb);
     const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     JX_CUDA(cudaMemcpyAsync(A.ia.get(), ia, sizeof(int) * (nb + 1), kind, s));
@@ -599,6 +609,30 @@ GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
     const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     JX_CUDA(cudaMemcpyAsync(b.get(), b_in, sizeof(double) * n, in, s));
     JX_CUDA(cudaMemcpyAsync(x.get(), x_io, sizeof(double) * n, in, s));
+    if (prm.graph_gmres) {
+        if (!ggmres) ggmres.reset(new GraphGmres());
+        if (!ggmres->exec || !ggmres->matches(prm)) {
+            ggmres->prepare(*this);
+            ggmres->build_single(*this);
+        }
+        double sm[8];
+        JX_CUDA(cudaGraphLaunch(ggmres->exec, s));
+        JX_CUDA(cudaMemcpyAsync(sm, ggmres->summary.get(), sizeof(sm), cudaMemcpyDeviceToHost, s));
+        const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        JX_CUDA(cudaMemcpyAsync(x_io, x.get(), sizeof(double) * n, out, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+        last = ggmres->result_from(sm, s, true);
+        count_launches(ggmres->kernels_run(last.iterations, (int)sm[6]));
+        if (sm[7] != 0.0) {
+            set_error("device wait timed out (spmv / smoother flags set)");
+            last.status = JXCPR_ERROR_DEVICE;
+            kerr.zero(s);
+            cpr.amg.err.zero(s);
+            JX_CUDA(cudaStreamSynchronize(s));
+        }
+        solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return last;
+    }
     if (prm.decouple) bsr_decouple_rhs(A.nb, A.bs, prm.decouple, dcoef.get(), b.get(), prm.consistent_rhs, s);
     gmres.prm = prm;
     cpr.prm.stage2_maxit = prm.stage2_maxit;

@@ -62,6 +62,7 @@ struct SolverParams {
     int graphs = 1;          // fast path: each CPR application replays one captured CUDA graph
     int orthog = 0;          // 0 modified Gram-Schmidt (the reference's), 1 classical Gram-Schmidt (one pass)
     int flexible = 0;        // 1: flexible GMRES (stores M^-1 v_j; for inexact / low-precision preconditioners)
+    int graph_gmres = 0;     // 1: the whole GMRES solve on the device as one CUDA graph (fast path; flexible, CGS2)
     double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
     double cheb_upper = 1.1;
     int stage2_lanes = 4;
@@ -110,6 +111,8 @@ struct CprPrecond {
     // one stage-2 block hybrid Gauss-Seidel sweep on A z = r (z in/out)
     void stage2_sweep(const double *r, double *z, cudaStream_t s);
     void bilu_stage(const double *r, double *z, cudaStream_t s);
+    // apply() with every kernel queued on s (fast path only; no private graph), for capture
+    void apply_enqueue(const double *r, double *z, cudaStream_t s);
     // one pressure V-cycle on A_p u = f, u in/out (FP64)
     void vcycle(const double *f, double *u, cudaStream_t s);
     int *err() { return amg.err.get(); }
@@ -140,6 +143,56 @@ struct Gmres {
                       const std::function<void(const double *, double *)> *ext = nullptr);
 };
 
+struct Solver;
+
+// Device-side state of the graph GMRES (one per solve).
+constexpr int kGgMaxK = 64;
+struct GgState {
+    int i, m, iter, cycles;
+    int converged, done, status, first;
+    int est_conv, conv_fail, cont, pad;
+    double b_norm, r_norm, r_norm0, epsilon, normdown, scale, rel;
+    unsigned long long t_start, t_end;  // device global timer (ns) at the solve's start and end
+};
+struct GgParams {
+    int k, max_iter, min_iter, check_restarted;
+    double tol, a_tol, convfac;
+};
+struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
+    double *rs, *c, *sn, *h1, *h2, *y, *hh;
+};
+
+// Restarted flexible GMRES(k) run on the device without host round trips:
+// the whole solve is recorded into a CUDA graph (nested conditional WHILE
+// nodes for the restart cycles and the Arnoldi steps).  Single-system solves
+// replay a graph of their own; batches record many solvers into one graph.
+struct GraphGmres {
+    long long n = 0;
+    int k = 0, max_iter = 0, G = 1, G1 = 1;
+    GgParams P{};
+    GgWork W{};
+    DevBuf<GgState> state;
+    DevBuf<double> work, partials, norms, summary, cin, cout;
+    std::vector<DevBuf<double>> own_z;  // flexible directions when the host GMRES keeps none
+    DevBuf<double *> vptr, zptr;
+    cudaStream_t aux[2] = {nullptr, nullptr};  // capture streams of the loop bodies
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels_fixed = 0, kernels_cycle = 0, kernels_step = 0;
+    ~GraphGmres();
+    void reset_graph();
+    // buffers and parameters for the solver's current setup (throws if it has no fast CPR)
+    void prepare(Solver &S);
+    bool matches(const SolverParams &prm) const;
+    // Records decoupling of S.b, the solve of A x = b into S.x and an 8-value
+    // summary written to `out` into the capture running on s.
+    void record(Solver &S, cudaStream_t s, double *out);
+    void build_single(Solver &S);
+    unsigned long long kernels_run(int iterations, int cycles) const;
+    // summary: iterations, converged, rel. residual, status, t_start, t_end, cycles, device error flags
+    GmresResult result_from(const double *summary_host, cudaStream_t s, bool with_norms);
+};
+
 // Full solver object: owns the device matrix, decoupling coefficients, CPR, GMRES.
 struct Solver {
     SolverParams prm;
@@ -156,6 +209,7 @@ struct Solver {
     GmresResult last;
     // a preconditioner supplied by the caller instead of CPR (stage1_solver_type 0 then applies it)
     std::function<void(const double *, double *)> ext_precond;
+    std::unique_ptr<GraphGmres> ggmres;  // graph_gmres 1
     // A on the host or the device (device = 1), copied into the solver.
     void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);
     // b, x host or device; x holds the initial guess on entry.

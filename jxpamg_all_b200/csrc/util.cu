@@ -26,6 +26,7 @@ const char *last_error() { return g_err; }
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---- device memory cache --------------------------------------------------

@@ -28,7 +28,7 @@ class CprGmres:
     pressure_index, stage1_maxit, stage2_maxit, stage1_solver_type,
     stage2_solver_type, decouple, consistent_rhs, smoother_order, coarse_exact,
     use_tma_spmv, precision, bf16_level, fast_smoother, stage2_lanes,
-    learned_fallback, record_features.  Real options: tol, a_tol, threshold,
+    learned_fallback, record_features, flexible, graph_gmres.  Real options: tol, a_tol, threshold,
     convfac_threshold, stage2_relax_weight, stage2_omega, strong_threshold,
     cheb_lower, cheb_upper.
 
@@ -36,6 +36,8 @@ class CprGmres:
     the reference); 1 the throughput path, whose precision (0 FP64, 1 FP32,
     2 FP32 + BF16 coarse levels) and fast_smoother (0 multicolour GS /
     l1-Jacobi, 1 Chebyshev-3, 2 learned) select the mixed and learned forms.
+    graph_gmres 1 runs the whole GMRES solve on the device as one CUDA graph
+    (fast path only).
     """
 
     def __init__(self, **options):
@@ -183,6 +185,70 @@ class CprGmres:
     def close(self):
         if getattr(self, "h", None):
             self._so.jxcpr_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CprGmresBatch:
+    """Many set-up CprGmres solvers solved by one CUDA-graph launch.
+
+    Each solver's whole GMRES solve is recorded as an independent branch of a
+    single graph (graph_gmres mode: flexible GMRES, CGS2, device-side loop
+    control).  The solvers must stay alive and unchanged while the batch is
+    used.
+    """
+
+    def __init__(self, solvers):
+        self._so = _lib.load()
+        self.solvers = list(solvers)
+        self.sizes = [s.nb * s.bs for s in self.solvers]
+        arr = (ctypes.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        h = ctypes.c_void_p()
+        _lib.check(self._so.jxcpr_batch_create(ctypes.byref(h), len(self.solvers), arr))
+        self.h = h
+
+    def solve(self, bs, x0s=None, device=False):
+        """Solves every system; returns dict of per-system arrays and the list of x.
+
+        Host numpy arrays, or device pointers (ints) with device=True (then x0s
+        are overwritten with the solutions)."""
+        m = len(self.solvers)
+        if device:
+            bp = (ctypes.c_void_p * m)(*bs)
+            xp = (ctypes.c_void_p * m)(*x0s)
+            xs = list(x0s)
+        else:
+            bb = [np.ascontiguousarray(b, np.float64) for b in bs]
+            xs = [np.zeros(n) if x0s is None else np.array(x0s[k], dtype=np.float64) for k, n in enumerate(self.sizes)]
+            bp = (ctypes.c_void_p * m)(*[b.ctypes.data for b in bb])
+            xp = (ctypes.c_void_p * m)(*[x.ctypes.data for x in xs])
+        it = np.zeros(m, np.int32)
+        rel = np.zeros(m)
+        lat = np.zeros(m)
+        fin = np.zeros(m)
+        st = np.zeros(m, np.int32)
+        rc = self._so.jxcpr_batch_solve(self.h, bp, xp, 1 if device else 0, _ptr(it), _ptr(rel), _ptr(lat),
+                                        _ptr(fin), _ptr(st))
+        if rc not in (0, STATUS_CONV):
+            _lib.check(rc)
+        return dict(x=xs, iterations=it, rel_residual=rel, latency_ms=lat, finish_ms=fin, status=st)
+
+    def last_ms(self):
+        v = np.zeros(1)
+        _lib.check(self._so.jxcpr_batch_last_ms(self.h, _ptr(v)))
+        return float(v[0])
+
+    def launch(self, stream_handle=0):
+        _lib.check(self._so.jxcpr_batch_launch(self.h, ctypes.c_void_p(stream_handle)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._so.jxcpr_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -31,7 +31,7 @@ import dataclasses
 
 import numpy as np
 
-__all__ = ["BSRSystem", "reservoir_system", "config_system", "CONFIGS"]
+__all__ = ["BSRSystem", "reservoir_system", "config_system", "CONFIGS", "batch_grids", "batch_systems"]
 
 
 @dataclasses.dataclass
@@ -235,3 +235,25 @@ CONFIGS = {
 def config_system(name: str) -> BSRSystem:
     nx, ny, nz, ph, ch, seed = CONFIGS[name]
     return reservoir_system(nx, ny, nz, seed, phases=ph, channelised_layers=ch)
+
+
+# Batched-solve workload: independent two-phase systems built as the 8,000-cell
+# log-normal case, system k with seed k, grid sizes drawn uniformly per axis
+# between these corners (about 2K to 264K cells).
+BATCH_GRID_MIN = (16, 16, 8)
+BATCH_GRID_MAX = (60, 110, 40)
+BATCH_SIZE_SEED = 2024
+
+
+def batch_grids(count=64, size_seed=BATCH_SIZE_SEED, grid_min=BATCH_GRID_MIN, grid_max=BATCH_GRID_MAX):
+    """The (nx, ny, nz) of each system of the batch, drawn from their own seeded generator."""
+    rng = np.random.default_rng(size_seed)
+    lo, hi = np.array(grid_min), np.array(grid_max)
+    return [tuple(int(v) for v in rng.integers(lo, hi + 1)) for _ in range(count)]
+
+
+def batch_systems(count=64, first_seed=0, size_seed=BATCH_SIZE_SEED, grid_min=BATCH_GRID_MIN,
+                  grid_max=BATCH_GRID_MAX):
+    """`count` independent 2x2 systems of uneven size (system k: seed first_seed + k)."""
+    return [reservoir_system(nx, ny, nz, first_seed + k)
+            for k, (nx, ny, nz) in enumerate(batch_grids(count, size_seed, grid_min, grid_max))]
