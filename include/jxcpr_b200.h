@@ -189,7 +189,8 @@ JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
  * graph launch for all systems.  Per system: iterations, FP64 relative residual, latency_ms = its own
  * solve time on the device, finish_ms = completion time since the first system started, status
  * (0, 256 not converged, 512 device error).  Returns 0, or the first error other than 256.
- * last_ms: device time of the last launch (CUDA events).  launch: the graph alone on `stream` (NULL:
+ * last_ms: device time of the last solve (CUDA events around the input copies, the launch and the output
+ * copies).  launch: the graph alone on `stream` (NULL:
  * the batch's own), with the inputs already in the solvers' buffers. */
 typedef struct jxcpr_batch jxcpr_batch;
 JXCPR_API int jxcpr_batch_create(jxcpr_batch **batch, int nsys, jxcpr_solver *const *solvers);

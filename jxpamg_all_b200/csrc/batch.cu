@@ -142,20 +142,20 @@ int jxcpr_batch_solve(jxcpr_batch *h, const double *const *b, double *const *x, 
         cudaStream_t s = h->s0;
         const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
         const cudaMemcpyKind outk = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        JX_CUDA(cudaEventRecord(h->t0, s));
         for (int k = 0; k < nsys; ++k) {
             Solver &S = *h->sys[k];
             const size_t bytes = sizeof(double) * (size_t)S.A.nb * S.A.bs;
             JX_CUDA(cudaMemcpyAsync(S.b.get(), b[k], bytes, in, s));
             JX_CUDA(cudaMemcpyAsync(S.x.get(), x[k], bytes, in, s));
         }
-        JX_CUDA(cudaEventRecord(h->t0, s));
         JX_CUDA(cudaGraphLaunch(h->exec, s));
-        JX_CUDA(cudaEventRecord(h->t1, s));
         for (int k = 0; k < nsys; ++k) {
             Solver &S = *h->sys[k];
             const size_t bytes = sizeof(double) * (size_t)S.A.nb * S.A.bs;
             JX_CUDA(cudaMemcpyAsync(x[k], S.x.get(), bytes, outk, s));
         }
+        JX_CUDA(cudaEventRecord(h->t1, s));
         JX_CUDA(cudaMemcpyAsync(h->sm_host.data(), h->summary.get(), sizeof(double) * 8 * nsys,
                                 cudaMemcpyDeviceToHost, s));
         JX_CUDA(cudaStreamSynchronize(s));

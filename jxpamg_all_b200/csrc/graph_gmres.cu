@@ -35,6 +35,7 @@ namespace gg {
 
 constexpr int kThreads = 256;
 constexpr int kRedThreads = 1024;
+constexpr int kSlice = 2048;  // elements per block of the Gram products
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -169,20 +170,36 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, const do
         dst[e] = src[e];
 }
 
-// Block (x, k): partial <V[k], w> over the x-th slice, k <= i (k = i + 1 with
-// self: <w, w>).  Blocks beyond the current basis size return at once.
+// Block x: partial <V[k], w> over the x-th slice of kSlice elements for every
+// k <= i (and <w, w> in row i + 1 with self).  The slice of w is staged in
+// shared memory once and each basis vector is streamed past it; warps reduce
+// with shuffles and combine through shared memory once at the end.
 __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const double *const *__restrict__ V,
                                                         const GgState *st, const double *__restrict__ w, int self,
                                                         double *__restrict__ partials) {
-    __shared__ double sh[32];
-    const int k = blockIdx.y, m = st->i + 1;
-    if (k > m || (k == m && !self)) return;
-    const double *v = k == m ? w : V[k];
-    double acc = 0.0;
-    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
-        acc = fma(v[e], w[e], acc);
-    acc = block_sum(acc, sh);
-    if (threadIdx.x == 0) partials[(long long)k * gridDim.x + blockIdx.x] = acc;
+    __shared__ double ws[kSlice];
+    __shared__ double part[kGgMaxK + 2][kThreads / 32];
+    const long long e0 = (long long)blockIdx.x * kSlice;
+    const int len = (int)min((long long)kSlice, n - e0);
+    for (int j = threadIdx.x; j < len; j += kThreads) ws[j] = w[e0 + j];
+    __syncthreads();
+    const int m = st->i + 1, kend = self ? m + 1 : m;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < kend; ++k) {
+        const double *v = k < m ? V[k] + e0 : ws;
+        double acc = 0.0;
+        for (int j = threadIdx.x; j < len; j += kThreads) acc = fma(v[j], ws[j], acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) part[k][warp] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < kend) {
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) v += part[threadIdx.x][q];
+        partials[(long long)threadIdx.x * gridDim.x + blockIdx.x] = v;
+    }
 }
 
 // h[k] = sum of partials row k, k <= i (one warp per row)
@@ -424,7 +441,7 @@ void GraphGmres::prepare(Solver &S) {
     k = prm.k_dim;
     max_iter = prm.max_iter;
     const long long nn = n > 0 ? n : 1;
-    G = std::max(1, std::min(2 * sm_count(), div_up(nn, gg::kThreads * 4)));
+    G = div_up(nn, gg::kSlice);  // blocks of the Gram products and norms: one slice each
     G1 = std::max(1, std::min(8 * sm_count(), div_up(nn, gg::kThreads)));
     state.alloc(1);
     // work: rs (k+1), c (k), sn (k), h1 (k+2), h2 (k+2), y (k), hh ((k+1) k)
@@ -528,13 +545,13 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         scatter_kernel<<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st);
         JX_LAUNCH_CHECK();
         bsr_spmv<double, double>(A, 1.0, cout.get(), 0.0, w, kerr, s2, staged);
-        dots_kernel<<<dim3(G, k + 2), kThreads, 0, s2>>>(nn, V, st, w, 0, pt);
+        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, 0, pt);
         JX_LAUNCH_CHECK();
         reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, W.h1);
         JX_LAUNCH_CHECK();
         update_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h1, w);
         JX_LAUNCH_CHECK();
-        dots_kernel<<<dim3(G, k + 2), kThreads, 0, s2>>>(nn, V, st, w, 1, pt);
+        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, 1, pt);
         JX_LAUNCH_CHECK();
         arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, P, W, norms.get(), h_in);
         JX_LAUNCH_CHECK();

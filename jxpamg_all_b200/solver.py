@@ -238,7 +238,25 @@ class CprGmresBatch:
             _lib.check(rc)
         return dict(x=xs, iterations=it, rel_residual=rel, latency_ms=lat, finish_ms=fin, status=st)
 
+    def solve_ptrs(self, b_ptrs, x_ptrs, device):
+        """Raw form of solve(): b_ptrs / x_ptrs are addresses (host with device=False, e.g. pinned
+        buffers, or device); returns the per-system arrays only."""
+        m = len(self.solvers)
+        bp = (ctypes.c_void_p * m)(*b_ptrs)
+        xp = (ctypes.c_void_p * m)(*x_ptrs)
+        it = np.zeros(m, np.int32)
+        rel = np.zeros(m)
+        lat = np.zeros(m)
+        fin = np.zeros(m)
+        st = np.zeros(m, np.int32)
+        rc = self._so.jxcpr_batch_solve(self.h, bp, xp, 1 if device else 0, _ptr(it), _ptr(rel), _ptr(lat),
+                                        _ptr(fin), _ptr(st))
+        if rc not in (0, STATUS_CONV):
+            _lib.check(rc)
+        return dict(iterations=it, rel_residual=rel, latency_ms=lat, finish_ms=fin, status=st)
+
     def last_ms(self):
+        """Device time of the last solve: input copies, the graph launch and the output copies."""
         v = np.zeros(1)
         _lib.check(self._so.jxcpr_batch_last_ms(self.h, _ptr(v)))
         return float(v[0])
