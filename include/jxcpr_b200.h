@@ -42,9 +42,14 @@ JXCPR_API int jxcpr_version(void);
 JXCPR_API unsigned long long jxcpr_launch_count(void);
 /* Message describing the calling thread's last failure ("" if none). */
 JXCPR_API const char *jxcpr_last_error(void);
-/* The library keeps freed device blocks for reuse (a freed block is handed out again only after a
- * device synchronisation); this returns every cached block to the driver. */
+/* The library keeps freed device blocks for reuse: a block made for a solver is reused on that
+ * solver's stream at once (stream order), any other block only after a device synchronisation;
+ * small blocks are carved from 32 MiB slabs.  This returns every idle block (and the slabs, once
+ * none of their blocks is in use) to the driver. */
 JXCPR_API int jxcpr_release_cached_memory(void);
+/* out[4] = {cudaMalloc calls, their total ms, device synchronisations of the cache, their total ms}
+ * since the library was loaded. */
+JXCPR_API int jxcpr_pool_stats(double *out);
 
 /* ---- BSR SpMV ------------------------------------------------------------
  * y = alpha*A*x + beta*y for a block-CSR matrix with bs x bs row-major blocks
@@ -192,6 +197,14 @@ JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
  * last_ms: device time of the last solve (CUDA events around the input copies, the launch and the output
  * copies).  launch: the graph alone on `stream` (NULL:
  * the batch's own), with the inputs already in the solvers' buffers. */
+/* batch_setup: jxcpr_solver_setup of system k (nb[k], bs[k], nnzb[k], ia[k], ja[k], a[k]; host arrays, or
+ * device arrays with device = 1) for every k on `threads` host threads (<= 0: one per core), each
+ * solver on its own stream.  Batches with an exact-order (smoother_order 0) or BILU (stage2_solver_type
+ * 5) solver are set up one system after another.  status[k] (may be NULL) gets each setup's code;
+ * returns the first failure (its message names the system) or 0. */
+JXCPR_API int jxcpr_batch_setup(int nsys, jxcpr_solver *const *solvers, const int *nb, const int *bs,
+                                const long long *nnzb, const int *const *ia, const int *const *ja,
+                                const double *const *a, int device, int threads, int *status);
 typedef struct jxcpr_batch jxcpr_batch;
 JXCPR_API int jxcpr_batch_create(jxcpr_batch **batch, int nsys, jxcpr_solver *const *solvers);
 JXCPR_API int jxcpr_batch_destroy(jxcpr_batch *batch);

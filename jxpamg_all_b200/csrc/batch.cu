@@ -8,6 +8,9 @@
 // times come from the device global timer at each branch's start and end.
 // No counterpart in the reference.
 #include <algorithm>
+#include <atomic>
+#include <string>
+#include <thread>
 #include <stdexcept>
 #include <memory>
 #include <vector>
@@ -71,6 +74,51 @@ void end_capture_quietly(cudaStream_t s) {
 
 extern "C" {
 
+int jxcpr_batch_setup(int nsys, jxcpr_solver *const *solvers, const int *nb, const int *bs, const long long *nnzb,
+                      const int *const *ia, const int *const *ja, const double *const *a, int device, int threads,
+                      int *status) {
+    if (nsys < 0 || (nsys > 0 && (!solvers || !nb || !bs || !nnzb || !ia || !ja || !a))) return JXCPR_ERROR_ARG;
+    if (nsys == 0) return JXCPR_SUCCESS;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        set_error("batch_setup: no current CUDA device");
+        return JXCPR_ERROR_DEVICE;
+    }
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    // The exact-order smoothers share one grid barrier per device and the BILU
+    // stage was not written for concurrent setups: such batches set up in turn.
+    for (int k = 0; k < nsys; ++k)
+        if (solvers[k] && (solvers[k]->s.prm.smoother_order == ORDER_EXACT || solvers[k]->s.prm.stage2_solver_type == 5))
+            threads = 1;
+    threads = std::min(threads, nsys);
+    std::vector<int> st(nsys, JXCPR_SUCCESS);
+    std::vector<std::string> msg(nsys);
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= nsys) break;
+            st[k] = solvers[k] ? jxcpr_solver_setup(solvers[k], nb[k], bs[k], nnzb[k], ia[k], ja[k], a[k], device)
+                               : JXCPR_ERROR_ARG;
+            if (st[k] != JXCPR_SUCCESS) msg[k] = last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
+    int worst = JXCPR_SUCCESS;
+    for (int k = 0; k < nsys; ++k) {
+        if (status) status[k] = st[k];
+        if (st[k] != JXCPR_SUCCESS && worst == JXCPR_SUCCESS) {
+            worst = st[k];
+            set_error("batch_setup: system %d: %s", k, msg[k].c_str());
+        }
+    }
+    return worst;
+}
+
 int jxcpr_batch_create(jxcpr_batch **out, int nsys, jxcpr_solver *const *solvers) {
     if (!out || nsys < 1 || !solvers) return JXCPR_ERROR_ARG;
     *out = nullptr;
@@ -85,6 +133,7 @@ int jxcpr_batch_create(jxcpr_batch **out, int nsys, jxcpr_solver *const *solvers
         B->sys.resize(nsys);
         for (int k = 0; k < nsys; ++k) B->sys[k] = &solvers[k]->s;
         for (Solver *S : B->sys) {
+            PoolStream scope(S->stream);
             S->prm.graph_gmres = 1;
             if (!S->ggmres) S->ggmres.reset(new GraphGmres());
             S->ggmres->prepare(*S);

@@ -109,6 +109,12 @@ int jxcpr_dot_dev(long long n, const double *x, const double *y, double *out_hos
 
 }  // extern "C"
 
+extern "C" int jxcpr_pool_stats(double *out) {
+    if (!out) return JXCPR_ERROR_ARG;
+    jxcpr::pool_stats(out);
+    return JXCPR_SUCCESS;
+}
+
 extern "C" int jxcpr_release_cached_memory(void) {
     try {
         jxcpr::pool_trim();

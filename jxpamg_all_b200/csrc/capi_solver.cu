@@ -115,16 +115,26 @@ int jxcpr_solver_create(jxcpr_solver **h) {
 int jxcpr_solver_destroy(jxcpr_solver *h) {
     if (!h) return JXCPR_ERROR_ARG;
     return guarded([&] {
-        cudaStream_t st = h->s.owns_stream ? h->s.stream : nullptr;
+        const bool owns = h->s.owns_stream;
+        cudaStream_t st = h->s.stream;
+        if (owns) cudaStreamSynchronize(st);
         delete h;
-        if (st) cudaStreamDestroy(st);
+        if (owns) {
+            pool_forget_stream(st);  // before a new stream can take the same handle
+            cudaStreamDestroy(st);
+        }
         return JXCPR_SUCCESS;
     });
 }
 
 int jxcpr_solver_set_stream(jxcpr_solver *h, void *stream) {
     if (!h) return JXCPR_ERROR_ARG;
-    if (h->s.owns_stream && h->s.stream) cudaStreamDestroy(h->s.stream);
+    // blocks made for the previous stream park when freed: the new stream's work is not ordered after it
+    pool_forget_stream(h->s.stream);
+    if (h->s.owns_stream && h->s.stream) {
+        cudaStreamSynchronize(h->s.stream);
+        cudaStreamDestroy(h->s.stream);
+    }
     h->s.stream = (cudaStream_t)stream;
     h->s.owns_stream = false;
     h->s.stream_set = true;
@@ -195,6 +205,10 @@ int jxcpr_solver_setup_report(jxcpr_solver *h, char *buf, int capacity) {
         out += line;
     }
     snprintf(line, sizeof line, "total %.2f ms\n", h->s.setup_ms);
+    out += line;
+    const double *al = h->s.alloc_stats;
+    snprintf(line, sizeof line, "device memory: %.0f cudaMalloc (%.2f ms), %.0f device syncs (%.2f ms)\n", al[0],
+             al[1], al[2], al[3]);
     out += line;
     if (h->s.cpr.fast)
         for (const std::string &t : h->s.cpr.fast->tune_log) out += "tuned " + t + "\n";

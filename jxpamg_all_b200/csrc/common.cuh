@@ -59,14 +59,32 @@ void count_launches(unsigned long long n);  // kernels replayed by a CUDA graph 
         JX_CUDA(cudaGetLastError());          \
     } while (0)
 
-// Device memory cache behind DevBuf.  A freed block is parked; it becomes
-// reusable only after a device synchronisation (the one cudaFree would have
-// done), so no work still queued on any stream can touch a block handed out
-// again.  Blocks are bucketed (powers of two up to 1 GiB, 256 MiB multiples
-// above); the cache is trimmed when it exceeds its limit or cudaMalloc fails.
+// Device memory cache behind DevBuf.  Blocks are bucketed (powers of two up
+// to 1 GiB, 256 MiB multiples above); buckets up to 1 MiB are carved from
+// 32 MiB slabs, so a setup makes few cudaMalloc calls.
+//  * Inside a PoolStream scope the thread's work goes to one stream: blocks
+//    are tagged with it, and a freed tagged block is reused at once by the
+//    next allocation under the same stream (stream order puts the new work
+//    after every earlier use), with no device synchronisation.
+//  * Other blocks are parked when freed and become reusable after a device
+//    synchronisation (the one cudaFree would have done).
+// pool_forget_stream(s) is called before a tagged stream is destroyed or
+// replaced: its idle blocks are parked and its live blocks park when freed.
 void *pool_alloc(size_t bytes);
 void pool_free(void *p);
 void pool_trim();
+void pool_forget_stream(cudaStream_t s);
+// process-wide: cudaMalloc calls, their total ms, device synchronisations, their total ms
+void pool_stats(double out[4]);
+
+struct PoolStream {
+    explicit PoolStream(cudaStream_t s);
+    ~PoolStream();
+    PoolStream(const PoolStream &) = delete;
+    PoolStream &operator=(const PoolStream &) = delete;
+    cudaStream_t prev;
+    bool prev_set;
+};
 
 // Owning device buffer (256-byte aligned, padded by 64 bytes so that
 // 16-byte-rounded bulk copies of the tail stay inside the allocation).

@@ -240,9 +240,16 @@ std::map<std::string, TuneChoice> &tune_cache() {
     static std::map<std::string, TuneChoice> *c = new std::map<std::string, TuneChoice>();
     return *c;
 }
-std::string tune_key(const char *name, int n, long long nnz, int kind, int E) {
+// mode 1: the exact shape; mode 2 (shared): the shape class -- rows within a
+// half octave, mean row length within 0.5 -- so similar operators of other
+// systems (a batch) reuse one timing.
+std::string tune_key(const char *name, int n, long long nnz, int kind, int E, int mode) {
     char k[160];
-    snprintf(k, sizeof k, "%s/%d/%lld/%d/%d", name, n, nnz, kind, E);
+    if (mode == 2 && n > 0)
+        snprintf(k, sizeof k, "%s/class/%d/%lld/%d/%d", name, (int)floor(2.0 * log2((double)n)),
+                 (long long)llround(2.0 * (double)nnz / n), kind, E);
+    else
+        snprintf(k, sizeof k, "%s/%d/%lld/%d/%d", name, n, nnz, kind, E);
     return k;
 }
 
@@ -257,7 +264,7 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
         build_level_mat(n, m, nnz, 1, ia, ja, a, kind, use_sell(opt, n, nnz), order, seg, order_dev, M, s);
         return;
     }
-    const std::string key = tune_key(name, n, nnz, kind, 1);
+    const std::string key = tune_key(name, n, nnz, kind, 1, opt.autotune);
     TuneChoice best;
     bool cached = false;
     {
@@ -821,7 +828,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
     if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
         const int kind = fp64 ? VAL_F64 : VAL_F32;
-        const std::string key = tune_key("stage2", A.nb, A.nnzb, kind, A.bs * A.bs);
+        const std::string key = tune_key("stage2", A.nb, A.nnzb, kind, A.bs * A.bs, opt.autotune);
         TuneChoice cached_choice;
         bool cached = false;
         if (opt.autotune) {

@@ -300,11 +300,16 @@ __global__ void __launch_bounds__(kCgsThreads) cgs_update_kernel(long long n, in
 
 void Gmres::setup(int n_, cudaStream_t s) {
     n = n_;
+    const size_t stride = ((size_t)(n > 0 ? n : 1) + 31) / 32 * 32;  // 256-byte aligned slices
+    const int nvec = prm.k_dim + 1 + (prm.flexible ? prm.k_dim : 0);
+    basis.alloc(stride * nvec);
     p.clear();
-    for (int i = 0; i <= prm.k_dim; ++i) p.emplace_back((size_t)(n > 0 ? n : 1));
     zf.clear();
-    if (prm.flexible)
-        for (int i = 0; i < prm.k_dim; ++i) zf.emplace_back((size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < nvec; ++i) {
+        VecRef v{basis.get() + stride * i};
+        if (i <= prm.k_dim) p.push_back(v);
+        else zf.push_back(v);
+    }
     r.alloc(n > 0 ? n : 1);
     w.alloc(n > 0 ? n : 1);
     cgs_blocks = std::max(1, std::min(4 * sm_count(), div_up(n > 0 ? n : 1, kCgsThreads)));
@@ -528,6 +533,9 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
         owns_stream = true;
     }
     cudaStream_t s = stream;
+    PoolStream scope(s);  // this setup's buffers are made for the solver's stream
+    double al0[4];
+    pool_stats(al0);
     auto t0 = std::chrono::steady_clock::now();
     ggmres.reset();  // its graph holds the previous setup's buffers
     A.alloc(nb, bs, nnzb);
@@ -560,6 +568,8 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     }
     JX_CUDA(cudaStreamSynchronize(s));
     setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    pool_stats(alloc_stats);
+    for (int i = 0; i < 4; ++i) alloc_stats[i] -= al0[i];
 }
 
 // Learned settings against the plain smoothers: a few GMRES iterations (tol 0)
@@ -604,6 +614,7 @@ void Solver::learned_probe(cudaStream_t s) {
 
 GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
     cudaStream_t s = stream;
+    PoolStream scope(s);
     const long long n = (long long)A.nb * A.bs;
     auto t0 = std::chrono::steady_clock::now();
     const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;

@@ -58,7 +58,7 @@ struct SolverParams {
     int bf16_level = 1;      // precision 2: first BF16 level
     int fast_smoother = 0;   // 0 colour GS / l1-Jacobi; 1 Chebyshev-3 on the levels without a GS colouring;
                              // 2 as 1 with learned thresholds and intervals; 3 Chebyshev-3 on every level
-    int autotune = 1;        // fast path: time the operator layouts at setup and keep the fastest
+    int autotune = 1;        // fast path: time the operator layouts at setup and keep the fastest (2: share per shape class)
     int graphs = 1;          // fast path: each CPR application replays one captured CUDA graph
     int orthog = 0;          // 0 modified Gram-Schmidt (the reference's), 1 classical Gram-Schmidt (one pass)
     int flexible = 0;        // 1: flexible GMRES (stores M^-1 v_j; for inexact / low-precision preconditioners)
@@ -131,8 +131,14 @@ struct GmresResult {
 struct Gmres {
     SolverParams prm;
     int n = 0;
-    std::vector<DevBuf<double>> p;
-    std::vector<DevBuf<double>> zf;       // flexible GMRES: z_j = M^-1 p_j
+    // Krylov basis p_0..p_k and (flexible GMRES) z_j = M^-1 p_j: slices of one allocation
+    struct VecRef {
+        double *ptr;
+        double *get() const { return ptr; }
+    };
+    DevBuf<double> basis;
+    std::vector<VecRef> p;
+    std::vector<VecRef> zf;
     DevBuf<double> r, w, partials, scal;  // scal: device scalars (dots)
     DevBuf<const double *> vptrs;         // device array of the basis pointers (classical Gram-Schmidt)
     int cgs_blocks = 1;
@@ -206,6 +212,7 @@ struct Solver {
     bool owns_stream = false;
     bool stream_set = false;  // the caller chose the stream (possibly the legacy default stream)
     double setup_ms = 0.0, solve_ms = 0.0, upload_ms = 0.0, decouple_ms = 0.0;
+    double alloc_stats[4] = {0, 0, 0, 0};  // during the last setup (process-wide): cudaMalloc calls / ms, device syncs / ms
     GmresResult last;
     // a preconditioner supplied by the caller instead of CPR (stage1_solver_type 0 then applies it)
     std::function<void(const double *, double *)> ext_precond;

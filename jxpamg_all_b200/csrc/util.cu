@@ -1,7 +1,9 @@
 // Error-message storage and device queries shared by the library.
 #include <stdarg.h>
 
+#include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -31,13 +33,34 @@ unsigned long long launch_count() { return g_launches.load(std::memory_order_rel
 
 // ---- device memory cache --------------------------------------------------
 namespace {
+thread_local cudaStream_t t_stream = nullptr;
+thread_local bool t_stream_set = false;
+
+constexpr size_t kSlabBucketMax = 1ull << 20;  // buckets carved from slabs
+constexpr size_t kSlabBytes = 32ull << 20;
+
+struct Block {
+    int dev;
+    size_t bucket;
+    bool tagged;
+    bool carved;
+    cudaStream_t stream;
+    unsigned long long epoch;
+};
+using TagKey = std::pair<int, std::pair<cudaStream_t, unsigned long long>>;
+
 struct MemPool {
     std::mutex mu;
-    std::map<int, std::multimap<size_t, void *>> idle;                  // per device: reusable blocks
-    std::map<int, std::vector<std::pair<size_t, void *>>> parked;       // freed since the last sync
-    std::unordered_map<void *, std::pair<int, size_t>> owner;          // block -> (device, bucket)
-    size_t cached = 0;                                                  // idle + parked bytes
+    std::map<int, std::multimap<size_t, void *>> idle;              // per device: reusable on any stream
+    std::map<TagKey, std::multimap<size_t, void *>> idle_tagged;     // reusable on their own stream
+    std::map<int, std::vector<std::pair<size_t, void *>>> parked;    // freed since the last device sync
+    std::unordered_map<void *, Block> owner;
+    std::map<cudaStream_t, unsigned long long> epoch;                // bumped by pool_forget_stream
+    std::map<int, std::vector<void *>> slabs;
+    std::map<int, std::pair<char *, size_t>> slab_cur;               // bump pointer, bytes left
+    size_t cached = 0;                                               // idle + parked bytes, not carved
     size_t limit = 24ull << 30;
+    double n_malloc = 0, ms_malloc = 0, n_sync = 0, ms_sync = 0;
 };
 MemPool &mem_pool() {
     static MemPool *p = new MemPool();  // never destroyed: DevBufs may be released at exit
@@ -53,22 +76,79 @@ size_t bucket_of(size_t bytes) {
     const size_t q = 256ull << 20;
     return (bytes + q - 1) / q * q;
 }
-// caller holds the lock
-void release_all(MemPool &P, int dev) {
-    for (auto &kv : P.idle[dev]) {
-        cudaFree(kv.second);
-        P.owner.erase(kv.second);
-        P.cached -= kv.first;
-    }
-    P.idle[dev].clear();
-    for (auto &kv : P.parked[dev]) {
-        cudaFree(kv.second);
-        P.owner.erase(kv.second);
-        P.cached -= kv.first;
-    }
+double ms_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+// The caller holds the lock.
+void device_sync(MemPool &P) {
+    const auto t = std::chrono::steady_clock::now();
+    JX_CUDA(cudaDeviceSynchronize());
+    P.n_sync += 1;
+    P.ms_sync += ms_since(t);
+}
+// The caller holds the lock and has synchronised the device: every cached block is idle.
+void unpark_all(MemPool &P, int dev) {
+    for (auto &kv : P.parked[dev]) P.idle[dev].emplace(kv.first, kv.second);
     P.parked[dev].clear();
+    for (auto it = P.idle_tagged.begin(); it != P.idle_tagged.end();) {
+        if (it->first.first != dev) {
+            ++it;
+            continue;
+        }
+        for (auto &kv : it->second) {
+            P.owner[kv.second].tagged = false;
+            P.idle[dev].emplace(kv.first, kv.second);
+        }
+        it = P.idle_tagged.erase(it);
+    }
+}
+// The caller holds the lock and has synchronised the device: the idle blocks
+// that are not carved from a slab go back to the driver.
+void release_idle(MemPool &P, int dev) {
+    unpark_all(P, dev);
+    auto &fl = P.idle[dev];
+    for (auto it = fl.begin(); it != fl.end();) {
+        auto o = P.owner.find(it->second);
+        if (o != P.owner.end() && o->second.carved) {
+            ++it;
+            continue;
+        }
+        cudaFree(it->second);
+        if (o != P.owner.end()) P.owner.erase(o);
+        P.cached -= it->first;
+        it = fl.erase(it);
+    }
+}
+void *carve(MemPool &P, int dev, size_t b) {
+    auto &cur = P.slab_cur[dev];
+    if (cur.second < b) {
+        void *slab = nullptr;
+        const auto t = std::chrono::steady_clock::now();
+        const cudaError_t e = cudaMalloc(&slab, kSlabBytes);
+        P.n_malloc += 1;
+        P.ms_malloc += ms_since(t);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        P.slabs[dev].push_back(slab);
+        cur = {static_cast<char *>(slab), kSlabBytes};
+    }
+    void *p = cur.first;
+    cur.first += b;
+    cur.second -= b;
+    return p;
 }
 }  // namespace
+
+PoolStream::PoolStream(cudaStream_t s) : prev(t_stream), prev_set(t_stream_set) {
+    t_stream = s;
+    t_stream_set = true;
+}
+PoolStream::~PoolStream() {
+    t_stream = prev;
+    t_stream_set = prev_set;
+}
 
 void *pool_alloc(size_t bytes) {
     MemPool &P = mem_pool();
@@ -76,38 +156,56 @@ void *pool_alloc(size_t bytes) {
     JX_CUDA(cudaGetDevice(&dev));
     const size_t b = bucket_of(bytes);
     std::lock_guard<std::mutex> lk(P.mu);
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        auto &fl = P.idle[dev];
+    const bool tag = t_stream_set;
+    const cudaStream_t ts = t_stream;
+    const unsigned long long ep = tag ? P.epoch[ts] : 0;
+    auto take = [&](std::multimap<size_t, void *> &fl) -> void * {
         auto it = fl.find(b);
-        if (it != fl.end()) {
-            void *p = it->second;
-            fl.erase(it);
-            P.cached -= b;
-            return p;
-        }
-        auto &pk = P.parked[dev];
-        if (attempt == 0 && !pk.empty()) {
-            // parked blocks become reusable once everything queued before their release is done
-            JX_CUDA(cudaDeviceSynchronize());
-            for (auto &kv : pk) fl.emplace(kv.first, kv.second);
-            pk.clear();
-            continue;
-        }
-        break;
+        if (it == fl.end()) return nullptr;
+        void *p = it->second;
+        fl.erase(it);
+        Block &B = P.owner[p];
+        if (!B.carved) P.cached -= b;
+        B.tagged = tag;
+        B.stream = ts;
+        B.epoch = ep;
+        return p;
+    };
+    if (tag) {
+        auto it = P.idle_tagged.find(TagKey{dev, {ts, ep}});
+        if (it != P.idle_tagged.end())
+            if (void *p = take(it->second)) return p;
+    }
+    if (void *p = take(P.idle[dev])) return p;
+    if (!tag && !P.parked[dev].empty()) {
+        // parked blocks become reusable once everything queued before their release is done
+        device_sync(P);
+        unpark_all(P, dev);
+        if (void *p = take(P.idle[dev])) return p;
     }
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        cudaDeviceSynchronize();
-        release_all(P, dev);
-        e = cudaMalloc(&p, b);
+    bool carved = false;
+    if (b <= kSlabBucketMax) {
+        p = carve(P, dev, b);
+        carved = p != nullptr;
     }
-    if (e != cudaSuccess) {
-        set_error("cudaMalloc(%zu bytes): %s", b, cudaGetErrorString(e));
-        throw CudaError{e, "cudaMalloc"};
+    if (!p) {
+        const auto t = std::chrono::steady_clock::now();
+        cudaError_t e = cudaMalloc(&p, b);
+        P.n_malloc += 1;
+        P.ms_malloc += ms_since(t);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            device_sync(P);
+            release_idle(P, dev);
+            e = cudaMalloc(&p, b);
+        }
+        if (e != cudaSuccess) {
+            set_error("cudaMalloc(%zu bytes): %s", b, cudaGetErrorString(e));
+            throw CudaError{e, "cudaMalloc"};
+        }
     }
-    P.owner[p] = {dev, b};
+    P.owner[p] = Block{dev, b, tag, carved, ts, ep};
     return p;
 }
 
@@ -120,17 +218,39 @@ void pool_free(void *p) {
         cudaFree(p);
         return;
     }
-    const int dev = it->second.first;
-    const size_t b = it->second.second;
-    P.parked[dev].emplace_back(b, p);
-    P.cached += b;
+    const Block B = it->second;
+    auto ep = P.epoch.find(B.stream);
+    const unsigned long long cur = ep == P.epoch.end() ? 0 : ep->second;
+    if (B.tagged && cur == B.epoch)
+        P.idle_tagged[TagKey{B.dev, {B.stream, B.epoch}}].emplace(B.bucket, p);
+    else
+        P.parked[B.dev].emplace_back(B.bucket, p);
+    if (!B.carved) P.cached += B.bucket;
     if (P.cached > P.limit) {
-        int cur = 0;
-        cudaGetDevice(&cur);
-        cudaSetDevice(dev);
+        int dv = 0;
+        cudaGetDevice(&dv);
+        cudaSetDevice(B.dev);
         cudaDeviceSynchronize();
-        release_all(P, dev);
-        cudaSetDevice(cur);
+        release_idle(P, B.dev);
+        cudaSetDevice(dv);
+    }
+}
+
+void pool_forget_stream(cudaStream_t s) {
+    MemPool &P = mem_pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    const unsigned long long old = P.epoch[s];
+    P.epoch[s] = old + 1;
+    for (auto it = P.idle_tagged.begin(); it != P.idle_tagged.end();) {
+        if (it->first.second.first != s || it->first.second.second != old) {
+            ++it;
+            continue;
+        }
+        for (auto &kv : it->second) {
+            P.owner[kv.second].tagged = false;
+            P.parked[it->first.first].emplace_back(kv.first, kv.second);
+        }
+        it = P.idle_tagged.erase(it);
     }
 }
 
@@ -142,12 +262,36 @@ void pool_trim() {
     std::vector<int> devs;
     for (auto &kv : P.idle) devs.push_back(kv.first);
     for (auto &kv : P.parked) devs.push_back(kv.first);
+    for (auto &kv : P.idle_tagged) devs.push_back(kv.first.first);
+    for (auto &kv : P.slabs) devs.push_back(kv.first);
+    std::sort(devs.begin(), devs.end());
+    devs.erase(std::unique(devs.begin(), devs.end()), devs.end());
     for (int d : devs) {
         cudaSetDevice(d);
         cudaDeviceSynchronize();
-        release_all(P, d);
+        release_idle(P, d);
+        // the slabs go back only when none of their blocks is in use (every carved block idle)
+        size_t carved_total = 0;
+        for (auto &kv : P.owner)
+            if (kv.second.dev == d && kv.second.carved) ++carved_total;
+        if (carved_total == P.idle[d].size()) {
+            for (auto &kv : P.idle[d]) P.owner.erase(kv.second);
+            P.idle[d].clear();
+            for (void *sl : P.slabs[d]) cudaFree(sl);
+            P.slabs[d].clear();
+            P.slab_cur[d] = {nullptr, 0};
+        }
     }
     cudaSetDevice(cur);
+}
+
+void pool_stats(double out[4]) {
+    MemPool &P = mem_pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    out[0] = P.n_malloc;
+    out[1] = P.ms_malloc;
+    out[2] = P.n_sync;
+    out[3] = P.ms_sync;
 }
 
 int sm_count() {

@@ -194,6 +194,28 @@ class CprGmres:
             pass
 
 
+def setup_many(solvers, systems, threads=0):
+    """jxcpr_solver_setup of solvers[k] with systems[k] (objects with ia, ja, a, block_size: host
+    numpy arrays) on `threads` host threads (0: one per core)."""
+    so = _lib.load()
+    m = len(solvers)
+    keep = [(np.ascontiguousarray(s.ia, np.int32), np.ascontiguousarray(s.ja, np.int32),
+             np.ascontiguousarray(s.a, np.float64)) for s in systems]
+    arr = lambda vals: (ctypes.c_void_p * m)(*vals)  # noqa: E731
+    nb = np.array([len(k[0]) - 1 for k in keep], np.int32)
+    bs = np.array([int(s.block_size) for s in systems], np.int32)
+    nnzb = np.array([len(k[1]) for k in keep], np.int64)
+    st = np.zeros(m, np.int32)
+    rc = so.jxcpr_batch_setup(m, arr([G.h.value for G in solvers]), _ptr(nb), _ptr(bs), _ptr(nnzb),
+                              arr([k[0].ctypes.data for k in keep]), arr([k[1].ctypes.data for k in keep]),
+                              arr([k[2].ctypes.data for k in keep]), 0, int(threads), _ptr(st))
+    _lib.check(rc)
+    for G, s, k in zip(solvers, systems, keep):
+        G.nb, G.bs = len(k[0]) - 1, int(s.block_size)
+        G._keep = k
+    return solvers
+
+
 class CprGmresBatch:
     """Many set-up CprGmres solvers solved by one CUDA-graph launch.
 
