@@ -120,7 +120,7 @@ int jxcpr_solver_destroy(jxcpr_solver *h) {
         if (owns) cudaStreamSynchronize(st);
         delete h;
         if (owns) {
-            pool_forget_stream(st);  // before a new stream can take the same handle
+            pool_forget_stream(st, true);  // synchronised above: its blocks are free for any stream
             cudaStreamDestroy(st);
         }
         return JXCPR_SUCCESS;
@@ -129,11 +129,15 @@ int jxcpr_solver_destroy(jxcpr_solver *h) {
 
 int jxcpr_solver_set_stream(jxcpr_solver *h, void *stream) {
     if (!h) return JXCPR_ERROR_ARG;
-    // blocks made for the previous stream park when freed: the new stream's work is not ordered after it
-    pool_forget_stream(h->s.stream);
-    if (h->s.owns_stream && h->s.stream) {
-        cudaStreamSynchronize(h->s.stream);
-        cudaStreamDestroy(h->s.stream);
+    // Blocks made for the previous stream must not be reused on it once the solver's work goes to
+    // another stream (that work is not ordered after the old stream's).
+    cudaStream_t old = h->s.stream;
+    if (h->s.owns_stream && old) {
+        cudaStreamSynchronize(old);
+        pool_forget_stream(old, true);
+        cudaStreamDestroy(old);
+    } else if (h->s.stream_set && old != (cudaStream_t)stream) {
+        pool_forget_stream(old, false);
     }
     h->s.stream = (cudaStream_t)stream;
     h->s.owns_stream = false;

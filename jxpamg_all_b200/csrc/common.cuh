@@ -68,12 +68,14 @@ void count_launches(unsigned long long n);  // kernels replayed by a CUDA graph 
 //    after every earlier use), with no device synchronisation.
 //  * Other blocks are parked when freed and become reusable after a device
 //    synchronisation (the one cudaFree would have done).
-// pool_forget_stream(s) is called before a tagged stream is destroyed or
-// replaced: its idle blocks are parked and its live blocks park when freed.
+// pool_forget_stream(s, drained) is called before a tagged stream is
+// destroyed or replaced: its idle blocks become reusable by any stream if
+// nothing is left queued on s (drained), else they are parked; its live
+// blocks park when freed.
 void *pool_alloc(size_t bytes);
 void pool_free(void *p);
 void pool_trim();
-void pool_forget_stream(cudaStream_t s);
+void pool_forget_stream(cudaStream_t s, bool drained);
 // process-wide: cudaMalloc calls, their total ms, device synchronisations, their total ms
 void pool_stats(double out[4]);
 

@@ -236,7 +236,7 @@ void pool_free(void *p) {
     }
 }
 
-void pool_forget_stream(cudaStream_t s) {
+void pool_forget_stream(cudaStream_t s, bool drained) {
     MemPool &P = mem_pool();
     std::lock_guard<std::mutex> lk(P.mu);
     const unsigned long long old = P.epoch[s];
@@ -248,7 +248,8 @@ void pool_forget_stream(cudaStream_t s) {
         }
         for (auto &kv : it->second) {
             P.owner[kv.second].tagged = false;
-            P.parked[it->first.first].emplace_back(kv.first, kv.second);
+            if (drained) P.idle[it->first.first].emplace(kv.first, kv.second);  // nothing left queued on s
+            else P.parked[it->first.first].emplace_back(kv.first, kv.second);
         }
         it = P.idle_tagged.erase(it);
     }
