@@ -81,9 +81,9 @@ JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, doubl
 
 /* <x, y> like jxcpr_dot_dev, but allocating nothing.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory when
- * they need the product -- code running inside a CUDA-graph capture region,
- * where cudaMalloc is not allowed, or an application whose memory pool owns
- * the whole device.  The partial sums live in a static device array reserved
+ * they need the product -- an application whose own memory pool has reserved
+ * the whole device, or a time-critical loop that allows no allocator call
+ * (cudaMalloc can synchronise the device and stall every stream).  The partial sums live in a static device array reserved
  * when the library loads (JXCPR_NOALLOC_DOT_MAX_PARTIALS partials of
  * JXCPR_NOALLOC_DOT_CHUNK elements each, 512 KB per GPU, kept until exit), so
  * n is limited to JXCPR_NOALLOC_DOT_MAX_PARTIALS * JXCPR_NOALLOC_DOT_CHUNK

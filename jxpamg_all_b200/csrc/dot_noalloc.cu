@@ -1,10 +1,9 @@
 // Inner product that allocates nothing: jxcpr_dot_dev_noalloc.
 //
 // Some callers cannot allocate device memory at the moment they need an inner
-// product -- a solver loop running inside a CUDA-graph capture region (where
-// cudaMalloc is not allowed), a host application whose memory pool has
-// reserved the whole device, or a real-time loop that forbids allocator calls
-// on its critical path.  jxcpr_dot_dev allocates its per-CTA partial sums on
+// product -- a host application whose memory pool has reserved the whole
+// device, or a time-critical loop that forbids allocator calls on its critical
+// path (cudaMalloc can synchronise the device and stall every stream).  jxcpr_dot_dev allocates its per-CTA partial sums on
 // every call, which these callers cannot accept.  This variant keeps the
 // partial sums and the result in a fixed array that the library reserves when
 // it is loaded: JXCPR_NOALLOC_DOT_MAX_PARTIALS doubles of partial sums (one per
@@ -31,7 +30,7 @@ constexpr int kMaxPartials = JXCPR_NOALLOC_DOT_MAX_PARTIALS;
 constexpr int kThreads = 256;
 
 // partial sums [0, kMaxPartials), result at [kMaxPartials]
-__device__ __align__(256) double g_dot_scratch[kMaxPartials + 32];
+static __device__ __align__(256) double g_dot_scratch[kMaxPartials + 32];
 
 std::mutex g_mu;
 double *g_addr[64] = {nullptr};

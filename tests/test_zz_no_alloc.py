@@ -1,5 +1,6 @@
 """jxcpr_dot_dev_noalloc: the inner product for callers that cannot allocate
-device memory (graph-capture regions, applications whose pool owns the GPU).
+device memory (applications whose own pool owns the GPU, loops that allow no
+allocator call).
 
 Checked through the C ABI against jxcpr_dot_dev on two calls in a row (the
 second reuses the static scratch the first one left behind), plus the size
