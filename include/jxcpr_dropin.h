@@ -173,7 +173,7 @@ JXCPR_API JXF_Int jxf_ParVectorInitialize(jxf_ParVector *v);
 JXCPR_API JXF_Int jxf_ParVectorSetConstantValues(jxf_ParVector *v, JXF_Real value);
 JXCPR_API JXF_Int jxf_ParVectorDestroy(jxf_ParVector *v);
 
-/* ---- decoupling (ABF = 1, True-IMPES = 5 on the GPU; other types return 4) ------------ */
+/* ---- decoupling on the GPU: ABF 1, ANL 2, SEM 3, QI 4, True-IMPES 5, True-IMPES (2nd) 6; thermal for 2-4 -- */
 JXCPR_API JXF_Int jxf_BSRMatrixDecouple(jxf_BSRMatrix *A, jxf_Vector *rhs, JXF_DecoupType decoup_type,
                                         JXF_Int is_thermal);
 JXCPR_API const char *jxf_DecoupTypeToString(JXF_DecoupType decoup_type);

@@ -126,5 +126,11 @@ void gs_sweep(const CsrView<double> &A, const Schedule &sch, const double *f, do
 // scratch (nb*bs) that receives the iterate at sweep start.
 void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
                double *vt, double w, double omega, int *err, cudaStream_t s);
+// Stage-2 block hybrid symmetric Gauss-Seidel (jxf_ParBSRHSGSRelax, par_relax_bsr.c:579-1062): a
+// forward pass along `fwd`, then a backward pass along `bwd`.  vt: scratch (nb*bs); work: the CPR's
+// work vector (nb*bs, zero when created), of which only the first nb entries are refreshed from x,
+// as the reference does, and which feeds the res2 term of the weighted update.
+void hsgs_sweep(const BsrView<double> &A, const Schedule &fwd, const Schedule &bwd, const double *b, double *x,
+                double *vt, double *work, double w, double omega, int *err, cudaStream_t s);
 
 }  // namespace jxcpr

@@ -48,6 +48,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"stage1_solver_type", &p.stage1_solver_type},
                {"stage2_solver_type", &p.stage2_solver_type},
                {"decouple", &p.decouple},
+               {"thermal", &p.thermal},
                {"consistent_rhs", &p.consistent_rhs},
                {"smoother_order", &p.smoother_order},
                {"coarse_exact", &p.coarse_exact},

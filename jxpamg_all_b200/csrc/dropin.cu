@@ -412,9 +412,8 @@ const char *jxf_DecoupTypeToString(JXF_DecoupType t) {
 JXF_Int jxf_BSRMatrixDecouple(jxf_BSRMatrix *A, jxf_Vector *rhs, JXF_DecoupType type, JXF_Int is_thermal) {
     if (!A) return JXCPR_ERROR_ARG;
     if (type == JXF_DECOUP_NONE) return JXCPR_SUCCESS;
-    if ((type != JXF_DECOUP_ABF && type != JXF_DECOUP_TIMPES) || is_thermal) {
-        set_error("jxf_BSRMatrixDecouple: %s%s not provided by this build (ABF and True-IMPES are)",
-                  jxf_DecoupTypeToString(type), is_thermal ? " (thermal)" : "");
+    if ((int)type < 1 || (int)type > 6) {
+        set_error("jxf_BSRMatrixDecouple: unknown decoupling type %d", (int)type);
         return JXCPR_ERROR_ARG;
     }
     return guard([&] {
@@ -427,7 +426,7 @@ JXF_Int jxf_BSRMatrixDecouple(jxf_BSRMatrix *A, jxf_Vector *rhs, JXF_DecoupType 
         D.ja.upload(A->j, (size_t)nnzb, s);
         D.a.upload(A->data, (size_t)nnzb * bs * bs, s);
         DevBuf<double> coef((size_t)std::max(nb, 1) * std::max(decouple_coef_size(bs, (int)type), 1));
-        bsr_decouple_matrix(D, (int)type, coef.get(), s);
+        bsr_decouple_matrix(D, (int)type, coef.get(), s, is_thermal ? 1 : 0);
         D.a.download(A->data, (size_t)nnzb * bs * bs, s);
         if (rhs && rhs->data) {
             DevBuf<double> b((size_t)std::max(nb * bs, 1));

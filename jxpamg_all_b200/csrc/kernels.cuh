@@ -81,7 +81,8 @@ void prolong_pressure(int nb, int bs, int p, const double *xp, double *x, cudaSt
 // Matrix part of jxf_BSRMatrixDecouple (type 1 ABF, 5 True-IMPES); `coef`
 // (nb * decouple_coef_size) receives what the right-hand side update needs.
 int decouple_coef_size(int bs, int type);
-void bsr_decouple_matrix(DeviceBsr &A, int type, double *coef, cudaStream_t s);
+// type: 1 ABF, 2 ANL, 3 SEM, 4 QI, 5 True-IMPES, 6 True-IMPES (second form); thermal applies to 2-4
+void bsr_decouple_matrix(DeviceBsr &A, int type, double *coef, cudaStream_t s, int thermal = 0);
 void bsr_decouple_rhs(int nb, int bs, int type, const double *coef, double *rhs, int consistent_rhs,
                       cudaStream_t s);
 

@@ -207,11 +207,14 @@ __device__ __forceinline__ void blk_inv_matvec(const double *__restrict__ mat, c
     for (int q = 0; q < 3; ++q) ov[q] = o[q];
 }
 
+// vt: the iterate at the start of the pass (read for neighbours not yet
+// updated in it); vt2: the vector of the res2 term (vt for HGS, the CPR's work
+// vector for HSGS).
 template <int BS>
 __device__ __forceinline__ void hgs_row(int i, const int *__restrict__ ia, const int *__restrict__ ja,
                                         const double *__restrict__ a, const int *__restrict__ rank,
                                         const double *__restrict__ b, double *x, const double *__restrict__ vt,
-                                        double w, double omega, bool plain) {
+                                        const double *__restrict__ vt2, double w, double omega, bool plain) {
     constexpr int B2 = BS * BS;
     const int ri = rank[i];
     const long long d = ia[i], e = ia[i + 1];
@@ -245,8 +248,8 @@ __device__ __forceinline__ void hgs_row(int i, const int *__restrict__ ia, const
         const bool fresh = rank[j] < ri;
 #pragma unroll
         for (int k = 0; k < BS; ++k) {
-            vj[k] = vt[(long long)j * BS + k];
-            xj[k] = fresh ? ((volatile const double *)x)[(long long)j * BS + k] : vj[k];
+            vj[k] = vt2[(long long)j * BS + k];
+            xj[k] = fresh ? ((volatile const double *)x)[(long long)j * BS + k] : vt[(long long)j * BS + k];
         }
         blk_matvec_stable<BS>(-1.0, a + jj * B2, xj, res0);
         blk_matvec_stable<BS>(1.0, a + jj * B2, vj, res2);
@@ -269,12 +272,14 @@ __global__ void hgs_sweep_grid_kernel(int ngroups, const int *__restrict__ gptr,
                                       const int *__restrict__ ia, const int *__restrict__ ja,
                                       const double *__restrict__ a, const int *__restrict__ rank,
                                       const double *__restrict__ b, double *x, const double *__restrict__ vt,
-                                      double w, double omega, int plain, GridBarrier *bar, int *err) {
+                                      const double *__restrict__ vt2, double w, double omega, int plain,
+                                      GridBarrier *bar, int *err) {
     const int nthreads = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     for (int g = 0; g < ngroups; ++g) {
         const int r0 = gptr[g], r1 = gptr[g + 1];
-        for (int t = r0 + tid; t < r1; t += nthreads) hgs_row<BS>(perm[t], ia, ja, a, rank, b, x, vt, w, omega, plain);
+        for (int t = r0 + tid; t < r1; t += nthreads)
+            hgs_row<BS>(perm[t], ia, ja, a, rank, b, x, vt, vt2, w, omega, plain);
         if (g + 1 < ngroups) {
             __threadfence();
             if (!grid_barrier(bar, gridDim.x, err)) return;
@@ -287,12 +292,12 @@ __global__ void hgs_sweep_block_kernel(int ngroups, const int *__restrict__ gptr
                                        const int *__restrict__ ia, const int *__restrict__ ja,
                                        const double *__restrict__ a, const int *__restrict__ rank,
                                        const double *__restrict__ b, double *x, const double *__restrict__ vt,
-                                       double w, double omega, int plain) {
+                                       const double *__restrict__ vt2, double w, double omega, int plain) {
     const int stride = gridDim.x * blockDim.x;
     for (int g = 0; g < ngroups; ++g) {
         const int r0 = gptr[g], r1 = gptr[g + 1];
         for (int t = r0 + blockIdx.x * blockDim.x + threadIdx.x; t < r1; t += stride)
-            hgs_row<BS>(perm[t], ia, ja, a, rank, b, x, vt, w, omega, plain);
+            hgs_row<BS>(perm[t], ia, ja, a, rank, b, x, vt, vt2, w, omega, plain);
         __syncthreads();
     }
 }
@@ -351,22 +356,22 @@ void gs_sweep(const CsrView<double> &A, const Schedule &sch, const double *f, do
     count_launch();
 }
 
-void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
-               double *vt, double w, double omega, int *err, cudaStream_t s) {
+namespace {
+// One pass of the block point update along `sch` (vt already holds the iterate at the pass start).
+void hgs_pass(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
+              const double *vt, const double *vt2, double w, double omega, int plain, int *err, cudaStream_t s) {
     const int nb = A.nb;
-    if (nb == 0 || sch.ngroups == 0) return;
-    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * A.bs, cudaMemcpyDeviceToDevice, s));
-    const double eps = 2.220446049250313e-16;
-    int plain = (fabs(w - 1) < eps && fabs(omega - 1) < eps) ? 1 : 0;
     if (nb <= kSmallRows || sch.ngroups == 1) {
         const int threads = sch.ngroups == 1 ? 256 : 1024;
         const int blocks = sch.ngroups == 1 ? div_up(nb, 256) : 1;
         if (A.bs == 2)
             hgs_sweep_block_kernel<2><<<blocks, threads, 0, s>>>(sch.ngroups, sch.group_ptr.get(), sch.perm.get(),
-                                                                 A.ia, A.ja, A.a, rank, b, x, vt, w, omega, plain);
+                                                                 A.ia, A.ja, A.a, rank, b, x, vt, vt2, w, omega,
+                                                                 plain);
         else
             hgs_sweep_block_kernel<3><<<blocks, threads, 0, s>>>(sch.ngroups, sch.group_ptr.get(), sch.perm.get(),
-                                                                 A.ia, A.ja, A.a, rank, b, x, vt, w, omega, plain);
+                                                                 A.ia, A.ja, A.a, rank, b, x, vt, vt2, w, omega,
+                                                                 plain);
         JX_LAUNCH_CHECK();
         return;
     }
@@ -381,10 +386,37 @@ void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, d
     const int *gp = sch.group_ptr.get(), *pm = sch.perm.get();
     const int *aia = A.ia, *aja = A.ja;
     const double *aa = A.a;
-    void *args[] = {&ng, &gp, &pm, &aia, &aja, &aa, &rank, &b, &x, &vt, &w, &omega, &plain, &bar, &err};
+    void *args[] = {&ng, &gp, &pm, &aia, &aja, &aa, &rank, &b, &x, &vt, &vt2, &w, &omega, &plain, &bar, &err};
     void *fn = A.bs == 2 ? (void *)hgs_sweep_grid_kernel<2> : (void *)hgs_sweep_grid_kernel<3>;
     JX_CUDA(cudaLaunchCooperativeKernel(fn, blocks, kSweepThreads, args, 0, s));
     count_launch();
+}
+
+int plain_weights(double w, double omega) {
+    const double eps = 2.220446049250313e-16;
+    return (fabs(w - 1) < eps && fabs(omega - 1) < eps) ? 1 : 0;
+}
+}  // namespace
+
+void hgs_sweep(const BsrView<double> &A, const Schedule &sch, const double *b, double *x, const int *rank,
+               double *vt, double w, double omega, int *err, cudaStream_t s) {
+    const int nb = A.nb;
+    if (nb == 0 || sch.ngroups == 0) return;
+    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * A.bs, cudaMemcpyDeviceToDevice, s));
+    hgs_pass(A, sch, b, x, rank, vt, vt, w, omega, plain_weights(w, omega), err, s);
+}
+
+void hsgs_sweep(const BsrView<double> &A, const Schedule &fwd, const Schedule &bwd, const double *b, double *x,
+                double *vt, double *work, double w, double omega, int *err, cudaStream_t s) {
+    const int nb = A.nb;
+    if (nb == 0 || fwd.ngroups == 0 || bwd.ngroups == 0) return;
+    const int plain = plain_weights(w, omega);
+    // the reference refreshes only the first nb (block-row count) entries of its work vector
+    if (!plain) JX_CUDA(cudaMemcpyAsync(work, x, sizeof(double) * nb, cudaMemcpyDeviceToDevice, s));
+    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * A.bs, cudaMemcpyDeviceToDevice, s));
+    hgs_pass(A, fwd, b, x, fwd.rank.get(), vt, work, w, omega, plain, err, s);
+    JX_CUDA(cudaMemcpyAsync(vt, x, sizeof(double) * nb * A.bs, cudaMemcpyDeviceToDevice, s));
+    hgs_pass(A, bwd, b, x, bwd.rank.get(), vt, work, w, omega, plain, err, s);
 }
 
 }  // namespace jxcpr

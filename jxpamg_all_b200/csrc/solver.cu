@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <chrono>
 
+#include <stdexcept>
+
 #include "solver.cuh"
 
 namespace jxcpr {
@@ -24,6 +26,10 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     Timer t;
     t.start(s);
     const bool fast_path = prm.smoother_order != ORDER_EXACT;
+    if (fast_path && prm.stage2_solver_type == 3) {
+        set_error("stage2_solver_type 3 (HSGS) is provided in the exact-order mode (smoother_order 0) only");
+        throw std::invalid_argument("hsgs");
+    }
     amg.prm.order = prm.smoother_order;
     amg.prm.coarse_exact = fast_path ? 0 : prm.coarse_exact;
     amg.prm.max_colors = prm.max_colors;
@@ -82,6 +88,12 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     rp.alloc(A.nb > 0 ? A.nb : 1);
     xp.alloc(A.nb > 0 ? A.nb : 1);
     vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+    hsgs_work.release();
+    if (prm.stage2_solver_type == 3) {
+        // the CPR's work vector, zero when created (jxf_cpr.c:396); HSGS keeps state in it
+        hsgs_work.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+        hsgs_work.zero(s);
+    }
     stats[0] = t.stop_ms(s) * 1e-3;
     stats[2] = 0.0;  // stage 2 (HGS) needs no setup beyond the level-0 schedule
     bilu.reset();
@@ -113,7 +125,7 @@ void CprPrecond::apply(const double *r, double *z, cudaStream_t s) {
     JX_CUDA(cudaMemsetAsync(xp.get(), 0, sizeof(double) * nb, s));
     for (int it = 0; it < prm.stage1_maxit; ++it) amg_vcycle(amg, rp.get(), xp.get(), s);
     prolong_pressure(nb, bs, prm.pressure_index, xp.get(), z, s);
-    if (prm.stage2_solver_type == 2)
+    if (prm.stage2_solver_type == 2 || prm.stage2_solver_type == 3)
         for (int it = 0; it < prm.stage2_maxit; ++it) stage2_sweep(r, z, s);
     bilu_stage(r, z, s);
 }
@@ -146,6 +158,11 @@ void CprPrecond::stage2_sweep(const double *r, double *z, cudaStream_t s) {
         return;
     }
     const AmgLevel &L0 = *amg.levels[0];
+    if (prm.stage2_solver_type == 3) {
+        hsgs_sweep(A, L0.fwd, L0.bwd, r, z, vt.get(), hsgs_work.get(), prm.stage2_relax_weight, prm.stage2_omega,
+                   amg.err.get(), s);
+        return;
+    }
     hgs_sweep(A, L0.fwd, r, z, L0.fwd.rank.get(), vt.get(), prm.stage2_relax_weight, prm.stage2_omega,
               amg.err.get(), s);
 }
@@ -547,7 +564,7 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const int csz = decouple_coef_size(bs, prm.decouple);
     dcoef.alloc((size_t)(nb > 0 ? nb : 1) * (csz > 0 ? csz : 1));
-    if (prm.decouple) bsr_decouple_matrix(A, prm.decouple, dcoef.get(), s);
+    if (prm.decouple) bsr_decouple_matrix(A, prm.decouple, dcoef.get(), s, prm.thermal);
     JX_CUDA(cudaStreamSynchronize(s));
     decouple_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() - upload_ms;
     kerr.alloc(1);

@@ -33,7 +33,8 @@ struct SolverParams {
     int stage1_maxit = 1;
     int stage2_maxit = 3;
     int stage1_solver_type = 1;  // 1: AMG
-    int stage2_solver_type = 2;  // 2: block hybrid Gauss-Seidel (HGS); 5: block ILU(0) correction (BILU)
+    int stage2_solver_type = 2;  // 2: block hybrid Gauss-Seidel (HGS); 3: symmetric HGS (HSGS, exact-order
+                                 // mode); 5: block ILU(0) correction (BILU)
     // BILU stage 2 (jxf_BILUSetup type 3 / jxf_BILUSolve tri-solve 14 parameters)
     int bilu_sweeps = 3;
     int bilu_ir_iters = 5;
@@ -42,8 +43,10 @@ struct SolverParams {
     double threshold = 1e-15;    // accepted and ignored, as in the reference
     double stage2_relax_weight = 0.7;
     double stage2_omega = 0.9;
-    // decoupling applied by the solver object (0 none, 1 ABF, 5 True-IMPES)
+    // decoupling applied by the solver object (JXF_DecoupType: 0 none, 1 ABF, 2 ANL, 3 SEM, 4 QI,
+    // 5 True-IMPES, 6 True-IMPES second form); thermal: the last unknown is temperature (types 2-4)
     int decouple = 0;
+    int thermal = 0;
     int consistent_rhs = 0;
     // AMG strength threshold (jxf_cpr.c:331 sets 0.25)
     double strong_threshold = 0.25;
@@ -104,6 +107,7 @@ struct CprPrecond {
     int learned_used = 0;
     LearnedPlan plan;  // per-level features and learned settings of the last setup
     DevBuf<double> rp, xp, vt;
+    DevBuf<double> hsgs_work;  // stage2_solver_type 3: the reference's persistent Vtemp vector
     double stats[4] = {0, 0, 0, 0};  // stage1 setup, stage1 solve, stage2 setup, stage2 solve (seconds)
     bool ready = false;
     void setup(const BsrView<double> &A_, cudaStream_t s);

@@ -82,13 +82,14 @@ def bsr_matvec(ia, ja, a, bs, x, alpha=1.0, y=None, beta=0.0):
     return y
 
 
-def bsr_decouple(ia, ja, a, bs, rhs, dtype_code, consistent_rhs=False):
-    """Returns (a', rhs') after jxf_BSRMatrixDecouple (1 = ABF, 5 = TIMPES)."""
+def bsr_decouple(ia, ja, a, bs, rhs, dtype_code, consistent_rhs=False, thermal=False):
+    """Returns (a', rhs') after jxf_BSRMatrixDecouple (1 ABF, 2 ANL, 3 SEM, 4 QI, 5 TIMPES,
+    6 TIMPES2; thermal applies to 2-4)."""
     nb = len(ia) - 1
     ia, ja = _i32(ia), _i32(ja)
     a2, r2 = _f64(a).copy(), _f64(rhs).copy()
-    st = orc().orc_bsr_decouple(c_int(nb), c_int(bs), _p(ia), _p(ja), _p(a2), _p(r2), c_int(dtype_code),
-                                c_int(1 if consistent_rhs else 0))
+    st = orc().orc_bsr_decouple2(c_int(nb), c_int(bs), _p(ia), _p(ja), _p(a2), _p(r2), c_int(dtype_code),
+                                 c_int(1 if thermal else 0), c_int(1 if consistent_rhs else 0))
     if st:
         raise ValueError(f"orc_bsr_decouple status {st}")
     return a2, r2
@@ -104,11 +105,12 @@ def ref_bsr_matvec(ia, ja, a, bs, x, alpha=1.0, y=None, beta=0.0):
     return y
 
 
-def ref_bsr_decouple(ia, ja, a, bs, rhs, dtype_code):
+def ref_bsr_decouple(ia, ja, a, bs, rhs, dtype_code, thermal=False):
     nb = len(ia) - 1
     ia, ja = _i32(ia), _i32(ja)
     a2, r2 = _f64(a).copy(), _f64(rhs).copy()
-    ref().ref_bsr_decouple(c_int(nb), c_int(bs), _p(ia), _p(ja), _p(a2), _p(r2), c_int(dtype_code), c_int(1))
+    ref().ref_bsr_decouple2(c_int(nb), c_int(bs), _p(ia), _p(ja), _p(a2), _p(r2), c_int(dtype_code),
+                            c_int(1 if thermal else 0), c_int(1))
     return a2, r2
 
 
@@ -148,13 +150,14 @@ class OracleCPR(_CprBase):
 
     _prefix = "orc_"
 
-    def __init__(self, ia, ja, a, bs, stage2_maxit=3):
+    def __init__(self, ia, ja, a, bs, stage2_maxit=3, stage2_type=2):
         self._lib = orc()
         self._lib.orc_cpr_create.restype = c_void_p
         self.nb, self.bs = len(ia) - 1, bs
         self._keep = (_i32(ia), _i32(ja), _f64(a))
         self.h = self._lib.orc_cpr_create(c_int(self.nb), c_int(bs), *(_p(v) for v in self._keep),
                                           c_int(stage2_maxit))
+        self._lib.orc_cpr_set_stage2_type(c_void_p(self.h), c_int(stage2_type))
 
     def apply(self, r):
         z = np.zeros(self.nb * self.bs)
@@ -249,6 +252,26 @@ def ref_hgs_relax(ia, ja, a, bs, x, b, w=0.7, omega=0.9, direction=1, sweeps=1):
     ref().ref_hgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), c_double(w),
                         c_double(omega), c_int(direction), c_int(sweeps))
     return x
+
+
+def hsgs_relax(ia, ja, a, bs, x, b, work, w=0.7, omega=0.9, sweeps=1):
+    """jxf_ParBSRHSGSRelax restated; returns (x, work) (work = the Vtemp vector, in/out)."""
+    nb = len(ia) - 1
+    x, work = _f64(x).copy(), _f64(work).copy()
+    keep = (_i32(ia), _i32(ja), _f64(a))
+    for _ in range(sweeps):
+        orc().orc_hsgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), _p(work),
+                             c_double(w), c_double(omega))
+    return x, work
+
+
+def ref_hsgs_relax(ia, ja, a, bs, x, b, work, w=0.7, omega=0.9, sweeps=1):
+    nb = len(ia) - 1
+    x, work = _f64(x).copy(), _f64(work).copy()
+    keep = (_i32(ia), _i32(ja), _f64(a))
+    ref().ref_hsgs_relax(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), _p(work),
+                         c_double(w), c_double(omega), c_int(sweeps))
+    return x, work
 
 
 # ---- block ILU(0) (orc_bilu.c restatement; ref_bilu = the reference library) ---------

@@ -10,6 +10,8 @@ int orc_bsr_matvec(int nb, int bs, const int *ia, const int *ja, const double *a
                    double beta, double *y);
 int orc_bsr_decouple(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
                      int consistent_rhs);
+int orc_bsr_decouple2(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
+                      int thermal, int consistent_rhs);
 void orc_restrict(int nb, int bs, int p, const double *r, double *rp);
 void orc_prolong(int nb, int bs, int p, const double *xp, double *x);
 void orc_bsr_submatrix(int nb, int bs, const int *ia, const int *ja, const double *a, int p, int *cia, int *cja,
@@ -34,9 +36,10 @@ typedef struct {
 } orc_amg;
 
 typedef struct {
-    int nb, bs, stage2_maxit;
+    int nb, bs, stage2_maxit, stage2_type;
     const int *ia, *ja;
     const double *a;
+    double *work; /* stage-2 work vector (nb * bs), zero at setup */
     orc_csr Ap;
     orc_amg amg;
 } orc_cpr;
@@ -58,6 +61,8 @@ int orc_gselim(const orc_csr *A, const double *f, double *u);
 void orc_amg_vcycle(const orc_amg *H, const double *f0, double *u0);
 void orc_hgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
                    double w, double omega, int direction);
+void orc_hsgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                    double *work, double w, double omega);
 void orc_cpr_setup(orc_cpr *C, int nb, int bs, const int *ia, const int *ja, const double *a, int stage2_maxit);
 void orc_cpr_apply(const orc_cpr *C, const double *r, double *z);
 void orc_cpr_free(orc_cpr *C);

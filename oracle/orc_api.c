@@ -42,6 +42,9 @@ void orc_cpr_destroy(void *hv)
     free(h);
 }
 
+/* stage2_type 2: forward HGS sweeps, 3: HSGS (jxf_cpr.c:572-585) */
+void orc_cpr_set_stage2_type(void *hv, int type) { ((orc_cpr_handle *)hv)->cpr.stage2_type = type; }
+
 void orc_cpr_apply_h(void *hv, const double *r, double *z)
 {
     orc_cpr_handle *h = (orc_cpr_handle *)hv;

@@ -196,17 +196,157 @@ static void timpes(int nb, int bs, const int *ia, const int *ja, double *a, doub
     free(Ac);
 }
 
-/* jxf_BSRMatrixDecouple, jxf_bsr_decoup.c:1273-1348 (types: 0 none, 1 ABF, 5 TIMPES) */
-int orc_bsr_decouple(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
-                     int consistent_rhs)
+/*
+ * Row-transform decouplings: one bs x bs matrix M_i per block row, built from
+ * the row's diagonal block (the first block), applied to every block of the
+ * row (C = M_i B with C = 0; C += M_ik B_kj, jxf_smat_mul :288-298) and to b_i
+ * by the reference's generic matrix-vector helper called with input and
+ * output aliased (jxf_smat_vec_mul :306-314: c_p = 0, then c_p += M_pk b_k
+ * reading already-overwritten entries; with `consistent_rhs` the product is
+ * formed from a copy).
+ *   ANL (type 2, :529-588): M = I, first row [1, -d_01, ..., -d_0,n-1].
+ *   SEM (type 3, :591-654): M = inv(D_i) (jxf_smat_inv_nc: the 2x2 / 3x3
+ *       cofactor inverses) with its first row replaced as in ANL.
+ *   QI  (type 4, :657-714): M = I, first row [1, -d_01/d_11, ..., -d_0l/d_ll].
+ * Thermal mode (the last unknown is temperature) changes the first row only in
+ * columns 1..n-2 and the last row likewise (SEM also sets M_0,n-1 = M_n-1,0 = 0
+ * and M_n-1,n-1 = 1).
+ */
+static void row_matrix(int type, int bs, int thermal, const double *d, double *M)
+{
+    const int b2 = bs * bs;
+    if (type == 3) {
+        memcpy(M, d, sizeof(double) * b2);
+        if (bs == 2) inv2(M); else inv3(M);
+        if (thermal) {
+            M[0] = 1.0;
+            M[bs - 1] = 0.0;
+            M[(bs - 1) * bs] = 0.0;
+            M[b2 - 1] = 1.0;
+            for (int l = 0; l < bs - 2; l++) {
+                M[1 + l] = -d[1 + l];
+                M[(bs - 1) * bs + 1 + l] = -d[(bs - 1) * bs + 1 + l];
+            }
+        } else {
+            M[0] = 1.0;
+            for (int l = 0; l < bs - 1; l++) M[1 + l] = -d[1 + l];
+        }
+        return;
+    }
+    for (int r = 0; r < bs; r++)
+        for (int c = 0; c < bs; c++) M[r * bs + c] = (r == c) ? 1.0 : 0.0;
+    const int nl = thermal ? bs - 2 : bs - 1;
+    for (int l = 0; l < nl; l++) {
+        if (type == 2) {
+            M[1 + l] = -d[1 + l];
+            if (thermal) M[(bs - 1) * bs + 1 + l] = -d[(bs - 1) * bs + 1 + l];
+        } else {
+            M[1 + l] = -d[1 + l] / d[(l + 1) * bs + l + 1];
+            if (thermal) M[(bs - 1) * bs + 1 + l] = -d[(bs - 1) * bs + 1 + l] / d[(l + 1) * bs + l + 1];
+        }
+    }
+}
+
+static void row_transform(int nb, int bs, int type, int thermal, const int *ia, double *a, double *rhs,
+                          int consistent_rhs)
+{
+    const int b2 = bs * bs;
+    for (int i = 0; i < nb; i++) {
+        double M[9], sm[9];
+        row_matrix(type, bs, thermal, a + (size_t)ia[i] * b2, M);
+        for (int j = ia[i]; j < ia[i + 1]; j++) {
+            double *blk = a + (size_t)j * b2;
+            for (int r = 0; r < bs; r++)
+                for (int c = 0; c < bs; c++) {
+                    double t = 0.0;
+                    for (int k = 0; k < bs; k++) t += M[r * bs + k] * blk[k * bs + c];
+                    sm[r * bs + c] = t;
+                }
+            memcpy(blk, sm, sizeof(double) * b2);
+        }
+        double *r = rhs + (size_t)i * bs;
+        if (consistent_rhs) {
+            double v[3], o[3];
+            memcpy(v, r, sizeof(double) * bs);
+            for (int p = 0; p < bs; p++) {
+                double t = 0.0;
+                for (int k = 0; k < bs; k++) t += M[p * bs + k] * v[k];
+                o[p] = t;
+            }
+            memcpy(r, o, sizeof(double) * bs);
+        } else {
+            for (int p = 0; p < bs; p++) {
+                r[p] = 0.0;
+                for (int k = 0; k < bs; k++) r[p] += M[p * bs + k] * r[k];
+            }
+        }
+    }
+}
+
+/*
+ * True-IMPES, second form (type 6, jxf_bsr_decoup.c:1102-1267): column-sum
+ * blocks Ac as for type 5, then the pressure row of every block in row i
+ * becomes row0 + c row1 (2x2, c = -Ac01/Ac11, 0 when |det Ac_i| < 1e-15) or
+ * row0 + c0 row1 + c1 row2 with (c0, c1) = the first two entries of
+ * inv(Ac_i) (3x3); b_i gets the same row operation.
+ */
+static void timpes2(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs)
+{
+    const int b2 = bs * bs;
+    double *Ac = (double *)calloc((size_t)nb * b2 + 1, sizeof(double));
+    for (int i = 0; i < nb; i++)
+        for (int j = ia[i]; j < ia[i + 1]; j++)
+            for (int k = 0; k < b2; k++) Ac[(size_t)ja[j] * b2 + k] += a[(size_t)j * b2 + k];
+    for (int i = 0; i < nb; i++) {
+        const double *ac = Ac + (size_t)i * b2;
+        if (bs == 2) {
+            const double det = ac[0] * ac[3] - ac[1] * ac[2];
+            const double c = fabs(det) < 1e-15 ? 0.0 : -ac[1] / ac[3];
+            for (int j = ia[i]; j < ia[i + 1]; j++) {
+                double *blk = a + (size_t)j * 4;
+                blk[0] = blk[0] + c * blk[2];
+                blk[1] = blk[1] + c * blk[3];
+            }
+            rhs[i * 2] = rhs[i * 2] + c * rhs[i * 2 + 1];
+        } else {
+            double binv[9];
+            memcpy(binv, ac, sizeof(binv));
+            inv3(binv);
+            const double c0 = binv[0], c1 = binv[1];
+            for (int j = ia[i]; j < ia[i + 1]; j++) {
+                double *blk = a + (size_t)j * 9;
+                blk[0] = blk[0] + c0 * blk[3] + c1 * blk[6];
+                blk[1] = blk[1] + c0 * blk[4] + c1 * blk[7];
+                blk[2] = blk[2] + c0 * blk[5] + c1 * blk[8];
+            }
+            rhs[i * 3] = rhs[i * 3] + c0 * rhs[i * 3 + 1] + c1 * rhs[i * 3 + 2];
+        }
+    }
+    free(Ac);
+}
+
+/* jxf_BSRMatrixDecouple, jxf_bsr_decoup.c:1273-1348 (types: 0 none, 1 ABF, 2 ANL, 3 SEM, 4 QI,
+ * 5 TIMPES, 6 TIMPES2; thermal applies to 2-4) */
+int orc_bsr_decouple2(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
+                      int thermal, int consistent_rhs)
 {
     if (bs != 2 && bs != 3) return 4;
     switch (type) {
         case 0: return 0;
         case 1: abf(nb, bs, ia, a, rhs, consistent_rhs); return 0;
+        case 2:
+        case 3:
+        case 4: row_transform(nb, bs, type, thermal, ia, a, rhs, consistent_rhs); return 0;
         case 5: timpes(nb, bs, ia, ja, a, rhs); return 0;
+        case 6: timpes2(nb, bs, ia, ja, a, rhs); return 0;
         default: return 4;
     }
+}
+
+int orc_bsr_decouple(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
+                     int consistent_rhs)
+{
+    return orc_bsr_decouple2(nb, bs, ia, ja, a, rhs, type, 0, consistent_rhs);
 }
 
 /* jxf_RestrictPressureVector, jxfpamg-0220/csrc/cpr/jxf_cpr.c:74-100 */

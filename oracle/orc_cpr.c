@@ -146,10 +146,59 @@ void orc_hgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a
     free(vt);
 }
 
+/* jxf_ParBSRHSGSRelax, jxfpamg-0220/csrc/amg/par_relax_bsr.c:579-1062, one
+ * rank, one thread: a forward block Gauss-Seidel pass over the rows, then a
+ * backward one, both reading the current iterate.  With w = omega = 1 each
+ * point is x_i = A_ii^-1 (b_i - sum_j A_ij x_j); otherwise
+ * x_i = (1 - w omega) x_i + w A_ii^-1 (omega b_i + res0 + (1 - omega) res2),
+ * res0 = -sum_j A_ij x_j, res2 = sum_j A_ij Vtemp_j, where Vtemp is the
+ * caller's work vector of which only the first nb entries (nb = block rows,
+ * not nb*bs unknowns) are refreshed from x at the start (:865); the others
+ * keep what the work vector held before. */
+void orc_hsgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                    double *work, double w, double omega)
+{
+    const int b2 = bs * bs;
+    const double eps = 2.220446049250313e-16; /* DBL_EPSILON */
+    const int plain = fabs(w - 1) < eps && fabs(omega - 1) < eps;
+    const double prod = 1.0 - w * omega, omo = 1.0 - omega;
+    if (!plain)
+        for (int i = 0; i < nb; i++) work[i] = x[i];
+    for (int pass = 0; pass < 2; pass++) {
+        const int begin = pass == 0 ? 0 : nb - 1, end = pass == 0 ? nb : -1, step = pass == 0 ? 1 : -1;
+        for (int i = begin; i != end; i += step) {
+            double res[3], res0[3], res2[3], tmp[3], out[3];
+            for (int k = 0; k < bs; k++) {
+                res[k] = b[i * bs + k];
+                res0[k] = 0.0;
+                res2[k] = 0.0;
+            }
+            if (plain) {
+                for (int jj = ia[i] + 1; jj < ia[i + 1]; jj++)
+                    blk_matvec_stable(-1.0, a + (size_t)jj * b2, x + (size_t)ja[jj] * bs, res, bs);
+                blk_inv_matvec(a + (size_t)ia[i] * b2, res, out, bs);
+                for (int k = 0; k < bs; k++) x[i * bs + k] = out[k];
+                continue;
+            }
+            for (int jj = ia[i] + 1; jj < ia[i + 1]; jj++) {
+                blk_matvec_stable(-1.0, a + (size_t)jj * b2, x + (size_t)ja[jj] * bs, res0, bs);
+                blk_matvec_stable(1.0, a + (size_t)jj * b2, work + (size_t)ja[jj] * bs, res2, bs);
+            }
+            for (int k = 0; k < bs; k++) tmp[k] = omega * res[k] + res0[k] + omo * res2[k];
+            blk_inv_matvec(a + (size_t)ia[i] * b2, tmp, out, bs);
+            for (int k = 0; k < bs; k++) {
+                x[i * bs + k] *= prod;
+                x[i * bs + k] += w * out[k];
+            }
+        }
+    }
+}
+
 /* ---------------------------------------------------------------------------
  * CPR: setup (jxfpamg-0220/csrc/cpr/jxf_cpr.c:268-422) and apply (:424-610):
  * restrict -> one AMG V-cycle from zero -> prolong (overwrite) -> stage2_maxit
- * forward HGS sweeps (w = 0.7, omega = 0.9).
+ * stage-2 sweeps (w = 0.7, omega = 0.9): forward HGS (stage2_type 2) or HSGS
+ * (3, with the CPR's work vector, zero when created, :396).
  * ------------------------------------------------------------------------ */
 void orc_cpr_setup(orc_cpr *C, int nb, int bs, const int *ia, const int *ja, const double *a, int stage2_maxit)
 {
@@ -160,6 +209,8 @@ void orc_cpr_setup(orc_cpr *C, int nb, int bs, const int *ia, const int *ja, con
     C->ja = ja;
     C->a = a;
     C->stage2_maxit = stage2_maxit;
+    C->stage2_type = 2;
+    C->work = (double *)calloc((size_t)nb * bs + 1, sizeof(double));
     orc_csr *Ap = &C->Ap;
     Ap->n = nb;
     Ap->m = nb;
@@ -177,13 +228,18 @@ void orc_cpr_apply(const orc_cpr *C, const double *r, double *z)
     orc_restrict(nb, bs, 0, r, rp);
     orc_amg_vcycle(&C->amg, rp, xp);
     orc_prolong(nb, bs, 0, xp, z);
-    for (int s = 0; s < C->stage2_maxit; s++) orc_hgs_relax(nb, bs, C->ia, C->ja, C->a, z, r, 0.7, 0.9, 1);
+    for (int s = 0; s < C->stage2_maxit; s++) {
+        if (C->stage2_type == 3) orc_hsgs_relax(nb, bs, C->ia, C->ja, C->a, z, r, C->work, 0.7, 0.9);
+        else orc_hgs_relax(nb, bs, C->ia, C->ja, C->a, z, r, 0.7, 0.9, 1);
+    }
     free(rp);
     free(xp);
 }
 
 void orc_cpr_free(orc_cpr *C)
 {
+    free(C->work);
+    C->work = NULL;
     orc_amg_free(&C->amg);
     orc_csr_free(&C->Ap);
 }

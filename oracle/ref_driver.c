@@ -107,18 +107,39 @@ int ref_bsr_matvec(int nb, int bs, const int *ia, const int *ja, const double *a
 }
 
 /* In-place decoupling of a (values only) and rhs (jxf_bsr_decoup.c:1273-1348). */
-int ref_bsr_decouple(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type, int quiet)
+int ref_bsr_decouple2(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type,
+                      int thermal, int quiet)
 {
     jxf_BSRMatrix *A = make_bsr(nb, bs, ia, ja, a);
     jxf_Vector *vb = make_vec(nb * bs, rhs);
     quiet_begin(quiet);
-    int ierr = jxf_BSRMatrixDecouple(A, vb, (JXF_DecoupType)type, 0);
+    int ierr = jxf_BSRMatrixDecouple(A, vb, (JXF_DecoupType)type, thermal);
     quiet_end(quiet);
     memcpy(a, jxf_BSRMatrixData(A), sizeof(double) * (size_t)ia[nb] * bs * bs);
     memcpy(rhs, jxf_VectorData(vb), sizeof(double) * nb * bs);
     jxf_SeqVectorDestroy(vb);
     jxf_BSRMatrixDestroy(A);
     return ierr;
+}
+
+int ref_bsr_decouple(int nb, int bs, const int *ia, const int *ja, double *a, double *rhs, int type, int quiet)
+{
+    return ref_bsr_decouple2(nb, bs, ia, ja, a, rhs, type, 0, quiet);
+}
+
+/* `sweeps` jxf_ParBSRHSGSRelax calls (par_relax_bsr.c:579-1062) updating x in place; work is the
+ * caller's Vtemp vector (nb * bs, in/out: the reference refreshes only its first nb entries). */
+int ref_hsgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                   double *work, double relax_weight, double omega, int sweeps)
+{
+    jxf_BSRMatrix *A = make_bsr(nb, bs, ia, ja, a);
+    jxf_ParBSRMatrix *Ap = to_par(A);
+    jxf_Vector *vx = make_vec(nb * bs, x), *vb = make_vec(nb * bs, b), *vw = make_vec(nb * bs, work);
+    jxf_ParVector *px = to_par_vec(Ap, vx), *pb = to_par_vec(Ap, vb), *pw = to_par_vec(Ap, vw);
+    for (int s = 0; s < sweeps; s++) jxf_ParBSRHSGSRelax(Ap, px, pb, pw, relax_weight, omega, 1);
+    memcpy(x, pvec_data(px), sizeof(double) * nb * bs);
+    memcpy(work, pvec_data(pw), sizeof(double) * nb * bs);
+    return 0;
 }
 
 /* One jxf_ParBSRHGSRelax sweep (par_relax_bsr.c:193-573) updating x in place. */

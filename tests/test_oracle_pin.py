@@ -26,11 +26,14 @@ def test_bsr_matvec_pin(systems, name, alpha, beta):
 
 
 @pytest.mark.parametrize("name", NAMES)
-@pytest.mark.parametrize("code", [1, 5])
-def test_decouple_pin(systems, name, code):
+@pytest.mark.parametrize("code", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("thermal", [False, True])
+def test_decouple_pin(systems, name, code, thermal):
+    """ABF, ANL, SEM, QI, True-IMPES and its second form, with and without the thermal variant
+    (which only ANL / SEM / QI read), bit for bit against the reference library."""
     s = systems(name)
-    a1, r1 = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, code)
-    a2, r2 = oracle.ref_bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, code)
+    a1, r1 = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, code, thermal=thermal)
+    a2, r2 = oracle.ref_bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, code, thermal=thermal)
     assert np.array_equal(a1, a2)
     assert np.array_equal(r1, r2)
 
@@ -77,3 +80,46 @@ def test_cpr_and_gmres_pin_live(systems, name):
     orc = oracle.gmres(s.ia, s.ja, a, s.block_size, b, tol=1e-6, max_iter=200, cpr=O)
     assert ref["iters"] == orc["iters"]
     assert np.array_equal(ref["x"], orc["x"])
+
+
+@pytest.mark.parametrize("code", [2, 3, 4, 6])
+def test_row_transform_consistent_rhs_keeps_solution(systems, code):
+    """With the right-hand side transformed by the same row operation as the matrix, x_true still
+    solves the decoupled system (the reference's aliased update does not keep it for ANL/SEM/QI)."""
+    from jxpamg_all_b200.synth import bsr_matvec_np
+
+    for name in ("tiny", "tiny3"):
+        s = systems(name)
+        a1, r1 = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, code, consistent_rhs=True)
+        res = bsr_matvec_np(s.ia, s.ja, a1, s.block_size, s.x_true) - r1
+        assert np.linalg.norm(res) <= 1e-10 * np.linalg.norm(r1)
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("weights", [(0.7, 0.9), (1.0, 1.0)])
+def test_hsgs_relax_pin(systems, name, weights):
+    """jxf_ParBSRHSGSRelax (forward + backward pass; the work vector refreshed only in its first
+    nb entries) against the reference, two calls in a row."""
+    s = systems(name)
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
+    rng = np.random.default_rng(11)
+    x0, w0 = rng.standard_normal(s.n), rng.standard_normal(s.n)
+    x1, k1 = oracle.hsgs_relax(s.ia, s.ja, a, s.block_size, x0, b, w0, *weights, sweeps=2)
+    x2, k2 = oracle.ref_hsgs_relax(s.ia, s.ja, a, s.block_size, x0, b, w0, *weights, sweeps=2)
+    assert np.array_equal(x1, x2) and np.array_equal(k1, k2)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_cpr_hsgs_stage2_pin(systems, name):
+    """CPR with stage2_solver_type 3 (HSGS): two applications in a row and the full solve."""
+    s = systems(name)
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
+    R = oracle.RefCPR(s.ia, s.ja, a, s.block_size, stage2_type=3)
+    O = oracle.OracleCPR(s.ia, s.ja, a, s.block_size, stage2_type=3)
+    r = np.random.default_rng(5).standard_normal(s.n)
+    assert np.array_equal(R.apply(r), O.apply(r))
+    assert np.array_equal(R.apply(b), O.apply(b))
+    ref = oracle.ref_gmres(s.ia, s.ja, s.a, s.block_size, s.b, decouple=1, tol=1e-6, max_iter=200, stage2_type=3)
+    orc = oracle.gmres(s.ia, s.ja, a, s.block_size, b, tol=1e-6, max_iter=200,
+                       cpr=oracle.OracleCPR(s.ia, s.ja, a, s.block_size, stage2_type=3))
+    assert ref["iters"] == orc["iters"]
