@@ -12,10 +12,16 @@ are not available).
 One step = one solve from x0 = 0 to FP64 rel-res <= 1e-6 (GMRES confirms the
 true residual b - A x in FP64 before it reports convergence).
   value : device-resident solve with the measured path (FP32 preconditioner,
-          learned per-level strength thresholds and Chebyshev intervals,
-          flexible FP64 GMRES), seconds; config.plain_fp64_s is the same
-          measurement for the plain FP64 path and config.speedup_vs_plain_fp64
-          their ratio.
+          learned per-level strength thresholds and Chebyshev intervals, the
+          stage-2 weights of the reference's mixed-precision driver, flexible
+          FP64 GMRES run on the device as one CUDA graph), seconds;
+          config.plain_fp64_s is the same measurement for the plain FP64 path
+          (the reference's CPR weights, host-driven MGS GMRES) and
+          config.speedup_vs_plain_fp64 their ratio; config.*same_driver* is
+          the plain FP64 preconditioner under the measured path's weights and
+          GMRES driver (what precision + learned settings alone gain), and
+          config.hybrid_* the reference's hybrid form (FP32 stage 1, FP64
+          stage-2 polish).
   e2e   : the measured path through the public C ABI from pinned host buffers,
           timed per step from the host->device upload of the matrix and b,
           through decoupling, CPR setup and solve, to the device->host read
@@ -68,11 +74,20 @@ WORKLOADS = {
 # plain FP64 GPU path (the comparison): the reference's method in the throughput ordering
 PLAIN_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0,
                   precision=0, fast_smoother=0)
-# measured path: FP32 preconditioner + learned settings, flexible FP64 GMRES
-SOLVER_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=2, flexible=1)
+# measured path: FP32 preconditioner + learned settings, the stage-2 weights of the reference's
+# mixed-precision driver (1.0 / 0.8, src/test_bsr_cprgmres_hybrid.c:373-374; its plain CPR uses
+# 0.7 / 0.9, jxf_cpr.c:547-548), flexible FP64 GMRES run on the device as one CUDA graph
+SOLVER_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=2, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8,
+                   graph_gmres=1)
+# ablation: the plain FP64 preconditioner with the measured path's stage-2 weights and GMRES driver,
+# so that what precision + learned settings alone gain is visible
+PLAIN_SAME_DRIVER_OPTS = dict(PLAIN_OPTS, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8, graph_gmres=1)
+# the reference's hybrid form (src/test_bsr_cprgmres_hybrid.c:217-439): FP32 stage 1, FP64 stage-2 polish
+# with weights 1.0 / 0.8, on the plain smoothers
+HYBRID_OPTS = dict(PLAIN_OPTS, precision=3, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8)
 BATCH_METRIC = "batched CPR-GMRES solves per second to 1e-6 FP64 rel-res (64 uneven systems), 1xB200"
 # batched solves: mixed precision (FP32 preconditioner), Chebyshev-3 on the dense levels, flexible FP64 GMRES
-BATCH_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=1, flexible=1)
+BATCH_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=1, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8)
 
 
 # per-workload method choices: the three-phase system is decoupled by True-IMPES and solved with
@@ -317,6 +332,15 @@ def run_ours(args):
     roof_plain = roofline_stage2(P, s, stream, 8)
     P.close()
 
+    # ---- the reference's hybrid form (FP32 stage 1 + FP64 polish), for comparison ------
+    Hy = make(dict(HYBRID_OPTS, **CONFIG_OPTS.get(args.config, {})))
+    hybrid_t, hybrid_it, hybrid_rel, _, _ = timed(Hy, "hybrid FP32/FP64")
+    Hy.close()
+    # ---- ablation: plain FP64 preconditioner, measured path's weights and GMRES driver ----
+    Pd = make(dict(PLAIN_SAME_DRIVER_OPTS, **CONFIG_OPTS.get(args.config, {})))
+    plain_d_t, plain_d_it, _, _, _ = timed(Pd, "plain FP64, same driver")
+    Pd.close()
+
     # ---- measured path: mixed precision + learned settings ------------------------
     G = make(measured_opts)
     setup_stats = G.stats()
@@ -382,14 +406,20 @@ def run_ours(args):
                                  " decoupling, AMG V(1,1) (HMIS, ext+i) "
                                  "+ 3 block-GS stage-2 sweeps",
                        "measured_path": "mixed+learned: FP32 preconditioner storage/arithmetic (AMG levels, transfers, "
-                                        "stage 2), FP64 flexible GMRES / SpMV / true residual / coarsest solve; learned "
-                                        "per-level strength thresholds and Chebyshev-3 intervals (" +
+                                        "stage 2 with the reference mixed driver's weights 1.0/0.8), FP64 flexible "
+                                        "GMRES run on the device as one CUDA graph / SpMV / true residual / coarsest "
+                                        "solve; learned per-level strength thresholds and Chebyshev-3 intervals (" +
                                         ("kept" if learned["learned_used"] else "rejected by the probe: plain smoothers")
-                                        + ")",
+                                        + "); the plain FP64 path is the reference's CPR (weights 0.7/0.9) with its "
+                                        "host-driven MGS GMRES",
                        "options": measured_opts,
                        "iterations": it_m, "final_rel_res": rel_m,
                        "plain_fp64_s": plain_t, "plain_fp64_iterations": plain_it, "plain_fp64_rel_res": plain_rel,
                        "speedup_vs_plain_fp64": plain_t / per_solve,
+                       "hybrid_fp32_fp64_s": hybrid_t, "hybrid_iterations": hybrid_it,
+                       "plain_fp64_same_driver_s": plain_d_t, "plain_fp64_same_driver_iterations": plain_d_it,
+                       "speedup_vs_plain_fp64_same_driver": plain_d_t / per_solve,
+                       "hybrid_speedup_vs_plain_fp64": plain_t / hybrid_t,
                        "x_rel_diff_vs_plain_fp64": err_vs_fp64,
                        "learned": learned,
                        "setup_s": setup_stats["setup_ms"] / 1e3, "plain_setup_s": plain_setup["setup_ms"] / 1e3,

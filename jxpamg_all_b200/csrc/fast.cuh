@@ -13,7 +13,12 @@
 //                preconditioner (GMRES, its SpMV, the true residual and the
 //                coarsest dense solve stay FP64);
 //   precision 2: as 1, plus BF16 values with a per-row FP32 scale on levels
-//                >= bf16_level.
+//                >= bf16_level;
+//   precision 3: the reference's hybrid form (src/test_bsr_cprgmres_hybrid.c:
+//                217-439): restriction, AMG and prolongation in FP32, the
+//                stage-2 sweeps in FP64 on the FP64 block matrix (that driver
+//                polishes with weights 1.0 / 0.8, stage2_relax_weight /
+//                stage2_omega).
 //
 // Level smoothers: multicolour Gauss-Seidel (sparse levels, one launch per
 // colour class over a colour-contiguous row copy), l1-Jacobi (dense levels),
@@ -82,7 +87,7 @@ struct FastLevel {
 };
 
 struct FastOptions {
-    int precision = 0;      // 0 FP64, 1 FP32, 2 FP32 + BF16 coarse levels
+    int precision = 0;      // 0 FP64, 1 FP32, 2 FP32 + BF16 coarse levels, 3 FP32 stage 1 + FP64 stage 2
     int bf16_level = 1;     // precision 2: first level stored in BF16
     int smoother = 0;       // 0 colour GS / l1-Jacobi, 1 Chebyshev-3 on the l1-Jacobi levels, 2 on every level
     double cheb_lower = 0.3, cheb_upper = 1.1;  // interval [lower, upper] * lambda_max(D^-1 A)

@@ -487,17 +487,17 @@ struct FastCpr final : FastCprBase {
         }
     }
 
-    template <typename TV, typename TXV>
+    template <typename TV, typename TXV, typename TAC>
     void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp,
-                        TA w, TA om, int plain, cudaStream_t s) {
+                        TAC w, TAC om, int plain, cudaStream_t s) {
         const int grid = div_up((long long)(r1 - r0) * V, 128);
 #define JX_HGS_CSR(VV)                                                                                        \
     do {                                                                                                      \
         if (bs == 2)                                                                                          \
-            fk::hgs_color<2, VV, TV, TA, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, \
+            fk::hgs_color<2, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
                                                                     z, vtp, w, om, plain);                     \
         else                                                                                                  \
-            fk::hgs_color<3, VV, TV, TA, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r, \
+            fk::hgs_color<3, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
                                                                     z, vtp, w, om, plain);                     \
     } while (0)
         switch (V) {
@@ -524,16 +524,17 @@ struct FastCpr final : FastCprBase {
         for (size_t c = 0; c + 1 < M.seg.size(); ++c) {
             const int r0 = M.seg[c], r1 = M.seg[c + 1];
             if (r1 <= r0) continue;
-            if constexpr (std::is_same<TX, double>::value)
-                launch_stage2<double, TXV>(M, M.a64.get(), r0, r1, r, z, vtp, w, om, plain, s);
+            if (M.kind == VAL_F64)  // FP64 path, and the hybrid form's FP64 stage 2: FP64 values and arithmetic
+                launch_stage2<double, TXV, double>(M, M.a64.get(), r0, r1, r, z, vtp, cfg.stage2_w, cfg.stage2_omega,
+                                                   plain, s);
             else
-                launch_stage2<float, TXV>(M, M.a32.get(), r0, r1, r, z, vtp, w, om, plain, s);
+                launch_stage2<float, TXV, TA>(M, M.a32.get(), r0, r1, r, z, vtp, w, om, plain, s);
             JX_LAUNCH_CHECK();
         }
     }
     // FP64 interface (C ABI / tests): the mixed path converts in and out.
     void stage2_sweep(const double *r, double *z, cudaStream_t s) override {
-        if constexpr (std::is_same<TX, double>::value) {
+        if (std::is_same<TX, double>::value || st2.kind == VAL_F64) {
             sweep_typed<double>(r, z, vt.get(), s);
         } else {
             const long long n = (long long)nb * bs;
@@ -547,16 +548,16 @@ struct FastCpr final : FastCprBase {
             JX_LAUNCH_CHECK();
         }
     }
-    template <typename TV, typename TXV>
-    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp, TA w,
-                       TA om, int plain, cudaStream_t s) {
+    template <typename TV, typename TXV, typename TAC>
+    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp, TAC w,
+                       TAC om, int plain, cudaStream_t s) {
         if (M.sell) {
             const int grid = div_up(r1 - r0, kThreads);
             if (bs == 2)
-                fk::hgs_sell<2, TV, TA, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                fk::hgs_sell<2, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
                                                                        M.rows.get(), r, z, vtp, w, om, plain);
             else
-                fk::hgs_sell<3, TV, TA, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                fk::hgs_sell<3, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
                                                                        M.rows.get(), r, z, vtp, w, om, plain);
         } else {
             launch_hgs_csr<TV, TXV>(opt.stage2_lanes, M, a, r0, r1, r, z, vtp, w, om, plain, s);
@@ -633,7 +634,8 @@ struct FastCpr final : FastCprBase {
             JX_LAUNCH_CHECK();
         }
         const bool st2_on = cfg.stage2_solver_type == 2 && cfg.stage2_maxit > 0;
-        if (fp64 || !st2_on) {
+        if (fp64 || !st2_on || st2.kind == VAL_F64) {
+            // FP64 stage 2 on the caller's vectors (FP64 path; hybrid form: FP32 stage 1, FP64 polish)
             fk::prolong_p<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index,
                                                                               L0.u.get(), z);
             JX_LAUNCH_CHECK();
@@ -673,6 +675,7 @@ struct FastCpr final : FastCprBase {
     }
 
     DevBuf<TX> nat_r, nat_z;
+    DevBuf<double> nat_r64, nat_z64;  // hybrid form: the FP64 stage 2 timed on FP64 vectors
     void stage2_native(int sweeps, cudaStream_t s) override {
         const long long n = (long long)nb * bs;
         if (!n) return;
@@ -683,10 +686,19 @@ struct FastCpr final : FastCprBase {
             nat_z.zero(s);
         }
         for (int k = 0; k < sweeps; ++k) {
-            if constexpr (std::is_same<TX, double>::value)
+            if constexpr (std::is_same<TX, double>::value) {
                 sweep_typed<double>(nat_r.get(), nat_z.get(), vt.get(), s);
-            else
+            } else if (st2.kind == VAL_F64) {
+                if (!nat_r64.get()) {
+                    nat_r64.alloc(n);
+                    nat_z64.alloc(n);
+                    nat_r64.zero(s);
+                    nat_z64.zero(s);
+                }
+                sweep_typed<double>(nat_r64.get(), nat_z64.get(), vt.get(), s);
+            } else {
                 sweep_typed<float>(nat_r.get(), nat_z.get(), vt32.get(), s);
+            }
         }
     }
 
@@ -705,7 +717,8 @@ struct FastCpr final : FastCprBase {
         }
         total += (double)nc * nc * 8.0;
         const double bsz = bs * bs;
-        total += cfg.stage2_maxit * ((double)st2.nnz * (bsz * vb(st2.kind) + 4.0) + 4.0 * nb * bs * xb);
+        const double xb2 = st2.kind == VAL_F64 ? 8.0 : xb;
+        total += cfg.stage2_maxit * ((double)st2.nnz * (bsz * vb(st2.kind) + 4.0) + 4.0 * nb * bs * xb2);
         return total;
     }
 
@@ -827,7 +840,8 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
     }
     if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
-        const int kind = fp64 ? VAL_F64 : VAL_F32;
+        // the hybrid form (precision 3) keeps the stage-2 block matrix in FP64
+        const int kind = (fp64 || opt.precision == 3) ? VAL_F64 : VAL_F32;
         const std::string key = tune_key("stage2", A.nb, A.nnzb, kind, A.bs * A.bs, opt.autotune);
         TuneChoice cached_choice;
         bool cached = false;

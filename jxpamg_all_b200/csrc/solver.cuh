@@ -57,7 +57,8 @@ struct SolverParams {
     int max_colors = 8;
     int use_tma_spmv = 0;
     // fast path (smoother_order 1)
-    int precision = 0;       // 0 FP64, 1 FP32 preconditioner, 2 FP32 + BF16 coarse levels
+    int precision = 0;       // 0 FP64, 1 FP32 preconditioner, 2 FP32 + BF16 coarse levels, 3 the reference's
+                             // hybrid form: FP32 restriction / AMG / prolongation, FP64 stage 2 on the FP64 matrix
     int bf16_level = 1;      // precision 2: first BF16 level
     int fast_smoother = 0;   // 0 colour GS / l1-Jacobi; 1 Chebyshev-3 on the levels without a GS colouring;
                              // 2 as 1 with learned thresholds and intervals; 3 Chebyshev-3 on every level

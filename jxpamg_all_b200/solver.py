@@ -144,6 +144,12 @@ class CprGmres:
         _lib.check(self._so.jxcpr_solver_cpr_apply(self.h, _ptr(np.ascontiguousarray(r, np.float64)), _ptr(z), 0))
         return z
 
+    def stage2_sweep(self, b, x0):
+        """One stage-2 sweep of the set-up preconditioner on A x = b from x0 (host arrays)."""
+        x = np.array(x0, dtype=np.float64)
+        _lib.check(self._so.jxcpr_solver_stage2_sweep(self.h, _ptr(np.ascontiguousarray(b, np.float64)), _ptr(x), 0))
+        return x
+
     def vcycle(self, rp, xp=None):
         xp = np.zeros(self.nb) if xp is None else np.array(xp, dtype=np.float64)
         _lib.check(self._so.jxcpr_solver_vcycle(self.h, _ptr(np.ascontiguousarray(rp, np.float64)), _ptr(xp), 0))

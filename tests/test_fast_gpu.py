@@ -43,6 +43,9 @@ VARIANTS = [
     dict(precision=0, fast_smoother=0, orthog=1),
     dict(precision=1, fast_smoother=1, flexible=1, autotune=0, graphs=0),
     dict(precision=0, fast_smoother=1, strong_threshold=0.5, strong_threshold_coarse=0.7),
+    # the reference's hybrid form: FP32 stage 1, FP64 stage 2 polish with weights 1.0 / 0.8
+    dict(precision=3, fast_smoother=0, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8),
+    dict(precision=3, fast_smoother=1, flexible=1),
 ]
 
 
@@ -109,3 +112,19 @@ def test_stage2_native_and_autotune_report(systems):
     lib.check(lib.load().jxcpr_solver_stage2_native(G.h, 2))
     rep = G.setup_report()
     assert "tuned stage2" in rep and "tuned A0" in rep
+
+
+def test_hybrid_stage2_is_fp64(systems):
+    """precision 3 runs stage 2 in FP64 on the FP64 matrix: with the stage-1 AMG switched off
+    (stage1_maxit 0 is not allowed, so compare stage-2 sweeps directly) one sweep from the same
+    iterate matches the FP64 fast path's sweep to FP64 rounding."""
+    s = systems("c0")
+    rng = np.random.default_rng(4)
+    r = rng.standard_normal(s.n)
+    z0 = rng.standard_normal(s.n)
+    out = []
+    for p in (0, 3):
+        G, *_ = solve(s, precision=p, fast_smoother=0, flexible=1, autotune=0)
+        out.append(G.stage2_sweep(r, z0))
+        G.close()
+    assert np.linalg.norm(out[0] - out[1]) <= 1e-12 * np.linalg.norm(out[0])
