@@ -473,7 +473,12 @@ def roofline_stage2(G, s, stream, value_bytes):
     # values + column indices + row pointers, b/x/vt read once, x written once, start-of-sweep copy (read+write)
     alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * xb * 6
     achieved = alg / sec / 1e9
-    return {"bound": "hbm", "kernel": f"stage-2 block hybrid Gauss-Seidel sweep (hgs_sell<{bs}>, "
+    layout = "?"
+    for line in G.setup_report().splitlines():
+        if line.startswith("tuned stage2") and " layout " in line:
+            layout = line.split(" layout ")[1].split()[0]
+    kname = f"hgs_sell<{bs}>" if layout == "sell" else f"hgs_color<{bs}> ({layout})"
+    return {"bound": "hbm", "kernel": f"stage-2 block hybrid Gauss-Seidel sweep ({kname}, "
             f"{'FP64' if value_bytes == 8 else 'FP32'} values, one launch per colour class + start copy)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": src, "traffic": None, "algorithmic_bytes": int(alg), "sweep_ms": sec * 1e3}

@@ -206,23 +206,34 @@ bool use_sell(const FastOptions &o, int n, long long nnz) {
     return n >= o.sell_min_rows && n > 0 && (double)nnz / n <= o.sell_max_mean;
 }
 
-// Device time (us) of one y = A x pass over M, averaged over `reps` after a warm-up.
-template <typename TX>
-double time_pass(const LevelMat &M, const TX *x, TX *y, cudaStream_t s, int reps = 3) {
-    fk::OpSpmv<TX> op{x, y, 0};
-    launch_rows<TX>(M, op, 0, M.nstored, s);
+// Device time (us) of `body`: the best of `trials` means over `reps` runs, after a warm-up run
+// (the minimum keeps one slow trial -- a clock ramp, another stream's burst -- from deciding).
+template <typename F>
+double time_best(F &&body, cudaStream_t s, int reps = 3, int trials = 3) {
+    body();
     cudaEvent_t e0, e1;
     JX_CUDA(cudaEventCreate(&e0));
     JX_CUDA(cudaEventCreate(&e1));
-    JX_CUDA(cudaEventRecord(e0, s));
-    for (int k = 0; k < reps; ++k) launch_rows<TX>(M, op, 0, M.nstored, s);
-    JX_CUDA(cudaEventRecord(e1, s));
-    JX_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    JX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    double best = 1e30;
+    for (int t = 0; t < trials; ++t) {
+        JX_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < reps; ++k) body();
+        JX_CUDA(cudaEventRecord(e1, s));
+        JX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        JX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, 1e3 * ms / reps);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return 1e3 * ms / reps;
+    return best;
+}
+
+// Device time (us) of one y = A x pass over M.
+template <typename TX>
+double time_pass(const LevelMat &M, const TX *x, TX *y, cudaStream_t s) {
+    fk::OpSpmv<TX> op{x, y, 0};
+    return time_best([&] { launch_rows<TX>(M, op, 0, M.nstored, s); }, s);
 }
 
 std::string layout_name(const LevelMat &M) {
@@ -873,20 +884,16 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
             DevBuf<double> rb((size_t)A.nb * A.bs), zb((size_t)A.nb * A.bs);
             rb.zero(s);
             zb.zero(s);
+            if (!fp64) {
+                F->r32.zero(s);
+                F->z32.zero(s);
+            }
+            // one sweep in the precision the preconditioner runs it in (no conversions timed)
             auto time_sweep = [&]() {
-                F->stage2_sweep(rb.get(), zb.get(), s);
-                cudaEvent_t e0, e1;
-                JX_CUDA(cudaEventCreate(&e0));
-                JX_CUDA(cudaEventCreate(&e1));
-                JX_CUDA(cudaEventRecord(e0, s));
-                for (int k = 0; k < 3; ++k) F->stage2_sweep(rb.get(), zb.get(), s);
-                JX_CUDA(cudaEventRecord(e1, s));
-                JX_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                JX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return 1e3 * ms / 3;
+                return time_best([&] {
+                    if (fp64 || F->st2.kind == VAL_F64) F->template sweep_typed<double>(rb.get(), zb.get(), F->vt.get(), s);
+                    else F->template sweep_typed<float>(F->r32.get(), F->z32.get(), F->vt32.get(), s);
+                }, s);
             };
             double best = 1e30;
             int best_lanes = 4;
