@@ -1,6 +1,8 @@
 // Fast CPR preconditioner: storage conversion (CSR / sliced ELL, FP64 / FP32 /
 // BF16), V-cycle and stage 2 (see fast.cuh for the modes).
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <memory>
@@ -246,10 +248,36 @@ struct TuneChoice {
     int sell = 0, lanes = 1;
     double us = 0.0;
 };
+// With JXCPR_TUNE_CACHE=<file> the choices also persist across processes: the
+// file is read at the first lookup and rewritten after every new timing, so a
+// later run (a profiler run, whose own timings would be distorted) uses the
+// layouts an undisturbed run chose.  Lines: key sell lanes us.
 std::mutex g_tune_mu;
-std::map<std::string, TuneChoice> &tune_cache() {
-    static std::map<std::string, TuneChoice> *c = new std::map<std::string, TuneChoice>();
+std::map<std::string, TuneChoice> &tune_cache() {  // the caller holds g_tune_mu
+    static std::map<std::string, TuneChoice> *c = nullptr;
+    if (!c) {
+        c = new std::map<std::string, TuneChoice>();
+        if (const char *path = getenv("JXCPR_TUNE_CACHE")) {
+            if (FILE *f = fopen(path, "r")) {
+                char key[200];
+                TuneChoice t;
+                while (fscanf(f, "%199s %d %d %lf", key, &t.sell, &t.lanes, &t.us) == 4) (*c)[key] = t;
+                fclose(f);
+            }
+        }
+    }
     return *c;
+}
+// The caller holds g_tune_mu.
+void tune_store(const std::string &key, const TuneChoice &t) {
+    tune_cache()[key] = t;
+    if (const char *path = getenv("JXCPR_TUNE_CACHE")) {
+        if (FILE *f = fopen(path, "w")) {
+            for (auto &kv : tune_cache())
+                fprintf(f, "%s %d %d %.6f\n", kv.first.c_str(), kv.second.sell, kv.second.lanes, kv.second.us);
+            fclose(f);
+        }
+    }
 }
 // mode 1: the exact shape; mode 2 (shared): the shape class -- rows within a
 // half octave, mean row length within 0.5 -- so similar operators of other
@@ -317,7 +345,7 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
             }
         }
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        tune_cache()[key] = best;
+        tune_store(key, best);
     }
     char line[200];
     snprintf(line, sizeof line, "%s rows %d mean %.1f layout %s %.2f us%s", name, n, n ? (double)nnz / n : 0.0,
@@ -925,7 +953,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
             c.lanes = F->opt.stage2_lanes;
             c.us = best;
             std::lock_guard<std::mutex> lk(g_tune_mu);
-            tune_cache()[key] = c;
+            tune_store(key, c);
         }
     }
     JX_CUDA(cudaStreamSynchronize(s));
