@@ -329,7 +329,7 @@ def run_ours(args):
     plain_setup = P.stats()
     plain_t, plain_it, plain_rel, _, clk_p = timed(P, "plain FP64")
     x_plain = d_x.cpu().numpy().copy()
-    roof_plain = roofline_stage2(P, s, stream, 8)
+    roof_plain = roofline_stage2(P, s, stream, 8, args.config)
     P.close()
 
     # ---- the reference's hybrid form (FP32 stage 1 + FP64 polish), for comparison ------
@@ -348,7 +348,7 @@ def run_ours(args):
     per_solve, it_m, rel_m, launches, clocks = timed(G, "mixed+learned")
     x_mixed = d_x.cpu().numpy().copy()
     err_vs_fp64 = float(np.linalg.norm(x_mixed - x_plain) / np.linalg.norm(x_plain))
-    roof = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) == 0 else 4)
+    roof = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) in (0, 3) else 4, args.config)
     G.close()
     if clk_p.get("reasons"):
         clocks["reasons"] = sorted(set(clocks.get("reasons", [])) | set(clk_p["reasons"]))
@@ -443,7 +443,13 @@ def run_ours(args):
     return 0
 
 
-def roofline_stage2(G, s, stream, value_bytes):
+# DRAM traffic of one stage-2 sweep's kernels (both colour launches), from an ncu capture of the same
+# solve (dram__bytes_read.sum + dram__bytes_write.sum, layouts reused through JXCPR_TUNE_CACHE):
+# (workload, value bytes, layout) -> bytes.
+STAGE2_TRAFFIC_BYTES = {("c1", 4, "sell"): 2 * 108.9e6}
+
+
+def roofline_stage2(G, s, stream, value_bytes, cfg="c1"):
     """Roofline of the stage-2 block Gauss-Seidel sweep (one launch per colour
     class) in the path's own storage precision: algorithmic bytes of one sweep /
     mean sweep time (CUDA events on the solver's stream)."""
@@ -481,7 +487,9 @@ def roofline_stage2(G, s, stream, value_bytes):
     return {"bound": "hbm", "kernel": f"stage-2 block hybrid Gauss-Seidel sweep ({kname}, "
             f"{'FP64' if value_bytes == 8 else 'FP32'} values, one launch per colour class + start copy)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": src, "traffic": None, "algorithmic_bytes": int(alg), "sweep_ms": sec * 1e3}
+            "peak_source": src, "traffic": STAGE2_TRAFFIC_BYTES.get((cfg, value_bytes, layout)),
+            "traffic_note": "ncu DRAM bytes of the sweep's colour launches (copy excluded); null where not captured",
+            "algorithmic_bytes": int(alg), "sweep_ms": sec * 1e3}
 
 
 # ---------------------------------------------------------------------------
