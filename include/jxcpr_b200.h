@@ -184,6 +184,12 @@ JXCPR_API int jxcpr_solver_level_features(jxcpr_solver *solver, int level, float
  * hierarchy, modelled bytes per GMRES iteration with each}.  The setup keeps the learned settings
  * unless their residual reduction per byte is worse. */
 JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
+/* Solves since the last setup in which the learned settings stalled (no convergence within three times
+ * the iterations the probe's residual reduction predicts, and at least that plus one restart cycle) and
+ * the plain preconditioner (default strength thresholds, plain smoothers) was built in their place for
+ * the rest of the solve and for later solves.  When the setup probe rejects the learned settings, the
+ * same plain preconditioner is built at once (learned_status reports them unused). */
+JXCPR_API int jxcpr_solver_learned_fallbacks(jxcpr_solver *solver);
 
 /* ---- batched solves: many set-up solvers, one graph launch; no reference counterpart -------------
  * create: records every solver's whole GMRES solve (option graph_gmres is switched on: flexible GMRES

@@ -282,6 +282,8 @@ int jxcpr_solver_learned_status(jxcpr_solver *h, double *out) {
     return JXCPR_SUCCESS;
 }
 
+int jxcpr_solver_learned_fallbacks(jxcpr_solver *h) { return h ? h->s.learned_fallbacks : -1; }
+
 int jxcpr_solver_level_cf(jxcpr_solver *h, int lev, int *cf) {
     if (!h || !cf || lev < 0 || lev >= h->s.cpr.amg.num_levels() - 1) return -1;
     const std::vector<int> &v = h->s.cpr.amg.levels[lev]->cf;

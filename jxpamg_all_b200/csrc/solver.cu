@@ -555,6 +555,8 @@ void Solver::setup(int nb, int bs, long long nnzb, const int *ia, const int *ja,
     pool_stats(al0);
     auto t0 = std::chrono::steady_clock::now();
     ggmres.reset();  // its graph holds the previous setup's buffers
+    learned_fallbacks = 0;
+    learned_rebuilt = 0;
     A.alloc(nb, bs, nnzb);
     const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     JX_CUDA(cudaMemcpyAsync(A.ia.get(), ia, sizeof(int) * (nb + 1), kind, s));
@@ -624,12 +626,78 @@ void Solver::learned_probe(cudaStream_t s) {
     const double ep = rp > 0.0 ? -log(rp) / (bp + common) : 1e300;
     cpr.probe_bytes[0] = bl + common;
     cpr.probe_bytes[1] = bp + common;
-    if (el >= ep) cpr.fast->set_plain_mode(false);  // learned settings stay
-    else cpr.learned_used = 0;
     gmres.prm = saved;
+    if (el >= ep) {
+        cpr.fast->set_plain_mode(false);  // learned settings stay
+    } else {
+        // The learned settings lose: the plain method replaces them entirely -- the learned
+        // strength thresholds shaped the hierarchy too, so the plain smoothers on it are no
+        // fallback (they can stall where the default hierarchy converges quickly).
+        rebuild_plain(s);
+    }
 }
 
+// The plain fast-path preconditioner (default strength thresholds, plain smoothers) in place of
+// the learned one, on the already decoupled matrix.
+void Solver::rebuild_plain(cudaStream_t s) {
+    const int fs = cpr.prm.fast_smoother;
+    cpr.prm.fast_smoother = 0;
+    cpr.ready = false;
+    cpr.setup(A.view(), s);
+    cpr.prm.fast_smoother = fs;
+    cpr.learned_used = 0;
+    cpr.probe_pending = false;
+    learned_rebuilt = 1;
+    if (ggmres) ggmres->reset_graph();
+}
+
+// Learned settings are kept by a short probe at setup; if the full solve then
+// stalls -- no convergence within a budget of three times the iterations the
+// probe's residual reduction predicts (at least that plus one restart cycle)
+// -- the plain preconditioner (default thresholds, plain smoothers) is built in
+// their place and GMRES continues from the current iterate with the remaining
+// iterations.
 GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
+    const bool guard = cpr.fast && cpr.learned_used && prm.learned_fallback && cpr.factor_fast > 0.0 &&
+                       cpr.factor_fast < 1.0 && prm.tol > 0.0 && prm.tol < 1.0;
+    if (!guard) return solve_once(b_in, x_io, device);
+    const SolverParams saved = prm;
+    const double expect = std::ceil(std::log(prm.tol) / std::log(cpr.factor_fast));
+    const double want = std::max(3.0 * expect, expect + prm.k_dim);
+    const int budget = (int)std::min<double>(prm.max_iter, want);
+    prm.max_iter = budget;
+    GmresResult first;
+    try {
+        first = solve_once(b_in, x_io, device);
+    } catch (...) {
+        prm = saved;
+        throw;
+    }
+    prm = saved;
+    if (first.converged || first.status || first.iterations < budget || budget >= saved.max_iter) return first;
+    const double ms0 = solve_ms;
+    {
+        PoolStream scope(stream);
+        rebuild_plain(stream);
+    }
+    learned_fallbacks += 1;
+    prm.max_iter = saved.max_iter - first.iterations;
+    try {
+        last = solve_once(b_in, x_io, device);
+    } catch (...) {
+        prm = saved;
+        throw;
+    }
+    prm = saved;
+    last.iterations += first.iterations;
+    std::vector<double> h = first.norms;
+    if (last.norms.size() > 1) h.insert(h.end(), last.norms.begin() + 1, last.norms.end());
+    last.norms = h;
+    solve_ms += ms0;
+    return last;
+}
+
+GmresResult Solver::solve_once(const double *b_in, double *x_io, int device) {
     cudaStream_t s = stream;
     PoolStream scope(s);
     const long long n = (long long)A.nb * A.bs;

@@ -226,6 +226,10 @@ struct Solver {
     void setup(int nb, int bs, long long nnzb, const int *ia, const int *ja, const double *a, int device);
     // b, x host or device; x holds the initial guess on entry.
     GmresResult solve(const double *b_in, double *x_io, int device);
+    GmresResult solve_once(const double *b_in, double *x_io, int device);
+    int learned_fallbacks = 0;  // solves in which the learned settings stalled and the plain ones took over
+    int learned_rebuilt = 0;    // the plain preconditioner replaced the learned one (probe or stall)
+    void rebuild_plain(cudaStream_t s);
     void learned_probe(cudaStream_t s);
 };
 

@@ -79,6 +79,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_bilu_apply.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_level_features.argtypes = [P, c_int, P]
     lib.jxcpr_solver_learned_status.argtypes = [P, P]
+    lib.jxcpr_solver_learned_fallbacks.argtypes = [P]
     lib.jxcpr_pool_stats.argtypes = [P]
     lib.jxcpr_batch_setup.argtypes = [c_int, P, P, P, P, P, P, P, c_int, c_int, P]
     lib.jxcpr_batch_create.argtypes = [ctypes.POINTER(c_void_p), c_int, P]

@@ -174,6 +174,10 @@ class CprGmres:
         return dict(learned_used=bool(o[0]), factor_learned=float(o[1]), factor_plain=float(o[2]),
                     bytes_learned=float(o[3]), bytes_plain=float(o[4]))
 
+    def learned_fallbacks(self):
+        """Solves in which the learned settings stalled and the plain preconditioner took over."""
+        return int(self._so.jxcpr_solver_learned_fallbacks(self.h))
+
     def bilu_factors(self):
         """Block ILU(0) factors of stage2_solver_type 5: (la, ua, dinv) as flat host arrays."""
         sz = np.zeros(2, np.int64)

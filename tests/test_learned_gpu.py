@@ -117,3 +117,31 @@ def test_trained_network_gain_over_plain_settings():
     print(f"learned / plain modelled cost on held-out systems: {np.round(ratios, 3)} mean {mean:.3f}, "
           f"learned settings kept on {used} of {len(ratios)}")
     assert mean <= 1.05
+
+
+def test_rejected_learned_settings_fall_back_to_the_plain_method():
+    """A system of the batch workload on which the learned strength thresholds build a poor
+    hierarchy (without the fallback the learned mode needs 300-400 iterations where the plain
+    method needs 29).  Either the setup probe rejects the learned settings or the solve stalls
+    against the probe's prediction; both replace them by the plain preconditioner (default
+    thresholds, plain smoothers), so the solve stays within a small multiple of the plain one."""
+    from jxpamg_all_b200 import synth
+    from jxpamg_all_b200.solver import CprGmres
+
+    g = synth.batch_grids()
+    s = synth.reservoir_system(*g[45], 45)
+    base = dict(decouple=1, max_iter=400, smoother_order=1, coarse_exact=0, precision=1, flexible=1)
+    P = CprGmres(**dict(base, fast_smoother=0)).setup(s.ia, s.ja, s.a, s.block_size)
+    _, it_plain, _, conv_p = P.solve(s.b)
+    L = CprGmres(**dict(base, fast_smoother=2)).setup(s.ia, s.ja, s.a, s.block_size)
+    x, it, rel, conv = L.solve(s.b)
+    st = L.learned_status()
+    assert conv_p and conv
+    assert it <= 4 * it_plain, (it, it_plain, st, L.learned_fallbacks())
+    if st["learned_used"]:
+        assert it <= it_plain + 10, (it, it_plain, st)
+    else:
+        _, it2, _, conv2 = L.solve(s.b)  # later solves run the plain preconditioner from the start
+        assert conv2 and it2 <= it_plain + 3, (it2, it_plain)
+    for G in (P, L):
+        G.close()
