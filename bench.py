@@ -446,7 +446,7 @@ def run_ours(args):
 # DRAM traffic of one stage-2 sweep's kernels (both colour launches), from an ncu capture of the same
 # solve (dram__bytes_read.sum + dram__bytes_write.sum, layouts reused through JXCPR_TUNE_CACHE):
 # (workload, value bytes, layout) -> bytes.
-STAGE2_TRAFFIC_BYTES = {("c1", 4, "sell"): 2 * 108.9e6}
+STAGE2_TRAFFIC_BYTES = {("c1", 4, "sell"): 209.4e6}
 
 
 def roofline_stage2(G, s, stream, value_bytes, cfg="c1"):
@@ -476,8 +476,9 @@ def roofline_stage2(G, s, stream, value_bytes, cfg="c1"):
     sec = e0.elapsed_time(e1) / 1e3 / reps
     bs, nb, nnzb, n = s.block_size, s.num_block_rows, s.nnzb, s.n
     xb = value_bytes  # the mixed path keeps the stage-2 vectors in FP32 too
-    # values + column indices + row pointers, b/x/vt read once, x written once, start-of-sweep copy (read+write)
-    alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * xb * 6
+    # values + column indices + row pointers; b read, x read and written, the start values of the
+    # classes before the last written to vt and read back by their neighbours (about n in all)
+    alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * xb * 5
     achieved = alg / sec / 1e9
     layout = "?"
     for line in G.setup_report().splitlines():

@@ -433,6 +433,7 @@ struct FastCpr final : FastCprBase {
     int nc = 0;
     LevelMat st2;  // decoupled block matrix, level-0 colour classes as segments
     DevBuf<double> vt;
+    DevBuf<int> st2_cls;  // stage 2: colour class of each block row (the sweeps' order)
     DevBuf<float> r32, z32, vt32;  // mixed path: stage-2 vectors in FP32
     CsrView<double> A0;  // FP64 level-0 operator (convergence-factor probe)
     DevBuf<double> pe, pr, pc, partials, nrm;
@@ -527,17 +528,17 @@ struct FastCpr final : FastCprBase {
     }
 
     template <typename TV, typename TXV, typename TAC>
-    void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp,
-                        TAC w, TAC om, int plain, cudaStream_t s) {
+    void launch_hgs_csr(int V, const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, TXV *vtp,
+                        TAC w, TAC om, int plain, fk::SweepOrder so, cudaStream_t s) {
         const int grid = div_up((long long)(r1 - r0) * V, 128);
 #define JX_HGS_CSR(VV)                                                                                        \
     do {                                                                                                      \
         if (bs == 2)                                                                                          \
             fk::hgs_color<2, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
-                                                                    z, vtp, w, om, plain);                     \
+                                                                    z, vtp, w, om, plain, so);                 \
         else                                                                                                  \
             fk::hgs_color<3, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
-                                                                    z, vtp, w, om, plain);                     \
+                                                                    z, vtp, w, om, plain, so);                 \
     } while (0)
         switch (V) {
             case 1: JX_HGS_CSR(1); break;
@@ -551,23 +552,34 @@ struct FastCpr final : FastCprBase {
     }
 
     // One stage-2 sweep on vectors of type TXV (FP64 path: the caller's r, z;
-    // mixed path: FP32 copies), vtp = start-of-sweep copy of z.
+    // mixed path: FP32 copies); vtp receives each colour class's start values as
+    // the class is updated (no start-of-sweep copy, see fk::hgs_color).
     template <typename TXV>
     void sweep_typed(const TXV *r, TXV *z, TXV *vtp, cudaStream_t s) {
         const LevelMat &M = st2;
         if (M.n == 0) return;
-        JX_CUDA(cudaMemcpyAsync(vtp, z, sizeof(TXV) * M.n * bs, cudaMemcpyDeviceToDevice, s));
         const double eps = 2.220446049250313e-16;
         const int plain = (fabs(cfg.stage2_w - 1) < eps && fabs(cfg.stage2_omega - 1) < eps) ? 1 : 0;
         const TA w = (TA)cfg.stage2_w, om = (TA)cfg.stage2_omega;
+        int first = -1, last = -1;
+        for (size_t c = 0; c + 1 < M.seg.size(); ++c)
+            if (M.seg[c + 1] > M.seg[c]) {
+                if (first < 0) first = (int)c;
+                last = (int)c;
+            }
         for (size_t c = 0; c + 1 < M.seg.size(); ++c) {
             const int r0 = M.seg[c], r1 = M.seg[c + 1];
             if (r1 <= r0) continue;
+            fk::SweepOrder so;
+            so.nmode = (int)c == first ? 0 : ((int)c == last ? 1 : 2);
+            so.save = (int)c != last ? 1 : 0;
+            so.cur = (int)c;
+            so.cls = st2_cls.get();
             if (M.kind == VAL_F64)  // FP64 path, and the hybrid form's FP64 stage 2: FP64 values and arithmetic
                 launch_stage2<double, TXV, double>(M, M.a64.get(), r0, r1, r, z, vtp, cfg.stage2_w, cfg.stage2_omega,
-                                                   plain, s);
+                                                   plain, so, s);
             else
-                launch_stage2<float, TXV, TA>(M, M.a32.get(), r0, r1, r, z, vtp, w, om, plain, s);
+                launch_stage2<float, TXV, TA>(M, M.a32.get(), r0, r1, r, z, vtp, w, om, plain, so, s);
             JX_LAUNCH_CHECK();
         }
     }
@@ -588,18 +600,18 @@ struct FastCpr final : FastCprBase {
         }
     }
     template <typename TV, typename TXV, typename TAC>
-    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, const TXV *vtp, TAC w,
-                       TAC om, int plain, cudaStream_t s) {
+    void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, TXV *vtp, TAC w,
+                       TAC om, int plain, fk::SweepOrder so, cudaStream_t s) {
         if (M.sell) {
             const int grid = div_up(r1 - r0, kThreads);
             if (bs == 2)
                 fk::hgs_sell<2, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
-                                                                       M.rows.get(), r, z, vtp, w, om, plain);
+                                                                       M.rows.get(), r, z, vtp, w, om, plain, so);
             else
                 fk::hgs_sell<3, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
-                                                                       M.rows.get(), r, z, vtp, w, om, plain);
+                                                                       M.rows.get(), r, z, vtp, w, om, plain, so);
         } else {
-            launch_hgs_csr<TV, TXV>(opt.stage2_lanes, M, a, r0, r1, r, z, vtp, w, om, plain, s);
+            launch_hgs_csr<TV, TXV, TAC>(opt.stage2_lanes, M, a, r0, r1, r, z, vtp, w, om, plain, so, s);
         }
     }
 
@@ -871,14 +883,24 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
     // stage 2: block rows in the level-0 colour order
     AmgLevel &H0 = *H.levels[0];
     F->vt.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
+    F->vt.zero(s);  // padding slots of the sliced-ELL copy read entry 0 (times a zero block): keep it finite
     if (!fp64) {
         const size_t nv = (size_t)(A.nb > 0 ? A.nb : 1) * A.bs;
         F->r32.alloc(nv);
         F->z32.alloc(nv);
         F->vt32.alloc(nv);
+        F->vt32.zero(s);
     }
     if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
+        {
+            const std::vector<int> &g = H0.fwd.h_group_ptr;
+            std::vector<int> cls(A.nb, 0);
+            for (size_t c = 0; c + 1 < g.size(); ++c)
+                for (int t = g[c]; t < g[c + 1]; ++t) cls[order[t]] = (int)c;
+            F->st2_cls.alloc(A.nb);
+            F->st2_cls.upload(cls.data(), A.nb, s);
+        }
         // the hybrid form (precision 3) keeps the stage-2 block matrix in FP64
         const int kind = (fp64 || opt.precision == 3) ? VAL_F64 : VAL_F32;
         const std::string key = tune_key("stage2", A.nb, A.nnzb, kind, A.bs * A.bs, opt.autotune);

@@ -305,11 +305,28 @@ __device__ __forceinline__ void block_solve(const TA D[BS * BS], const TA rhs[BS
 
 // x_i <- (1 - w omega) x_i + w D_i^-1 (omega b_i - sum_{j != i} A_ij (x_j - (1 - omega) vt_j))
 // (jxf_ParBSRHGSRelax's update with res = b, res0 = -sum A x, res2 = sum A vt);
-// plain (w = omega = 1): x_i <- D_i^-1 (b_i - sum A_ij x_j).  vt = x at sweep start.
+// plain (w = omega = 1): x_i <- D_i^-1 (b_i - sum A_ij x_j).  vt_j = x_j at the sweep start.
+//
+// No start-of-sweep copy: a colour class's launch saves its rows' old values in vt (save = 1)
+// before updating them, and a neighbour's vt_j is read only if its class came earlier in this
+// sweep -- otherwise x_j still holds the start value.  nmode 0: every neighbour comes later (the
+// first class), 1: every neighbour came earlier (the last class), 2: decided per neighbour by its
+// class index cls[j] against this launch's cur.  The arithmetic is the copy-based sweep's.
+struct SweepOrder {
+    int nmode, save, cur;
+    const int *cls;
+};
+
+template <typename TA, typename TXV>
+__device__ __forceinline__ TA start_value(const TXV *x, TXV *vt, long long o, int j, SweepOrder so) {
+    const bool earlier = so.nmode == 1 || (so.nmode == 2 && __ldg(so.cls + j) < so.cur);
+    return earlier ? (TA)__ldg(vt + o) : (TA)x[o];
+}
+
 template <int BS, int V, typename TV, typename TA, typename TXV>
 __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
                           const int *__restrict__ ja, const TV *__restrict__ a, const TXV *__restrict__ b,
-                          TXV *x, const TXV *__restrict__ vt, TA w, TA omega, int plain) {
+                          TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int t = r0 + (int)(gt / V);
     const int lane = (int)(gt % V);
@@ -326,7 +343,7 @@ __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const in
 #pragma unroll
         for (int m = 0; m < BS; ++m) {
             const TA xj = (TA)x[(long long)j * BS + m];
-            c[m] = plain ? xj : xj - omo * (TA)__ldg(vt + (long long)j * BS + m);
+            c[m] = plain ? xj : xj - omo * start_value<TA, TXV>(x, vt, (long long)j * BS + m, j, so);
         }
 #pragma unroll
         for (int q = 0; q < BS; ++q)
@@ -346,7 +363,9 @@ __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const in
 #pragma unroll
     for (int q = 0; q < BS; ++q) {
         const long long o = (long long)i * BS + q;
-        x[o] = plain ? (TXV)out[q] : (TXV)(prod * (TA)vt[o] + w * out[q]);
+        const TXV old = x[o];
+        if (!plain && so.save) vt[o] = old;
+        x[o] = plain ? (TXV)out[q] : (TXV)(prod * (TA)old + w * out[q]);
     }
 }
 
@@ -356,8 +375,7 @@ template <int BS, typename TV, typename TA, typename TXV>
 __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long *__restrict__ sp,
                                                 const int *__restrict__ col, const TV *__restrict__ a,
                                                 const int *__restrict__ rows, const TXV *__restrict__ b,
-                                                TXV *x, const TXV *__restrict__ vt, TA w, TA omega,
-                                                int plain) {
+                                                TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
     const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= r1) return;
     const int i = __ldg(rows + t);
@@ -370,7 +388,7 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
 #pragma unroll
     for (int q = 0; q < BS; ++q) {
         rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
-        xv[q] = plain ? (TA)0 : (TA)vt[(long long)i * BS + q];
+        xv[q] = plain ? (TA)0 : (TA)x[(long long)i * BS + q];
         acc[q] = 0;
     }
     load_block<BS, TV, TA>(a, o, D);
@@ -384,8 +402,8 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
 #pragma unroll
         for (int m = 0; m < BS; ++m) {
             const TA x0 = (TA)x[(long long)j0 * BS + m], x1 = (TA)x[(long long)j1 * BS + m];
-            c0[m] = plain ? x0 : x0 - omo * (TA)__ldg(vt + (long long)j0 * BS + m);
-            c1[m] = plain ? x1 : x1 - omo * (TA)__ldg(vt + (long long)j1 * BS + m);
+            c0[m] = plain ? x0 : x0 - omo * start_value<TA, TXV>(x, vt, (long long)j0 * BS + m, j0, so);
+            c1[m] = plain ? x1 : x1 - omo * start_value<TA, TXV>(x, vt, (long long)j1 * BS + m, j1, so);
         }
 #pragma unroll
         for (int q = 0; q < BS; ++q)
@@ -400,7 +418,7 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
 #pragma unroll
         for (int m = 0; m < BS; ++m) {
             const TA x0 = (TA)x[(long long)j0 * BS + m];
-            c0[m] = plain ? x0 : x0 - omo * (TA)__ldg(vt + (long long)j0 * BS + m);
+            c0[m] = plain ? x0 : x0 - omo * start_value<TA, TXV>(x, vt, (long long)j0 * BS + m, j0, so);
         }
 #pragma unroll
         for (int q = 0; q < BS; ++q)
@@ -413,8 +431,10 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
     block_solve<BS, TA>(D, r2, out);
     const TA prod = (TA)1 - w * omega;
 #pragma unroll
-    for (int q = 0; q < BS; ++q)
+    for (int q = 0; q < BS; ++q) {
+        if (!plain && so.save) vt[(long long)i * BS + q] = (TXV)xv[q];
         x[(long long)i * BS + q] = plain ? (TXV)out[q] : (TXV)(prod * xv[q] + w * out[q]);
+    }
 }
 
 // ---- sliced-ELL fill ----------------------------------------------------------
