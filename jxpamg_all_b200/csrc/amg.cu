@@ -14,6 +14,7 @@
 // (operation/matops/par_gs.c:20-74), here factored once at setup.
 #include <algorithm>
 #include <chrono>
+#include <future>
 #include <vector>
 
 #include "amg.cuh"
@@ -199,20 +200,35 @@ void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // hierarchy
 // ---------------------------------------------------------------------------
-static void level_schedules(AmgLevel &L, int order, cudaStream_t s) {
+// Gauss-Seidel schedules of a level, built on the host from its pattern.  The
+// host work runs on a worker thread while the setup carries on with the next
+// levels (the pattern is copied here, on the setup's stream, first).
+struct ScheduleJob {
+    std::vector<int> perm[2], gptr[2], rank[2];
+    bool both = false;
+};
+
+static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, cudaStream_t s) {
     const int n = L.A.nrows;
     std::vector<int> ia(n + 1), ja(L.A.nnz > 0 ? L.A.nnz : 1);
     L.A.ia.download(ia.data(), n + 1, s);
     L.A.ja.download(ja.data(), L.A.nnz, s);
     JX_CUDA(cudaStreamSynchronize(s));
-    std::vector<int> perm, gptr, rank;
-    build_schedule_host(n, ia.data(), ja.data(), order, true, perm, gptr, rank);
-    upload_schedule(perm, gptr, rank, L.fwd, s);
-    if (order == ORDER_EXACT) {
-        build_schedule_host(n, ia.data(), ja.data(), order, false, perm, gptr, rank);
-        upload_schedule(perm, gptr, rank, L.bwd, s);
-    }
-    // multicolour: the backward sweep visits the same classes in reverse order (fwd schedule, reversed)
+    return std::async(std::launch::async, [n, order, ia = std::move(ia), ja = std::move(ja)]() {
+        ScheduleJob J;
+        build_schedule_host(n, ia.data(), ja.data(), order, true, J.perm[0], J.gptr[0], J.rank[0]);
+        if (order == ORDER_EXACT) {
+            J.both = true;
+            build_schedule_host(n, ia.data(), ja.data(), order, false, J.perm[1], J.gptr[1], J.rank[1]);
+        }
+        // multicolour: the backward sweep visits the same classes in reverse order (fwd schedule, reversed)
+        return J;
+    });
+}
+
+static void finish_level_schedules(AmgLevel &L, ScheduleJob J, cudaStream_t s) {
+    upload_schedule(J.perm[0], J.gptr[0], J.rank[0], L.fwd, s);
+    if (J.both) upload_schedule(J.perm[1], J.gptr[1], J.rank[1], L.bwd, s);
 }
 
 static double now_ms() {
@@ -240,10 +256,20 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
     H.levels.clear();
     H.levels.emplace_back(new AmgLevel());
     H.levels[0]->A = std::move(A0);
+    // which levels get Gauss-Seidel schedules: all in the exact order; in the fast path level 0
+    // (stage 2 sweeps the block matrix, which has its pattern) and the levels sparse enough for GS
+    auto wants_schedule = [&](const AmgLevel &L, bool first) {
+        const double mean_row = L.A.nrows > 0 ? (double)L.A.nnz / L.A.nrows : 0.0;
+        const bool dense = H.prm.order != ORDER_EXACT && mean_row > H.prm.jacobi_mean_row;
+        return !dense || first;
+    };
+    std::vector<std::future<ScheduleJob>> jobs;
     int level = 0;
     while (true) {
         AmgLevel &L = *H.levels[level];
         const int n = L.A.nrows;
+        jobs.emplace_back();
+        if (wants_schedule(L, level == 0)) jobs.back() = start_level_schedules(L, H.prm.order, s);
         DevPattern S;
         if (H.prm.theta_for_level) {
             L.theta = H.prm.theta_for_level(level, L.A.view());
@@ -276,18 +302,17 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         ++level;
         if (level == H.prm.max_levels - 1 || nc <= H.prm.coarse_threshold) break;
     }
-    for (auto &Lp : H.levels) {
-        AmgLevel &L = *Lp;
+    for (size_t l = 0; l < H.levels.size(); ++l) {
+        AmgLevel &L = *H.levels[l];
         const int n = L.A.nrows;
         if (H.prm.order == ORDER_EXACT) {
             L.f.alloc(n > 0 ? n : 1);
             L.u.alloc(n > 0 ? n : 1);
         }
-        if (&L == H.levels.back().get()) continue;
+        if (l + 1 == H.levels.size()) continue;  // the coarsest level is solved directly
         const double mean_row = n > 0 ? (double)L.A.nnz / n : 0.0;
         const bool dense = H.prm.order != ORDER_EXACT && mean_row > H.prm.jacobi_mean_row;
-        // level 0 always gets a schedule: stage 2 sweeps the block matrix, which has its pattern
-        if (!dense || &L == H.levels.front().get()) level_schedules(L, H.prm.order, s);
+        if (l < jobs.size() && jobs[l].valid()) finish_level_schedules(L, jobs[l].get(), s);
         H.log.mark("schedules(host)", s);
         if (H.prm.order == ORDER_EXACT)
             L.smoother = SMOOTH_EXACT_GS;
