@@ -840,6 +840,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
                 build_tuned<TX>(nm.c_str(), n, n, Av.nnz, Av.ia, Av.ja, Av.a, kind, {}, {}, nullptr, opt, Lv.A,
                                 F->tune_log, s);
             }
+            H.log.mark("fast_operators", s);
             alloc_vec(Lv.dinv, n);
             if (n) {
                 fk::dinv_diag<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, Av.ia, Av.ja, Av.a, Lv.dinv.get());
@@ -861,6 +862,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
                 chebyshev3_coefficients(Lv.cheb_lo, Lv.cheb_hi, Lv.cheb);
                 alloc_vec(Lv.y1, n);
                 alloc_vec(Lv.y2, n);
+                H.log.mark("fast_lambda_max", s);
             }
             alloc_vec(Lv.r, n);
             alloc_vec(Lv.z, n);
@@ -871,6 +873,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
                             {}, nullptr, opt, Lv.P, F->tune_log, s);
             build_tuned<TX>(("R" + std::to_string(l)).c_str(), Rv.nrows, Rv.ncols, Rv.nnz, Rv.ia, Rv.ja, Rv.a, pk, {},
                             {}, nullptr, opt, Lv.R, F->tune_log, s);
+            H.log.mark("fast_transfers", s);
         }
         F->lv.push_back(std::move(lev));
     }
@@ -978,6 +981,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
             tune_store(key, c);
         }
     }
+    H.log.mark("fast_stage2", s);
     JX_CUDA(cudaStreamSynchronize(s));
     return F.release();
 }
