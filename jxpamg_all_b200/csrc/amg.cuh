@@ -100,6 +100,7 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
 
 // setup_host.cu (sequential graph passes)
 void rs_first_pass_host(int n, const int *sia, const int *sja, int *cf);
+void rs_first_pass_host(int n, const int *sia, const int *sja, const int *stia, const int *stja, int *cf);
 void build_schedule_host(int n, const int *ia, const int *ja, int order, bool forward, std::vector<int> &perm,
                          std::vector<int> &group_ptr, std::vector<int> &rank);
 void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr, const std::vector<int> &rank,

@@ -70,31 +70,44 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
 
 // ---- construction -----------------------------------------------------------------
 // Sliced-ELL layout on the host: segments of `order` (offsets seg_in), rows
-// sorted by decreasing length inside windows, each segment padded to whole slices.
+// sorted by decreasing length inside windows (a stable counting sort: equal
+// lengths keep their order), each segment padded to whole slices.
 void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, const std::vector<int> &seg_in,
                  std::vector<int> &rows, std::vector<long long> &sp, std::vector<int> &seg_out) {
-    rows.clear();
     seg_out.assign(1, 0);
-    std::vector<int> win;
+    size_t total = 0;
+    for (size_t c = 0; c + 1 < seg_in.size(); ++c) total += (size_t)(seg_in[c + 1] - seg_in[c] + 31) / 32 * 32;
+    rows.assign(total, -1);
+    std::vector<int> rlen(total, 0), len, cnt;
+    size_t pos = 0;
     for (size_t c = 0; c + 1 < seg_in.size(); ++c) {
         for (int w0 = seg_in[c]; w0 < seg_in[c + 1]; w0 += kSellWindow) {
-            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow);
-            win.assign(order.begin() + w0, order.begin() + w1);
-            std::stable_sort(win.begin(), win.end(),
-                             [&](int x, int y) { return ia[x + 1] - ia[x] > ia[y + 1] - ia[y]; });
-            rows.insert(rows.end(), win.begin(), win.end());
+            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow), nw = w1 - w0;
+            len.resize(nw);
+            int maxlen = 0;
+            for (int t = 0; t < nw; ++t) {
+                const int i = order[w0 + t];
+                len[t] = ia[i + 1] - ia[i];
+                maxlen = std::max(maxlen, len[t]);
+            }
+            cnt.assign((size_t)maxlen + 2, 0);  // key maxlen - len: longest rows first
+            for (int t = 0; t < nw; ++t) cnt[maxlen - len[t] + 1]++;
+            for (int k = 0; k <= maxlen; ++k) cnt[k + 1] += cnt[k];
+            for (int t = 0; t < nw; ++t) {
+                const size_t q = pos + cnt[maxlen - len[t]]++;
+                rows[q] = order[w0 + t];
+                rlen[q] = len[t];
+            }
+            pos += nw;
         }
-        while (rows.size() % 32) rows.push_back(-1);
-        seg_out.push_back((int)rows.size());
+        pos = (pos + 31) / 32 * 32;
+        seg_out.push_back((int)pos);
     }
-    const size_t ns = rows.size() / 32;
+    const size_t ns = total / 32;
     sp.assign(ns + 1, 0);
     for (size_t sl = 0; sl < ns; ++sl) {
         int w = 0;
-        for (int q = 0; q < 32; ++q) {
-            const int i = rows[sl * 32 + q];
-            if (i >= 0) w = std::max(w, ia[i + 1] - ia[i]);
-        }
+        for (int q = 0; q < 32; ++q) w = std::max(w, rlen[sl * 32 + q]);
         sp[sl + 1] = sp[sl] + 32LL * w;
     }
 }

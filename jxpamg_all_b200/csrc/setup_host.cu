@@ -41,7 +41,6 @@ struct Buckets {
 }  // namespace
 
 void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF) {
-    const int C_PT = 1, F_PT = -1, Z_PT = -2, SF_PT = -3, UNDEC = 0;
     const int nnz = Si[n];
     std::vector<int> STi(n + 1, 0), STj(nnz > 0 ? nnz : 1);
     for (int k = 0; k < nnz; ++k) STi[Sj[k] + 1]++;
@@ -51,6 +50,12 @@ void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF) {
         for (int i = 0; i < n; ++i)
             for (int k = Si[i]; k < Si[i + 1]; ++k) STj[pos[Sj[k]]++] = i;
     }
+    rs_first_pass_host(n, Si, Sj, STi.data(), STj.data(), CF);
+}
+
+// STi/STj: the transpose of S with the rows of each column in ascending order.
+void rs_first_pass_host(int n, const int *Si, const int *Sj, const int *STi, const int *STj, int *CF) {
+    const int C_PT = 1, F_PT = -1, Z_PT = -2, SF_PT = -3, UNDEC = 0;
     std::vector<int> measure(n);
     int maxmeasure = 0;
     for (int i = 0; i < n; ++i) {
