@@ -279,19 +279,27 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         }
         amg_strength(L.A.view(), L.theta, H.prm.max_row_sum, S, s);
         H.log.mark("strength", s);
-        // the pattern and its transpose (stable: rows ascending in each column) go to the host
-        std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1), stia(n + 1), stja(S.nnz > 0 ? S.nnz : 1);
-        {
-            DevBuf<int> tia(n + 1), tja(S.nnz > 0 ? S.nnz : 1), tperm(S.nnz > 0 ? S.nnz : 1);
-            pattern_transpose(n, n, S.nnz, S.ia.get(), S.ja.get(), tia.get(), tja.get(), tperm.get(), s);
+        L.cf.assign(n, 0);
+        if (H.prm.rs_range_rows > 0 && n >= 2 * H.prm.rs_range_rows) {
+            std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);
             S.ia.download(sia.data(), n + 1, s);
             S.ja.download(sja.data(), S.nnz, s);
-            tia.download(stia.data(), n + 1, s);
-            tja.download(stja.data(), S.nnz, s);
             JX_CUDA(cudaStreamSynchronize(s));
+            rs_first_pass_ranges(n, sia.data(), sja.data(), H.prm.rs_range_rows, L.cf.data());
+        } else {
+            // the pattern and its transpose (stable: rows ascending in each column) go to the host
+            std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1), stia(n + 1), stja(S.nnz > 0 ? S.nnz : 1);
+            {
+                DevBuf<int> tia(n + 1), tja(S.nnz > 0 ? S.nnz : 1), tperm(S.nnz > 0 ? S.nnz : 1);
+                pattern_transpose(n, n, S.nnz, S.ia.get(), S.ja.get(), tia.get(), tja.get(), tperm.get(), s);
+                S.ia.download(sia.data(), n + 1, s);
+                S.ja.download(sja.data(), S.nnz, s);
+                tia.download(stia.data(), n + 1, s);
+                tja.download(stja.data(), S.nnz, s);
+                JX_CUDA(cudaStreamSynchronize(s));
+            }
+            rs_first_pass_host(n, sia.data(), sja.data(), stia.data(), stja.data(), L.cf.data());
         }
-        L.cf.assign(n, 0);
-        rs_first_pass_host(n, sia.data(), sja.data(), stia.data(), stja.data(), L.cf.data());
         H.log.mark("rs_first_pass(host)", s);
         DevBuf<int> cf(n > 0 ? n : 1);
         cf.upload(L.cf.data(), n, s);

@@ -65,6 +65,7 @@ struct AmgParams {
     int coarse_exact = 1;  // 1: substitution in the reference's order; 0: explicit inverse (GEMV)
     int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
     double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows go straight to l1-Jacobi
+    int rs_range_rows = 0;  // > 0: the coarsening's first pass runs on row ranges of this size (host threads)
     // Optional per-level strength thresholds: called before level l is
     // coarsened with its operator; returns the threshold to use (learned model).
     std::function<double(int level, const CsrView<double> &A)> theta_for_level;
@@ -99,8 +100,11 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
              long long table_budget_entries = (1LL << 27));
 
 // setup_host.cu (sequential graph passes)
-void rs_first_pass_host(int n, const int *sia, const int *sja, int *cf);
-void rs_first_pass_host(int n, const int *sia, const int *sja, const int *stia, const int *stja, int *cf);
+void rs_first_pass_host(int n, const int *sia, const int *sja, int *cf, const int *gia = nullptr);
+void rs_first_pass_host(int n, const int *sia, const int *sja, const int *stia, const int *stja, int *cf,
+                        const int *gia = nullptr);
+// The first pass on row ranges of range_rows rows (n / range_rows ranges; one range: the whole pattern).
+void rs_first_pass_ranges(int n, const int *sia, const int *sja, int range_rows, int *cf);
 void build_schedule_host(int n, const int *ia, const int *ja, int order, bool forward, std::vector<int> &perm,
                          std::vector<int> &group_ptr, std::vector<int> &rank);
 void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr, const std::vector<int> &rank,

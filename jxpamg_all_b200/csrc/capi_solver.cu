@@ -53,6 +53,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"smoother_order", &p.smoother_order},
                {"coarse_exact", &p.coarse_exact},
                {"max_colors", &p.max_colors},
+               {"rs_range_rows", &p.rs_range_rows},
                {"use_tma_spmv", &p.use_tma_spmv},
                {"precision", &p.precision},
                {"bf16_level", &p.bf16_level},

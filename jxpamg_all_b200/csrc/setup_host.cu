@@ -7,6 +7,14 @@
 //   insertion order; it is reproduced here with O(1) bucket operations:
 //   buckets indexed by measure, points appended at the tail, the highest
 //   non-empty bucket tracked.
+//   rs_first_pass_ranges runs the pass on row ranges of a fixed size, each on
+//   the diagonal block of S for its rows (strong connections to other ranges
+//   are not seen), as every process of a distributed run of the reference does
+//   (par_coarsen_ruge.c:37-44 take S_diag, :197 and :212 count the measures in
+//   it alone for the HMIS first pass, :261 marks SF_PT only when the row is
+//   empty in the diagonal and the off-diagonal block).  The ranges depend
+//   on n and the range size only, so the splitting is the same on any host;
+//   the ranges run on host threads.
 // * build_schedule_host -- grouping of rows for the Gauss-Seidel sweeps on
 //   the device: either the level schedule of the natural ordering (row i
 //   waits for every j < i of its row in a forward sweep, j > i backward) or a
@@ -14,6 +22,8 @@
 //
 // Both read the pattern once (O(nnz)); everything numeric stays on the GPU.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "amg.cuh"
@@ -40,7 +50,7 @@ struct Buckets {
 };
 }  // namespace
 
-void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF) {
+void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF, const int *gia) {
     const int nnz = Si[n];
     std::vector<int> STi(n + 1, 0), STj(nnz > 0 ? nnz : 1);
     for (int k = 0; k < nnz; ++k) STi[Sj[k] + 1]++;
@@ -50,11 +60,14 @@ void rs_first_pass_host(int n, const int *Si, const int *Sj, int *CF) {
         for (int i = 0; i < n; ++i)
             for (int k = Si[i]; k < Si[i + 1]; ++k) STj[pos[Sj[k]]++] = i;
     }
-    rs_first_pass_host(n, Si, Sj, STi.data(), STj.data(), CF);
+    rs_first_pass_host(n, Si, Sj, STi.data(), STj.data(), CF, gia);
 }
 
 // STi/STj: the transpose of S with the rows of each column in ascending order.
-void rs_first_pass_host(int n, const int *Si, const int *Sj, const int *STi, const int *STj, int *CF) {
+// gia (optional): the row offsets of the whole strength pattern when S is the
+// diagonal block of a row range; a point is SF_PT only when that row is empty.
+void rs_first_pass_host(int n, const int *Si, const int *Sj, const int *STi, const int *STj, int *CF,
+                        const int *gia) {
     const int C_PT = 1, F_PT = -1, Z_PT = -2, SF_PT = -3, UNDEC = 0;
     std::vector<int> measure(n);
     int maxmeasure = 0;
@@ -64,8 +77,9 @@ void rs_first_pass_host(int n, const int *Si, const int *Sj, const int *STi, con
     }
     Buckets B(n, maxmeasure + n + 2);
     int num_left = 0;
+    const int *rows = gia ? gia : Si;
     for (int j = 0; j < n; ++j) {
-        if (Si[j + 1] - Si[j] == 0) {
+        if (rows[j + 1] - rows[j] == 0) {
             CF[j] = SF_PT;
             measure[j] = 0;
         } else {
@@ -140,6 +154,36 @@ void rs_first_pass_host(int n, const int *Si, const int *Sj, const int *STi, con
             }
         }
     }
+}
+
+void rs_first_pass_ranges(int n, const int *Si, const int *Sj, int range_rows, int *CF) {
+    const int nr = range_rows > 0 ? std::max(1, n / range_rows) : 1;
+    if (nr == 1) {
+        rs_first_pass_host(n, Si, Sj, CF, nullptr);
+        return;
+    }
+    auto one = [&](int r) {
+        const int r0 = (int)((long long)n * r / nr), r1 = (int)((long long)n * (r + 1) / nr), m = r1 - r0;
+        std::vector<int> li(m + 1, 0), lj;
+        lj.reserve((size_t)(Si[r1] - Si[r0]) + 1);
+        for (int i = r0; i < r1; ++i) {
+            for (int k = Si[i]; k < Si[i + 1]; ++k) {
+                const int j = Sj[k];
+                if (j >= r0 && j < r1) lj.push_back(j - r0);
+            }
+            li[i - r0 + 1] = (int)lj.size();
+        }
+        rs_first_pass_host(m, li.data(), lj.data(), CF + r0, Si + r0);
+    };
+    const int threads = std::max(1, std::min(nr, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        for (int r = next.fetch_add(1); r < nr; r = next.fetch_add(1)) one(r);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
 }
 
 void build_schedule_host(int n, const int *ia, const int *ja, int order, bool forward, std::vector<int> &perm,

@@ -33,6 +33,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     amg.prm.order = prm.smoother_order;
     amg.prm.coarse_exact = fast_path ? 0 : prm.coarse_exact;
     amg.prm.max_colors = prm.max_colors;
+    amg.prm.rs_range_rows = fast_path ? prm.rs_range_rows : 0;
     amg.prm.strong_threshold = prm.strong_threshold;
     amg.prm.theta_for_level = nullptr;
     fast.reset();

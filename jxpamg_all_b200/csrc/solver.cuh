@@ -55,6 +55,9 @@ struct SolverParams {
     int smoother_order = ORDER_EXACT;  // 0 exact order (bit-identical), 1 throughput / mixed path
     int coarse_exact = 1;
     int max_colors = 8;
+    // fast path: the coarsening's first pass on row ranges of this many rows, one host thread per
+    // range (levels with fewer than twice as many rows, and the exact order always, take one pass)
+    int rs_range_rows = 131072;
     int use_tma_spmv = 0;
     // fast path (smoother_order 1)
     int precision = 0;       // 0 FP64, 1 FP32 preconditioner, 2 FP32 + BF16 coarse levels, 3 the reference's

@@ -73,6 +73,17 @@ def _f64(a):
 
 
 # ---- restatement ---------------------------------------------------------------
+def hmis_cf(ia, ja, a, theta=0.25, max_row_sum=0.9, range_rows=0):
+    """C/F splitting of a CSR operator: strength, the Ruge-Stueben first pass (on row ranges of
+    range_rows rows when > 0) and the PMIS pass; C points 1, F points -1."""
+    ia, ja, a = _i32(ia), _i32(ja), _f64(a)
+    n = len(ia) - 1
+    cf = np.zeros(n, np.int32)
+    orc().orc_hmis_ranges(c_int(n), _p(ia), _p(ja), _p(a), c_double(theta), c_double(max_row_sum),
+                          c_int(range_rows), _p(cf))
+    return cf
+
+
 def bsr_matvec(ia, ja, a, bs, x, alpha=1.0, y=None, beta=0.0):
     nb = len(ia) - 1
     ia, ja, a, x = _i32(ia), _i32(ja), _f64(a), _f64(x)

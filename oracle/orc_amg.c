@@ -126,7 +126,10 @@ static void bk_remove(buckets *B, int m, int i)
     while (B->maxm > 0 && B->bhead[B->maxm] < 0) B->maxm--;
 }
 
-void orc_rs_first_pass(const orc_csr *S, int *CF)
+/* gia (optional): row offsets of the whole strength pattern when S is the
+ * diagonal block of a row range; SF_PT only when that row is empty
+ * (par_coarsen_ruge.c:261 tests the diagonal and the off-diagonal block). */
+static void rs_first_pass_core(const orc_csr *S, const int *gia, int *CF)
 {
     int n = S->n;
     int nnz = S->ia[n];
@@ -156,8 +159,9 @@ void orc_rs_first_pass(const orc_csr *S, int *CF)
     B.maxm = 0;
     const int UNDEC = 0;
     int num_left = 0;
+    const int *rows = gia ? gia : S->ia;
     for (int j = 0; j < n; j++) {
-        if (S->ia[j + 1] - S->ia[j] == 0) {
+        if (rows[j + 1] - rows[j] == 0) {
             CF[j] = SF_PT;
             measure[j] = 0;
         } else {
@@ -237,6 +241,42 @@ void orc_rs_first_pass(const orc_csr *S, int *CF)
     }
     free(B.next); free(B.prev); free(B.bhead); free(B.btail);
     free(measure); free(STi); free(STj);
+}
+
+void orc_rs_first_pass(const orc_csr *S, int *CF)
+{
+    rs_first_pass_core(S, NULL, CF);
+}
+
+/* The first pass on n / range_rows row ranges (range r: rows n*r/nr to
+ * n*(r+1)/nr), each on the diagonal block of S for its rows -- what every
+ * process of a distributed run does (par_coarsen_ruge.c:37-44 take S_diag,
+ * :197 sets the measures from its transpose, :212 adds no off-process
+ * measures for the HMIS first pass, coarsen_type 11, and the pass,
+ * :250-425, walks S_diag only).  range_rows <= 0 or fewer than two ranges:
+ * the whole pattern. */
+void orc_rs_first_pass_ranges(const orc_csr *S, int range_rows, int *CF)
+{
+    int n = S->n;
+    int nr = range_rows > 0 ? n / range_rows : 1;
+    if (nr < 1) nr = 1;
+    for (int r = 0; r < nr; r++) {
+        int r0 = (int)((long long)n * r / nr), r1 = (int)((long long)n * (r + 1) / nr), m = r1 - r0;
+        orc_csr L;
+        L.n = L.m = m;
+        L.a = NULL;
+        L.ia = (int *)xcalloc(m + 1, sizeof(int));
+        L.ja = (int *)xcalloc(S->ia[r1] - S->ia[r0] + 1, sizeof(int));
+        int cnt = 0;
+        for (int i = r0; i < r1; i++) {
+            for (int k = S->ia[i]; k < S->ia[i + 1]; k++)
+                if (S->ja[k] >= r0 && S->ja[k] < r1) L.ja[cnt++] = S->ja[k] - r0;
+            L.ia[i - r0 + 1] = cnt;
+        }
+        rs_first_pass_core(&L, S->ia + r0, CF + r0);
+        free(L.ia);
+        free(L.ja);
+    }
 }
 
 /* Park-Miller minimal standard generator (Park & Miller, CACM 1988), in the
@@ -359,6 +399,22 @@ void orc_hmis(const orc_csr *S, int *CF)
 {
     orc_rs_first_pass(S, CF);
     orc_pmis(S, CF);
+}
+
+/* HMIS with the first pass on row ranges, on a CSR operator: strength
+ * (theta, max_row_sum) then orc_rs_first_pass_ranges and the PMIS pass. */
+void orc_hmis_ranges(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,
+                     int range_rows, int *CF)
+{
+    orc_csr A, S;
+    A.n = A.m = n;
+    A.ia = (int *)ia;
+    A.ja = (int *)ja;
+    A.a = (double *)a;
+    orc_strength(&A, theta, max_row_sum, &S);
+    orc_rs_first_pass_ranges(&S, range_rows, CF);
+    orc_pmis(&S, CF);
+    orc_csr_free(&S);
 }
 
 /* ---------------------------------------------------------------------------

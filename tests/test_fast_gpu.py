@@ -104,6 +104,40 @@ def test_default_threshold_hierarchy_matches_exact_path(systems):
             assert np.array_equal(u, v)
 
 
+@pytest.mark.parametrize("rows", [1000, 2000, 3000])
+def test_first_pass_on_row_ranges_matches_oracle(systems, rows):
+    """rs_range_rows: the coarsening's first pass runs on row ranges (each on its own diagonal
+    block of the strength pattern, on host threads); every level's C/F splitting equals the
+    oracle's ranged HMIS on that level's operator, and the solve still converges."""
+    s = systems("c0")
+    F, x, it, rel, conv = solve(s, precision=1, fast_smoother=1, flexible=1, rs_range_rows=rows)
+    G, x0, it0, rel0, conv0 = solve(s, precision=1, fast_smoother=1, flexible=1, rs_range_rows=0)
+    ranged = 0
+    for lev in range(F.num_levels() - 1):
+        ia, ja, a = F.level_matrix(lev)[:3]
+        n = len(ia) - 1
+        ranged += n >= 2 * rows
+        assert np.array_equal(F.level_cf(lev, n), oracle.hmis_cf(ia, ja, a, range_rows=rows)), lev
+    assert ranged >= 1
+    assert conv and conv0 and abs(it - it0) <= max(2, it0 // 10), (it, it0)
+    assert true_rel(s, x) <= 1.05e-6
+    F.close()
+    G.close()
+
+
+def test_row_ranges_leave_small_levels_whole(systems):
+    """Levels with fewer than two ranges' rows (and the exact order always) coarsen in one pass."""
+    s = systems("small")
+    E = CprGmres(decouple=1, rs_range_rows=100).setup(s.ia, s.ja, s.a, s.block_size)
+    O = oracle.OracleCPR(s.ia, s.ja, oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)[0], s.block_size)
+    n = len(O.level_matrix(0, 0)[0]) - 1
+    assert np.array_equal(E.level_cf(0, n), O.level_cf(0, n))
+    F, *_ = solve(s, precision=1, fast_smoother=1, flexible=1, rs_range_rows=n)
+    assert np.array_equal(F.level_cf(0, n), O.level_cf(0, n))
+    for G in (E, F):
+        G.close()
+
+
 def test_stage2_native_and_autotune_report(systems):
     from jxpamg_all_b200 import lib
 
