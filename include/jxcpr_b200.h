@@ -116,6 +116,9 @@ JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *
  *         decouple (0 none, 1 ABF, 5 True-IMPES), consistent_rhs (0: the
  *         reference's right-hand-side arithmetic, 1: solution-preserving),
  *         smoother_order (0 exact sequential order, 1 multicolour),
+ *         rs_range_rows (131072; order 1: the coarsening's first pass on row
+ *         ranges of this size, as each process of a distributed run does it,
+ *         par_coarsen_ruge.c:37-44; 0 one pass over the level),
  *         coarse_exact (1 substitution in the reference's order, 0 inverse),
  *         use_tma_spmv (1), print_level, logging, block_size (ignored)
  *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),
