@@ -6,8 +6,8 @@
 //                 WHILE (cycle continues) {              Arnoldi step i
 //                    z_i = M^-1 v_i  (CPR kernels recorded in place)
 //                    w = A z_i
-//                    h1 = V^T w,  w -= V h1              two-pass classical
-//                    h2 = V^T w,  s = ||w||^2            Gram-Schmidt (CGS2)
+//                    h1 = V^T w                          two-pass classical
+//                    w -= V h1, h2 = V^T w, s = ||w||^2  Gram-Schmidt (CGS2)
 //                    Givens rotation of column i (one thread), test
 //                    v_{i+1} = (w - V h2) / sqrt(s - ||h2||^2)
 //                 }
@@ -20,9 +20,10 @@
 // back substitution) follows the host GMRES (jxfpamg-0220/csrc/krylov/
 // pgmres.c:1090-1560) step for step; two things differ by design: each cycle
 // restarts from the true residual b - A x instead of the rotated estimate,
-// and the orthogonalisation is CGS2 (three passes over the basis, a fixed
-// number of kernels per step, which a graph needs) instead of MGS (i + 1
-// passes).  The norm of the new vector comes from Pythagoras,
+// and the orthogonalisation is CGS2 (three passes over the basis -- the first
+// products, the first update fused with the second products, the final
+// update -- and a fixed number of kernels per step, which a graph needs)
+// instead of MGS (i + 1 passes).  The norm of the new vector comes from Pythagoras,
 // ||w - V h2||^2 = ||w||^2 - ||h2||^2, as in delayed CGS2 (Swirydowicz et al.,
 // 2020).  Flexible: the preconditioned directions z_i are kept and x += Z y.
 #include <cmath>
@@ -36,6 +37,7 @@ namespace gg {
 constexpr int kThreads = 256;
 constexpr int kRedThreads = 1024;
 constexpr int kSlice = 2048;  // elements per block of the Gram products
+constexpr int kSlice2 = 512;  // elements per block of the fused update + second Gram products
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -171,11 +173,11 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, const do
 }
 
 // Block x: partial <V[k], w> over the x-th slice of kSlice elements for every
-// k <= i (and <w, w> in row i + 1 with self).  The slice of w is staged in
-// shared memory once and each basis vector is streamed past it; warps reduce
-// with shuffles and combine through shared memory once at the end.
+// k <= i.  The slice of w is staged in shared memory once and each basis
+// vector is streamed past it; warps reduce with shuffles and combine through
+// shared memory once at the end.
 __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const double *const *__restrict__ V,
-                                                        const GgState *st, const double *__restrict__ w, int self,
+                                                        const GgState *st, const double *__restrict__ w,
                                                         double *__restrict__ partials) {
     __shared__ double ws[kSlice];
     __shared__ double part[kGgMaxK + 2][kThreads / 32];
@@ -183,10 +185,10 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const doubl
     const int len = (int)min((long long)kSlice, n - e0);
     for (int j = threadIdx.x; j < len; j += kThreads) ws[j] = w[e0 + j];
     __syncthreads();
-    const int m = st->i + 1, kend = self ? m + 1 : m;
+    const int m = st->i + 1, kend = m;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = 0; k < kend; ++k) {
-        const double *v = k < m ? V[k] + e0 : ws;
+        const double *v = V[k] + e0;
         double acc = 0.0;
         for (int j = threadIdx.x; j < len; j += kThreads) acc = fma(v[j], ws[j], acc);
 #pragma unroll
@@ -215,22 +217,48 @@ __global__ void __launch_bounds__(kRedThreads) reduce_h_kernel(const double *__r
     }
 }
 
-// w -= sum_{k <= i} h[k] V[k]
-__global__ void __launch_bounds__(kThreads) update_kernel(long long n, const double *const *__restrict__ V,
-                                                          const GgState *st, const double *__restrict__ h,
-                                                          double *__restrict__ w) {
+// The first update and the second Gram products in one pass over the basis:
+// w -= sum_{k <= i} h[k] V[k], then partial <V[k], w> (k <= i) and <w, w> of
+// the updated w over the block's slice of kSlice2 elements.  A thread handles
+// one element at a time: it reads that element of every V[k] for the update
+// and again for the products right after, from L1 / L2, so the basis crosses
+// HBM once (the separate update and product kernels read it twice).
+__global__ void __launch_bounds__(kThreads) update_dots_kernel(long long n, const double *const *__restrict__ V,
+                                                               const GgState *st, const double *__restrict__ h,
+                                                               double *__restrict__ w, double *__restrict__ partials) {
     __shared__ const double *vs[kGgMaxK + 2];
     __shared__ double hs[kGgMaxK + 2];
+    __shared__ double part[kGgMaxK + 2][kThreads / 32];
     const int m = st->i + 1;
     for (int k = threadIdx.x; k < m; k += kThreads) {
         vs[k] = V[k];
         hs[k] = h[k];
     }
+    for (int q = threadIdx.x; q < (m + 1) * (kThreads / 32); q += kThreads) part[q / (kThreads / 32)][q % (kThreads / 32)] = 0.0;
     __syncthreads();
-    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
-        double s = w[e];
-        for (int k = 0; k < m; ++k) s = fma(-hs[k], vs[k][e], s);
-        w[e] = s;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long e0 = (long long)blockIdx.x * kSlice2;
+    for (int r = 0; r < kSlice2 / kThreads; ++r) {
+        const long long e = e0 + (long long)r * kThreads + threadIdx.x;
+        const bool live = e < n;
+        double sv = live ? w[e] : 0.0;
+        if (live) {
+            for (int k = 0; k < m; ++k) sv = fma(-hs[k], vs[k][e], sv);
+            w[e] = sv;
+        }
+        for (int k = 0; k <= m; ++k) {  // uniform trip count: every lane takes part in the shuffles
+            double v = live ? (k < m ? vs[k][e] : sv) * sv : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) part[k][warp] += v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x <= m) {
+        double v = 0.0;
+#pragma unroll
+        for (int q = 0; q < kThreads / 32; ++q) v += part[threadIdx.x][q];
+        partials[(long long)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
 }
 
@@ -442,6 +470,7 @@ void GraphGmres::prepare(Solver &S) {
     max_iter = prm.max_iter;
     const long long nn = n > 0 ? n : 1;
     G = div_up(nn, gg::kSlice);  // blocks of the Gram products and norms: one slice each
+    G2 = div_up(nn, gg::kSlice2);  // blocks of the fused update + second products
     G1 = std::max(1, std::min(8 * sm_count(), div_up(nn, gg::kThreads)));
     state.alloc(1);
     // work: rs (k+1), c (k), sn (k), h1 (k+2), h2 (k+2), y (k), hh ((k+1) k)
@@ -455,7 +484,7 @@ void GraphGmres::prepare(Solver &S) {
     W.h2 = W.h1 + (k + 2);
     W.y = W.h2 + (k + 2);
     W.hh = W.y + k;
-    partials.alloc((size_t)(k + 2) * G);
+    partials.alloc((size_t)(k + 2) * std::max(G, G2));
     norms.alloc((size_t)max_iter + 2);
     summary.alloc(8);
     cin.alloc(nn);
@@ -545,15 +574,13 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         scatter_kernel<<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st);
         JX_LAUNCH_CHECK();
         bsr_spmv<double, double>(A, 1.0, cout.get(), 0.0, w, kerr, s2, staged);
-        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, 0, pt);
+        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, pt);
         JX_LAUNCH_CHECK();
         reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, W.h1);
         JX_LAUNCH_CHECK();
-        update_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h1, w);
+        update_dots_kernel<<<G2, kThreads, 0, s2>>>(nn, V, st, W.h1, w, pt);
         JX_LAUNCH_CHECK();
-        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, 1, pt);
-        JX_LAUNCH_CHECK();
-        arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, P, W, norms.get(), h_in);
+        arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G2, st, P, W, norms.get(), h_in);
         JX_LAUNCH_CHECK();
         final_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h2, w);
         JX_LAUNCH_CHECK();

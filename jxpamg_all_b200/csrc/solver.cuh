@@ -182,7 +182,7 @@ struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
 // replay a graph of their own; batches record many solvers into one graph.
 struct GraphGmres {
     long long n = 0;
-    int k = 0, max_iter = 0, G = 1, G1 = 1;
+    int k = 0, max_iter = 0, G = 1, G1 = 1, G2 = 1;
     GgParams P{};
     GgWork W{};
     DevBuf<GgState> state;
