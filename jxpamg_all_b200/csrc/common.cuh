@@ -13,6 +13,7 @@
 
 #include <cstddef>
 #include <string>
+#include <utility>
 
 #define JXCPR_SUCCESS 0
 #define JXCPR_ERROR_GENERIC 1
@@ -58,6 +59,39 @@ void count_launches(unsigned long long n);  // kernels replayed by a CUDA graph 
         ::jxcpr::count_launch();              \
         JX_CUDA(cudaGetLastError());          \
     } while (0)
+
+// Programmatic dependent launch.  A kernel launched by launch_dep while
+// tl_dep_launch is set carries the programmatic-stream-serialization
+// attribute (in a captured graph: a programmatic edge), so the GPU may start
+// scheduling its blocks while the kernel before it drains.  Every kernel
+// launched that way calls grid_dep_wait() before it reads or writes global
+// memory: the wait returns once the previous kernel has completed and its
+// writes are visible (at once for a kernel launched without the attribute).
+__device__ __forceinline__ void grid_dep_wait() {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+extern thread_local int tl_dep_launch;
+struct DepLaunchScope {
+    int saved;
+    explicit DepLaunchScope(int on) : saved(tl_dep_launch) { tl_dep_launch = on; }
+    ~DepLaunchScope() { tl_dep_launch = saved; }
+};
+template <typename... KArgs, typename... Args>
+void launch_dep(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = tl_dep_launch ? 1 : 0;
+    JX_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
 
 // Device memory cache behind DevBuf.  Blocks are bucketed (powers of two up
 // to 1 GiB, 256 MiB multiples above); buckets up to 1 MiB are carved from

@@ -95,6 +95,7 @@ struct FastOptions {
     int sell_min_rows = 16384; // without autotuning: sliced ELL for operators with at least this many rows ...
     double sell_max_mean = 40; // ... and at most this mean row length
     int graphs = 1;            // replay each preconditioner application as one captured CUDA graph
+    int dep_launch = 1;        // kernels of an application launched as programmatic dependents (launch_dep)
     int autotune = 1;          // time the layouts (CSR with 1..32 lanes, sliced ELL) of every operator, keep the fastest;
                                // 2: share the choice among operators of one shape class (batches)
     // per-level Chebyshev interval overrides (learned); empty = use cheb_lower/upper

@@ -43,7 +43,8 @@ template <typename TX, int V, typename TV, class Op>
 void launch_csr(const LevelMat &M, const TV *a, const Op &op, int r0, int r1, cudaStream_t s) {
     fk::CsrFmt<V, TV> f{M.ia.get(), M.ja.get(), a, M.rscale.get(), M.perm};
     const long long threads = (long long)(r1 - r0) * V;
-    fk::row_kernel<fk::CsrFmt<V, TV>, Op, TX><<<div_up(threads, kThreads), kThreads, 0, s>>>(f, op, r0, r1);
+    launch_dep(fk::row_kernel<fk::CsrFmt<V, TV>, Op, TX>, dim3(div_up(threads, kThreads)), dim3(kThreads), s,
+               f, op, r0, r1);
 }
 
 template <typename TX, class Op>
@@ -53,7 +54,8 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
         using TV = typename std::remove_cv<typename std::remove_pointer<decltype(a)>::type>::type;
         if (M.sell) {
             fk::SellFmt<TV> f{M.sp.get(), M.ja.get(), a, M.rscale.get(), M.rows.get()};
-            fk::row_kernel<fk::SellFmt<TV>, Op, TX><<<div_up(r1 - r0, kThreads), kThreads, 0, s>>>(f, op, r0, r1);
+            launch_dep(fk::row_kernel<fk::SellFmt<TV>, Op, TX>, dim3(div_up(r1 - r0, kThreads)), dim3(kThreads), s,
+                       f, op, r0, r1);
             return;
         }
         switch (M.lanes) {
@@ -377,6 +379,7 @@ std::vector<int> download_ints(const int *d, int n, cudaStream_t s) {
 
 template <typename TX>
 __global__ void add_kernel(int n, TX *__restrict__ u, const TX *__restrict__ c) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) u[i] += c[i];
 }
@@ -512,7 +515,8 @@ struct FastCpr final : FastCprBase {
     }
     void coarse(const TX *f, TX *u, cudaStream_t s) {
         if (nc == 0) return;
-        fk::dense_gemv<TX><<<div_up((long long)nc * 32, kThreads), kThreads, 0, s>>>(nc, Ainv, f, u);
+        launch_dep(fk::dense_gemv<TX>, dim3(div_up((long long)nc * 32, kThreads)), dim3(kThreads), s, nc, Ainv, f,
+                   u);
         JX_LAUNCH_CHECK();
     }
 
@@ -547,11 +551,11 @@ struct FastCpr final : FastCprBase {
 #define JX_HGS_CSR(VV)                                                                                        \
     do {                                                                                                      \
         if (bs == 2)                                                                                          \
-            fk::hgs_color<2, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
-                                                                    z, vtp, w, om, plain, so);                 \
+            launch_dep(fk::hgs_color<2, VV, TV, TAC, TXV>, dim3(grid), dim3(128), s, r0, r1, M.perm, M.ia.get(), \
+                       M.ja.get(), a, r, z, vtp, w, om, plain, so);                                          \
         else                                                                                                  \
-            fk::hgs_color<3, VV, TV, TAC, TXV><<<grid, 128, 0, s>>>(r0, r1, M.perm, M.ia.get(), M.ja.get(), a, r,\
-                                                                    z, vtp, w, om, plain, so);                 \
+            launch_dep(fk::hgs_color<3, VV, TV, TAC, TXV>, dim3(grid), dim3(128), s, r0, r1, M.perm, M.ia.get(), \
+                       M.ja.get(), a, r, z, vtp, w, om, plain, so);                                          \
     } while (0)
         switch (V) {
             case 1: JX_HGS_CSR(1); break;
@@ -598,17 +602,18 @@ struct FastCpr final : FastCprBase {
     }
     // FP64 interface (C ABI / tests): the mixed path converts in and out.
     void stage2_sweep(const double *r, double *z, cudaStream_t s) override {
+        DepLaunchScope dep(opt.dep_launch);
         if (std::is_same<TX, double>::value || st2.kind == VAL_F64) {
             sweep_typed<double>(r, z, vt.get(), s);
         } else {
             const long long n = (long long)nb * bs;
             if (!n) return;
-            fk::convert<double, float><<<div_up(n, kThreads), kThreads, 0, s>>>(n, r, r32.get());
+            launch_dep(fk::convert<double, float>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, r, r32.get());
             JX_LAUNCH_CHECK();
-            fk::convert<double, float><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z, z32.get());
+            launch_dep(fk::convert<double, float>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, z, z32.get());
             JX_LAUNCH_CHECK();
             sweep_typed<float>(r32.get(), z32.get(), vt32.get(), s);
-            fk::convert<float, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z32.get(), z);
+            launch_dep(fk::convert<float, double>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, z32.get(), z);
             JX_LAUNCH_CHECK();
         }
     }
@@ -618,10 +623,12 @@ struct FastCpr final : FastCprBase {
         if (M.sell) {
             const int grid = div_up(r1 - r0, kThreads);
             if (bs == 2)
-                fk::hgs_sell<2, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                launch_dep(fk::hgs_sell<2, TV, TAC, TXV>, dim3(grid), dim3(kThreads), s,
+                           r0, r1, M.sp.get(), M.ja.get(), a,
                                                                        M.rows.get(), r, z, vtp, w, om, plain, so);
             else
-                fk::hgs_sell<3, TV, TAC, TXV><<<grid, kThreads, 0, s>>>(r0, r1, M.sp.get(), M.ja.get(), a,
+                launch_dep(fk::hgs_sell<3, TV, TAC, TXV>, dim3(grid), dim3(kThreads), s,
+                           r0, r1, M.sp.get(), M.ja.get(), a,
                                                                        M.rows.get(), r, z, vtp, w, om, plain, so);
         } else {
             launch_hgs_csr<TV, TXV, TAC>(opt.stage2_lanes, M, a, r0, r1, r, z, vtp, w, om, plain, so, s);
@@ -679,13 +686,16 @@ struct FastCpr final : FastCprBase {
     void apply_enqueue(const double *r, double *z, cudaStream_t s) override { apply_direct(r, z, s); }
 
     void apply_direct(const double *r, double *z, cudaStream_t s) {
+        DepLaunchScope dep(opt.dep_launch);
         FastLevel<TX> &L0 = *lv[0];
         constexpr bool fp64 = std::is_same<TX, double>::value;
         const long long n = (long long)nb * bs;
         if (fp64) {
-            fk::restrict_p<TX><<<div_up(nb, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get());
+            launch_dep(fk::restrict_p<TX>, dim3(div_up(nb, kThreads)), dim3(kThreads), s,
+                       nb, bs, cfg.pressure_index, r, L0.f.get());
         } else {
-            fk::restrict_cvt<TX><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, r, L0.f.get(),
+            launch_dep(fk::restrict_cvt<TX>, dim3(div_up(n, kThreads)), dim3(kThreads), s,
+                       nb, bs, cfg.pressure_index, r, L0.f.get(),
                                                                         r32.get());
         }
         JX_LAUNCH_CHECK();
@@ -694,13 +704,15 @@ struct FastCpr final : FastCprBase {
             // further AMG iterations as residual corrections: u += V(f - A u)
             residual(L0, L0.f.get(), L0.u.get(), L0.r.get(), s);
             vcycle_tx(L0.r.get(), L0.c.get(), s);
-            add_kernel<TX><<<div_up(L0.n, kThreads), kThreads, 0, s>>>(L0.n, L0.u.get(), L0.c.get());
+            launch_dep(add_kernel<TX>, dim3(div_up(L0.n, kThreads)), dim3(kThreads), s, L0.n, L0.u.get(),
+                       L0.c.get());
             JX_LAUNCH_CHECK();
         }
         const bool st2_on = cfg.stage2_solver_type == 2 && cfg.stage2_maxit > 0;
         if (fp64 || !st2_on || st2.kind == VAL_F64) {
             // FP64 stage 2 on the caller's vectors (FP64 path; hybrid form: FP32 stage 1, FP64 polish)
-            fk::prolong_p<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index,
+            launch_dep(fk::prolong_p<TX, double>, dim3(div_up(n, kThreads)), dim3(kThreads), s,
+                       nb, bs, cfg.pressure_index,
                                                                               L0.u.get(), z);
             JX_LAUNCH_CHECK();
             if (st2_on)
@@ -708,21 +720,23 @@ struct FastCpr final : FastCprBase {
             return;
         }
         // mixed path: stage 2 on FP32 copies of r and z, result converted to FP64
-        fk::prolong_p<TX, float><<<div_up(n, kThreads), kThreads, 0, s>>>(nb, bs, cfg.pressure_index, L0.u.get(),
+        launch_dep(fk::prolong_p<TX, float>, dim3(div_up(n, kThreads)), dim3(kThreads), s,
+                   nb, bs, cfg.pressure_index, L0.u.get(),
                                                                          z32.get());
         JX_LAUNCH_CHECK();
         for (int it = 0; it < cfg.stage2_maxit; ++it) sweep_typed<float>(r32.get(), z32.get(), vt32.get(), s);
-        fk::convert<float, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, z32.get(), z);
+        launch_dep(fk::convert<float, double>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, z32.get(), z);
         JX_LAUNCH_CHECK();
     }
 
     void vcycle(const double *fp, double *up, cudaStream_t s) override {
+        DepLaunchScope dep(opt.dep_launch);
         FastLevel<TX> &L0 = *lv[0];
         const int n = L0.n;
-        fk::convert<double, TX><<<div_up(n, kThreads), kThreads, 0, s>>>(n, fp, L0.f.get());
+        launch_dep(fk::convert<double, TX>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, fp, L0.f.get());
         JX_LAUNCH_CHECK();
         vcycle_tx(L0.f.get(), L0.u.get(), s);
-        fk::convert<TX, double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, L0.u.get(), up);
+        launch_dep(fk::convert<TX, double>, dim3(div_up(n, kThreads)), dim3(kThreads), s, n, L0.u.get(), up);
         JX_LAUNCH_CHECK();
     }
 
@@ -741,6 +755,7 @@ struct FastCpr final : FastCprBase {
     DevBuf<TX> nat_r, nat_z;
     DevBuf<double> nat_r64, nat_z64;  // hybrid form: the FP64 stage 2 timed on FP64 vectors
     void stage2_native(int sweeps, cudaStream_t s) override {
+        DepLaunchScope dep(opt.dep_launch);
         const long long n = (long long)nb * bs;
         if (!n) return;
         if (!nat_r.get()) {

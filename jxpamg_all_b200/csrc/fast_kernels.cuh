@@ -203,6 +203,7 @@ struct OpCheb {
 // One launch of `op` over stored rows [r0, r1) of a matrix in format Fmt.
 template <class Fmt, class Op, typename TX>
 __global__ void __launch_bounds__(256) row_kernel(Fmt fmt, Op op, int r0, int r1) {
+    grid_dep_wait();
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int t = r0 + (int)(gt / Fmt::V);
     const int lane = (int)(gt % Fmt::V);
@@ -221,12 +222,14 @@ __global__ void __launch_bounds__(256) row_kernel(Fmt fmt, Op op, int r0, int r1
 
 template <typename TX>
 __global__ void restrict_p(int nb, int bs, int p, const double *__restrict__ r, TX *__restrict__ rp) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nb) rp[i] = (TX)r[(long long)i * bs + p];
 }
 
 template <typename TX, typename TZ>
 __global__ void prolong_p(int nb, int bs, int p, const TX *__restrict__ up, TZ *__restrict__ z) {
+    grid_dep_wait();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nb * bs) return;
     const int i = (int)(t / bs), k = (int)(t % bs);
@@ -237,6 +240,7 @@ __global__ void prolong_p(int nb, int bs, int p, const TX *__restrict__ up, TZ *
 template <typename TX>
 __global__ void restrict_cvt(int nb, int bs, int p, const double *__restrict__ r, TX *__restrict__ rp,
                              float *__restrict__ r32) {
+    grid_dep_wait();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)nb * bs) return;
     const double v = r[t];
@@ -247,6 +251,7 @@ __global__ void restrict_cvt(int nb, int bs, int p, const double *__restrict__ r
 // u = Ainv f (FP64 inverse of the coarsest operator), one warp per row.
 template <typename TX>
 __global__ void dense_gemv(int n, const double *__restrict__ Ainv, const TX *__restrict__ f, TX *__restrict__ u) {
+    grid_dep_wait();
     const int row = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -327,6 +332,7 @@ template <int BS, int V, typename TV, typename TA, typename TXV>
 __global__ void hgs_color(int r0, int r1, const int *__restrict__ perm, const int *__restrict__ ia,
                           const int *__restrict__ ja, const TV *__restrict__ a, const TXV *__restrict__ b,
                           TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
+    grid_dep_wait();
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int t = r0 + (int)(gt / V);
     const int lane = (int)(gt % V);
@@ -376,6 +382,7 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
                                                 const int *__restrict__ col, const TV *__restrict__ a,
                                                 const int *__restrict__ rows, const TXV *__restrict__ b,
                                                 TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
+    grid_dep_wait();
     const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= r1) return;
     const int i = __ldg(rows + t);
@@ -532,6 +539,7 @@ __global__ void dinv_a_x(int n, const int *__restrict__ ia, const int *__restric
 
 template <typename TA, typename TB>
 __global__ void convert(long long n, const TA *__restrict__ in, TB *__restrict__ out) {
+    grid_dep_wait();
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (TB)in[i];
 }

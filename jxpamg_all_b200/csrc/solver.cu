@@ -73,6 +73,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         opt.stage2_lanes = prm.stage2_lanes;
         opt.autotune = prm.autotune;
         opt.graphs = prm.graphs;
+        opt.dep_launch = prm.dep_launch;
         if (plan.active) {
             opt.level_lower = plan.lower;
             opt.level_upper = plan.upper;

@@ -58,6 +58,7 @@ struct SolverParams {
     // fast path: the coarsening's first pass on row ranges of this many rows, one host thread per
     // range (levels with fewer than twice as many rows, and the exact order always, take one pass)
     int rs_range_rows = 131072;
+    int dep_launch = 1;  // fast path: programmatic dependent launches inside each CPR application
     int use_tma_spmv = 0;
     // fast path (smoother_order 1)
     int precision = 0;       // 0 FP64, 1 FP32 preconditioner, 2 FP32 + BF16 coarse levels, 3 the reference's

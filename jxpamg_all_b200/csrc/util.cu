@@ -31,6 +31,8 @@ void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_
 void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+thread_local int tl_dep_launch = 0;
+
 // ---- device memory cache --------------------------------------------------
 namespace {
 thread_local cudaStream_t t_stream = nullptr;
