@@ -326,106 +326,158 @@ __global__ void interp_bound_kernel(int n, const int *__restrict__ sia, const in
     bound[i] = b;
 }
 
-__device__ __forceinline__ int find_in(const int *list, int len, int v) {
+// Lowest t < len with list[t] == v, or -1: the whole warp searches (v uniform).
+__device__ __forceinline__ int warp_find(const int *list, int len, int v) {
+    const int lane = threadIdx.x & 31;
+    for (int t0 = 0; t0 < len; t0 += 32) {
+        const int t = t0 + lane;
+        const unsigned hit = __ballot_sync(0xffffffffu, t < len && list[t] == v);
+        if (hit) return t0 + __ffs(hit) - 1;
+    }
+    return -1;
+}
+
+// One lane's own search (lanes look for different values).
+__device__ __forceinline__ int lane_find(const int *list, int len, int v) {
     for (int t = 0; t < len; ++t)
         if (list[t] == v) return t;
     return -1;
 }
 
-// Discovery-ordered interpolation set of each F row (fine indices, deduped).
+// Discovery-ordered interpolation set of each F row (fine indices, deduped),
+// one warp per row: the candidates are taken in order, each one searched for
+// by the whole warp in the set built so far.
 __global__ void interp_list_kernel(int n, const int *__restrict__ sia, const int *__restrict__ sja,
                                    const int *__restrict__ cf, const long long *__restrict__ boff,
                                    int *__restrict__ scratch, int *__restrict__ cnt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= n) return;  // whole warps
+    const int i = (int)gw;
     const int ci = cf[i];
-    if (ci >= 0) {
-        cnt[i] = 1;
-        return;
-    }
-    if (ci == CF_SF) {
-        cnt[i] = 0;
+    if (ci >= 0 || ci == CF_SF) {
+        if (lane == 0) cnt[i] = ci >= 0 ? 1 : 0;
         return;
     }
     int *list = scratch + boff[i];
     int len = 0;
+    auto add = [&](int v) {
+        if (warp_find(list, len, v) < 0) {
+            if (lane == 0) list[len] = v;
+            __syncwarp();
+            ++len;
+        }
+    };
     for (int k = sia[i]; k < sia[i + 1]; ++k) {
         const int i1 = sja[k];
         const int c1 = cf[i1];
         if (c1 >= 0) {
-            if (find_in(list, len, i1) < 0) list[len++] = i1;
+            add(i1);
         } else if (c1 != CF_SF) {
             for (int q = sia[i1]; q < sia[i1 + 1]; ++q) {
                 const int k1 = sja[q];
-                if (cf[k1] >= 0 && find_in(list, len, k1) < 0) list[len++] = k1;
+                if (cf[k1] >= 0) add(k1);
             }
         }
     }
-    cnt[i] = len;
+    if (lane == 0) cnt[i] = len;
 }
 
-__device__ __forceinline__ bool is_strong_f(const int *__restrict__ sia, const int *__restrict__ sja,
-                                            const int *__restrict__ cf, int i, int i1) {
+// i1 a strong F neighbour of i (whole warp)
+__device__ __forceinline__ bool warp_is_strong_f(const int *__restrict__ sia, const int *__restrict__ sja,
+                                                 const int *__restrict__ cf, int i, int i1) {
     const int c1 = cf[i1];
     if (c1 >= 0 || c1 == CF_SF) return false;
-    for (int k = sia[i]; k < sia[i + 1]; ++k)
-        if (sja[k] == i1) return true;
-    return false;
+    return warp_find(sja + sia[i], sia[i + 1] - sia[i], i1) >= 0;
 }
 
+// Weights of each F row, one warp per row.  Every floating-point operation is
+// the sequential row algorithm's, in its order: the entries of row i are
+// taken one after another (the warp only searches the interpolation set in
+// parallel); the sum over a strong F neighbour's row is accumulated in column
+// order from flags computed 32 entries at a time; the distribution adds to
+// distinct weights (distinct columns), so its lanes may run side by side.
 __global__ void interp_fill_kernel(int n, const int *__restrict__ aia, const int *__restrict__ aja,
                                    const double *__restrict__ aa, const int *__restrict__ sia,
                                    const int *__restrict__ sja, const int *__restrict__ cf,
                                    const int *__restrict__ f2c, const long long *__restrict__ boff,
                                    const int *__restrict__ scratch, const int *__restrict__ pia,
                                    int *__restrict__ pja, double *__restrict__ pa) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= n) return;  // whole warps
+    const int i = (int)gw;
     const int ci = cf[i];
     const int jb = pia[i];
     if (ci >= 0) {
-        pja[jb] = f2c[i];
-        pa[jb] = 1.0;
+        if (lane == 0) {
+            pja[jb] = f2c[i];
+            pa[jb] = 1.0;
+        }
         return;
     }
     if (ci == CF_SF) return;
     const int *list = scratch + boff[i];
     const int len = pia[i + 1] - jb;
-    for (int t = 0; t < len; ++t) {
+    for (int t = lane; t < len; t += 32) {
         pja[jb + t] = f2c[list[t]];
         pa[jb + t] = 0.0;
     }
+    __syncwarp();
     if (aia[i] == aia[i + 1]) return;  // empty row
     double diagonal = aa[aia[i]];
     for (int k = aia[i] + 1; k < aia[i + 1]; ++k) {
         const int i1 = aja[k];
-        const int slot = find_in(list, len, i1);
+        const int slot = warp_find(list, len, i1);
         if (slot >= 0) {
-            pa[jb + slot] += aa[k];
-        } else if (is_strong_f(sia, sja, cf, i, i1)) {
+            if (lane == 0) pa[jb + slot] += aa[k];
+        } else if (warp_is_strong_f(sia, sja, cf, i, i1)) {
             double sum = 0.0;
             int sgn = 1;
             if (aia[i1] < aia[i1 + 1] && aa[aia[i1]] < 0) sgn = -1;
-            for (int q = aia[i1] + 1; q < aia[i1 + 1]; ++q) {
-                const int i2 = aja[q];
-                if ((find_in(list, len, i2) >= 0 || i2 == i) && (sgn * aa[q]) < 0) sum += aa[q];
+            const int qb = aia[i1] + 1, qe = aia[i1 + 1];
+            for (int q0 = qb; q0 < qe; q0 += 32) {
+                const int q = q0 + lane;
+                double v = 0.0;
+                int f = 0;
+                if (q < qe) {
+                    const int i2 = aja[q];
+                    v = aa[q];
+                    f = ((i2 == i || lane_find(list, len, i2) >= 0) && (sgn * v) < 0) ? 1 : 0;
+                }
+                const int m = min(32, qe - q0);
+                for (int u = 0; u < m; ++u) {
+                    const double vu = __shfl_sync(0xffffffffu, v, u);
+                    if (__shfl_sync(0xffffffffu, f, u)) sum += vu;
+                }
             }
             if (sum != 0) {
                 const double distribute = aa[k] / sum;
-                for (int q = aia[i1] + 1; q < aia[i1 + 1]; ++q) {
+                double dadd = 0.0;
+                int has = 0;
+                for (int q = qb + lane; q < qe; q += 32) {
                     const int i2 = aja[q];
-                    const int s2 = find_in(list, len, i2);
-                    if (s2 >= 0 && (sgn * aa[q]) < 0) pa[jb + s2] += distribute * aa[q];
-                    if (i2 == i && (sgn * aa[q]) < 0) diagonal += distribute * aa[q];
+                    const double v = aa[q];
+                    if ((sgn * v) < 0) {
+                        const int s2 = lane_find(list, len, i2);
+                        if (s2 >= 0) pa[jb + s2] += distribute * v;
+                        if (i2 == i) {
+                            dadd = distribute * v;
+                            has = 1;
+                        }
+                    }
                 }
+                const unsigned hb = __ballot_sync(0xffffffffu, has);
+                if (hb) diagonal += __shfl_sync(0xffffffffu, dadd, __ffs(hb) - 1);
             } else {
                 diagonal += aa[k];
             }
         } else if (cf[i1] != CF_SF) {
             diagonal += aa[k];
         }
+        __syncwarp();
     }
-    for (int t = 0; t < len; ++t) pa[jb + t] /= -diagonal;
+    for (int t = lane; t < len; t += 32) pa[jb + t] /= -diagonal;
 }
 
 int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *cf_dev, DeviceCsr &P,
@@ -448,7 +500,8 @@ int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *c
     JX_CUDA(cudaStreamSynchronize(s));
     DevBuf<int> scratch(total > 0 ? total : 1);
     cnt.zero(s);
-    interp_list_kernel<<<grid, 256, 0, s>>>(n, S.ia.get(), S.ja.get(), cf_dev, boff.get(), scratch.get(),
+    const int wgrid = (int)div_up((long long)n * 32, 256);  // one warp per row
+    interp_list_kernel<<<wgrid, 256, 0, s>>>(n, S.ia.get(), S.ja.get(), cf_dev, boff.get(), scratch.get(),
                                             cnt.get());
     JX_LAUNCH_CHECK();
     DevBuf<int> pia(n + 1);
@@ -462,7 +515,7 @@ int amg_extpi_interp(const CsrView<double> &A, const DevPattern &S, const int *c
     P.ia = std::move(pia);
     P.ja.alloc(nnz > 0 ? nnz : 1);
     P.a.alloc(nnz > 0 ? nnz : 1);
-    interp_fill_kernel<<<grid, 256, 0, s>>>(n, A.ia, A.ja, A.a, S.ia.get(), S.ja.get(), cf_dev, f2c.get(),
+    interp_fill_kernel<<<wgrid, 256, 0, s>>>(n, A.ia, A.ja, A.a, S.ia.get(), S.ja.get(), cf_dev, f2c.get(),
                                             boff.get(), scratch.get(), P.ia.get(), P.ja.get(), P.a.get());
     JX_LAUNCH_CHECK();
     JX_CUDA(cudaStreamSynchronize(s));
