@@ -120,6 +120,8 @@ JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *
  *         ranges of this size, as each process of a distributed run does it,
  *         par_coarsen_ruge.c:37-44; 0 one pass over the level),
  *         coarse_exact (1 substitution in the reference's order, 0 inverse),
+ *         dep_launch (1; order 1: the preconditioner's kernels launched as
+ *         programmatic dependents inside its CUDA graphs),
  *         use_tma_spmv (1), print_level, logging, block_size (ignored)
  *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),
  *         convfac_threshold (1e4), stage2_relax_weight (0.7), stage2_omega (0.9)
