@@ -73,6 +73,38 @@ def _f64(a):
 
 
 # ---- restatement ---------------------------------------------------------------
+def strength(ia, ja, a, theta=0.25, max_row_sum=0.9):
+    """Strength pattern (sia, sja) of a CSR operator (par_strength.c rules)."""
+    ia, ja, a = _i32(ia), _i32(ja), _f64(a)
+    n = len(ia) - 1
+    sia = np.zeros(n + 1, np.int32)
+    nnz = orc().orc_strength_csr(c_int(n), _p(ia), _p(ja), _p(a), c_double(theta), c_double(max_row_sum),
+                                 _p(sia), None)
+    sja = np.zeros(max(nnz, 1), np.int32)
+    orc().orc_strength_csr(c_int(n), _p(ia), _p(ja), _p(a), c_double(theta), c_double(max_row_sum), _p(sia),
+                           _p(sja))
+    return sia, sja[:nnz]
+
+
+def rs_first_pass(sia, sja, range_rows=0):
+    """Markers of the Ruge-Stueben first pass on a strength pattern (row ranges when > 0)."""
+    sia, sja = _i32(sia), _i32(sja)
+    n = len(sia) - 1
+    cf = np.zeros(n, np.int32)
+    orc().orc_rs_first_pass_csr(c_int(n), _p(sia), _p(sja), c_int(range_rows), _p(cf))
+    return cf
+
+
+def ref_rs_first_pass(sia, sja):
+    """The reference's first pass (jxf_PAMGCoarsenRuge, coarsen_type 10) on a strength pattern."""
+    sia, sja = _i32(sia), _i32(sja)
+    n = len(sia) - 1
+    cf = np.zeros(n, np.int32)
+    if ref().ref_rs_first_pass(c_int(n), _p(sia), _p(sja if len(sja) else np.zeros(1, np.int32)), _p(cf)) != 0:
+        raise RuntimeError("reference first pass failed")
+    return cf
+
+
 def hmis_cf(ia, ja, a, theta=0.25, max_row_sum=0.9, range_rows=0):
     """C/F splitting of a CSR operator: strength, the Ruge-Stueben first pass (on row ranges of
     range_rows rows when > 0) and the PMIS pass; C points 1, F points -1."""

@@ -53,6 +53,9 @@ void orc_hmis(const orc_csr *S, int *CF);
 void orc_rs_first_pass_ranges(const orc_csr *S, int range_rows, int *CF);
 void orc_hmis_ranges(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,
                      int range_rows, int *CF);
+int orc_strength_csr(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,
+                     int *sia, int *sja);
+void orc_rs_first_pass_csr(int n, const int *sia, const int *sja, int range_rows, int *cf);
 void orc_extpi_interp(const orc_csr *A, const orc_csr *S, const int *CF, orc_csr *P);
 void orc_rap(const orc_csr *A, const orc_csr *P, orc_csr *Ac);
 void orc_amg_setup(const orc_csr *A0, int max_levels, int coarse_threshold, orc_amg *H);

@@ -401,6 +401,35 @@ void orc_hmis(const orc_csr *S, int *CF)
     orc_pmis(S, CF);
 }
 
+/* Strength pattern of a CSR operator into the caller's arrays (sia[n+1];
+ * with sja == NULL only the entry count is returned). */
+int orc_strength_csr(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,
+                     int *sia, int *sja)
+{
+    orc_csr A, S;
+    A.n = A.m = n;
+    A.ia = (int *)ia;
+    A.ja = (int *)ja;
+    A.a = (double *)a;
+    orc_strength(&A, theta, max_row_sum, &S);
+    int nnz = S.ia[n];
+    if (sia) memcpy(sia, S.ia, sizeof(int) * (n + 1));
+    if (sja) memcpy(sja, S.ja, sizeof(int) * nnz);
+    orc_csr_free(&S);
+    return nnz;
+}
+
+/* The first pass (on row ranges when range_rows > 0) on a strength pattern. */
+void orc_rs_first_pass_csr(int n, const int *sia, const int *sja, int range_rows, int *cf)
+{
+    orc_csr S;
+    S.n = S.m = n;
+    S.ia = (int *)sia;
+    S.ja = (int *)sja;
+    S.a = NULL;
+    orc_rs_first_pass_ranges(&S, range_rows, cf);
+}
+
 /* HMIS with the first pass on row ranges, on a CSR operator: strength
  * (theta, max_row_sum) then orc_rs_first_pass_ranges and the PMIS pass. */
 void orc_hmis_ranges(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,

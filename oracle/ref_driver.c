@@ -26,7 +26,7 @@
 #include "jxf_parbsr_mv.h"
 #include "jxf_parbilu.h"
 
-int ref_driver_version(void) { return 2; }
+int ref_driver_version(void) { return 3; }
 
 /* ---- stdout silencing ------------------------------------------------- */
 static int g_saved_stdout = -1;
@@ -258,6 +258,31 @@ int ref_cpr_amg_solve(void *hv, const double *rp, double *xp, int quiet)
                              (JXF_ParVector)cpr->xp);
     quiet_end(quiet);
     memcpy(xp, pvec_data(cpr->xp), sizeof(double) * h->nb);
+    return ierr;
+}
+
+/* The Ruge-Stueben first pass of the reference's HMIS (jxf_PAMGCoarsenRuge
+ * with coarsen_type 10, as par_coarsen_hmis.c:32 calls it) on a strength
+ * pattern given as CSR, one process.  cf receives its markers (1 C, -1 F,
+ * -2 Z, -3 SF). */
+int ref_rs_first_pass(int n, const int *ia, const int *ja, int *cf)
+{
+    int nnz = ia[n];
+    JXF_Int *rs = NULL;
+    jxf_GeneratePartitioning(n, 1, &rs);
+    jxf_ParCSRMatrix *S = jxf_ParCSRMatrixCreate(MPI_COMM_WORLD, n, n, rs, rs, 0, nnz, 0);
+    jxf_ParCSRMatrixInitialize(S);
+    jxf_CSRMatrix *d = jxf_ParCSRMatrixDiag(S);
+    memcpy(jxf_CSRMatrixI(d), ia, sizeof(int) * (n + 1));
+    if (nnz) memcpy(jxf_CSRMatrixJ(d), ja, sizeof(int) * nnz);
+    for (int k = 0; k < nnz; k++) jxf_CSRMatrixData(d)[k] = 1.0;
+    JXF_Int *CF = NULL;
+    int ierr = jxf_PAMGCoarsenRuge(S, S, 0, 10, 0, &CF);
+    if (CF) {
+        memcpy(cf, CF, sizeof(int) * n);
+        jxf_TFree(CF);
+    }
+    jxf_ParCSRMatrixDestroy(S);
     return ierr;
 }
 
