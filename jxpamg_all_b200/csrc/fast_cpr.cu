@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 
 #include "fast.cuh"
@@ -73,45 +74,71 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
 // ---- construction -----------------------------------------------------------------
 // Sliced-ELL layout on the host: segments of `order` (offsets seg_in), rows
 // sorted by decreasing length inside windows (a stable counting sort: equal
-// lengths keep their order), each segment padded to whole slices.
+// lengths keep their order), each segment padded to whole slices.  Windows
+// are independent (each starts on a slice boundary), so large layouts sort
+// them on host threads.
 void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, const std::vector<int> &seg_in,
                  std::vector<int> &rows, std::vector<long long> &sp, std::vector<int> &seg_out) {
+    struct Win {
+        int w0, w1;
+        size_t pos;
+    };
+    std::vector<Win> wins;
     seg_out.assign(1, 0);
-    size_t total = 0;
-    for (size_t c = 0; c + 1 < seg_in.size(); ++c) total += (size_t)(seg_in[c + 1] - seg_in[c] + 31) / 32 * 32;
-    rows.assign(total, -1);
-    std::vector<int> rlen(total, 0), len, cnt;
     size_t pos = 0;
     for (size_t c = 0; c + 1 < seg_in.size(); ++c) {
         for (int w0 = seg_in[c]; w0 < seg_in[c + 1]; w0 += kSellWindow) {
-            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow), nw = w1 - w0;
+            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow);
+            wins.push_back({w0, w1, pos});
+            pos += w1 - w0;
+        }
+        pos = (pos + 31) / 32 * 32;
+        seg_out.push_back((int)pos);
+    }
+    const size_t total = pos, ns = total / 32;
+    rows.assign(total, -1);
+    std::vector<int> width(ns, 0);
+    auto sort_windows = [&](size_t b, size_t e) {
+        std::vector<int> len, cnt, slen;
+        for (size_t k = b; k < e; ++k) {
+            const Win &W = wins[k];
+            const int nw = W.w1 - W.w0;
             len.resize(nw);
+            slen.resize(nw);
             int maxlen = 0;
             for (int t = 0; t < nw; ++t) {
-                const int i = order[w0 + t];
+                const int i = order[W.w0 + t];
                 len[t] = ia[i + 1] - ia[i];
                 maxlen = std::max(maxlen, len[t]);
             }
             cnt.assign((size_t)maxlen + 2, 0);  // key maxlen - len: longest rows first
             for (int t = 0; t < nw; ++t) cnt[maxlen - len[t] + 1]++;
-            for (int k = 0; k <= maxlen; ++k) cnt[k + 1] += cnt[k];
+            for (int q = 0; q <= maxlen; ++q) cnt[q + 1] += cnt[q];
             for (int t = 0; t < nw; ++t) {
-                const size_t q = pos + cnt[maxlen - len[t]]++;
-                rows[q] = order[w0 + t];
-                rlen[q] = len[t];
+                const int q = cnt[maxlen - len[t]]++;
+                rows[W.pos + q] = order[W.w0 + t];
+                slen[q] = len[t];
             }
-            pos += nw;
+            // a window starts on a slice boundary and its slices hold its rows alone (the
+            // padding of a segment's last slice follows its last window), longest first
+            for (int q = 0; q < nw; q += 32) width[W.pos / 32 + q / 32] = slen[q];
         }
-        pos = (pos + 31) / 32 * 32;
-        seg_out.push_back((int)pos);
+    };
+    const size_t nwin = wins.size();
+    const int threads = total >= (size_t)(1 << 16)
+                            ? (int)std::min<size_t>(std::min<size_t>(nwin, 16),
+                                                    std::max(1u, std::thread::hardware_concurrency()))
+                            : 1;
+    if (threads <= 1) {
+        sort_windows(0, nwin);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < threads; ++t) pool.emplace_back(sort_windows, nwin * t / threads, nwin * (t + 1) / threads);
+        sort_windows(0, nwin / threads);
+        for (auto &th : pool) th.join();
     }
-    const size_t ns = total / 32;
     sp.assign(ns + 1, 0);
-    for (size_t sl = 0; sl < ns; ++sl) {
-        int w = 0;
-        for (int q = 0; q < 32; ++q) w = std::max(w, rlen[sl * 32 + q]);
-        sp[sl + 1] = sp[sl] + 32LL * w;
-    }
+    for (size_t sl = 0; sl < ns; ++sl) sp[sl + 1] = sp[sl] + 32LL * width[sl];
 }
 
 template <typename TV>
