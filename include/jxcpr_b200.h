@@ -122,9 +122,22 @@ JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *
  *         coarse_exact (1 substitution in the reference's order, 0 inverse),
  *         dep_launch (1; order 1: the preconditioner's kernels launched as
  *         programmatic dependents inside its CUDA graphs),
- *         use_tma_spmv (1), print_level, logging, block_size (ignored)
+ *         use_tma_spmv (1), print_level, logging, block_size (ignored),
+ *         order-1 (fast path) choices: precision (0 FP64, 1 FP32, 2 FP32 + BF16
+ *         from level bf16_level (1), 3 FP32 stage 1 + FP64 stage 2),
+ *         fast_smoother (0 colour GS / l1-Jacobi, 1 Chebyshev-3 on the dense
+ *         levels, 2 learned settings, 3 Chebyshev-3 everywhere), max_colors (8:
+ *         levels needing more colours use l1-Jacobi), flexible (0), graphs (1),
+ *         graph_gmres (0), orthog (0 modified, 1 one-pass classical
+ *         Gram-Schmidt), autotune (1; 2 shared per shape class), stage2_lanes
+ *         (4: CSR stage 2 without autotuning), learned_fallback (1: the probe
+ *         and the stall guard may replace the learned settings),
+ *         record_features (0), thermal (0)
  *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),
- *         convfac_threshold (1e4), stage2_relax_weight (0.7), stage2_omega (0.9)
+ *         convfac_threshold (1e4), stage2_relax_weight (0.7), stage2_omega (0.9),
+ *         strong_threshold (0.25, jxf_cpr.c:331), strong_threshold_coarse (-1:
+ *         levels >= 1 use strong_threshold; fast path), cheb_lower (0.3),
+ *         cheb_upper (1.1): the Chebyshev interval times lambda_max(D^-1 A)
  */
 typedef struct jxcpr_solver jxcpr_solver;
 
