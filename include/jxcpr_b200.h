@@ -83,13 +83,19 @@ JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, doubl
  * reference: it exists for callers that cannot allocate device memory when
  * they need the product -- an application whose own memory pool has reserved
  * the whole device, or a time-critical loop that allows no allocator call
- * (cudaMalloc can synchronise the device and stall every stream).  The partial sums live in a static device array reserved
- * when the library loads (JXCPR_NOALLOC_DOT_MAX_PARTIALS partials of
+ * (cudaMalloc can synchronise the device and stall every stream).  The partial
+ * sums live in a static device array (JXCPR_NOALLOC_DOT_MAX_PARTIALS partials of
  * JXCPR_NOALLOC_DOT_CHUNK elements each, 512 KB per GPU, kept until exit), so
  * n is limited to JXCPR_NOALLOC_DOT_MAX_PARTIALS * JXCPR_NOALLOC_DOT_CHUNK
  * (268,435,456) elements; larger n returns JXCPR_ERROR_ARG with a message.
- * The first call on each device resolves the array's device address and
- * should come before any stream capture.  All calls share the array: calls
+ * The array is loaded with its code module on each device at the FIRST call
+ * there (CUDA loads modules lazily), which takes device memory once: make a
+ * warm-up call (n = 0 will do) on each device before your pool reserves it;
+ * later calls allocate nothing.  The first call also resolves the array's
+ * device address.  Every call copies the result to *out_host and synchronises
+ * `stream`, so it must not be called while that stream is being captured.
+ * The result equals jxcpr_dot_dev's up to rounding (a different, fixed
+ * summation order; both are deterministic).  All calls share the array: calls
  * that overlap on the GPU (concurrent streams) race and must be serialised. */
 #define JXCPR_NOALLOC_DOT_CHUNK 4096
 #define JXCPR_NOALLOC_DOT_MAX_PARTIALS 65536
@@ -130,14 +136,19 @@ JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *
  *         levels needing more colours use l1-Jacobi), flexible (0), graphs (1),
  *         graph_gmres (0), orthog (0 modified, 1 one-pass classical
  *         Gram-Schmidt), autotune (1; 2 shared per shape class), stage2_lanes
- *         (4: CSR stage 2 without autotuning), learned_fallback (1: the probe
+ *         (4: CSR stage 2 without autotuning), stage2_chunk (8: stage 2 visits
+ *         chunks of this many consecutive block rows in natural order, the
+ *         chunks coloured for parallelism; 4 or 16 also accepted; 0: the
+ *         level-0 colour order), learned_fallback (1: the probe
  *         and the stall guard may replace the learned settings),
  *         record_features (0), thermal (0)
  *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),
  *         convfac_threshold (1e4), stage2_relax_weight (0.7), stage2_omega (0.9),
  *         strong_threshold (0.25, jxf_cpr.c:331), strong_threshold_coarse (-1:
  *         levels >= 1 use strong_threshold; fast path), cheb_lower (0.3),
- *         cheb_upper (1.1): the Chebyshev interval times lambda_max(D^-1 A)
+ *         cheb_upper (1.1): the Chebyshev interval times lambda_max(D^-1 A),
+ *         jacobi_mean_row (12: fast path, levels with longer mean rows use
+ *         l1-Jacobi instead of multicolour GS)
  */
 typedef struct jxcpr_solver jxcpr_solver;
 
@@ -187,6 +198,17 @@ JXCPR_API int jxcpr_solver_bilu_apply(jxcpr_solver *solver, const double *f, dou
  * path) on internal vectors, asynchronously on the solver's stream (no reference counterpart): the
  * kernel a roofline measurement times with events on that stream. */
 JXCPR_API int jxcpr_solver_stage2_native(jxcpr_solver *solver, int sweeps);
+
+/* Host only (no device work): the stage-2 sweep order of the fast path for a block pattern (no
+ * reference counterpart; it reorders jxf_ParBSRHGSRelax's natural sweep, jxfpamg-0220/csrc/amg/
+ * par_relax_bsr.c:193-573).  Chunks of `chunk` (4, 8 or 16) consecutive block rows, greedily coloured
+ * in natural order so that no two coupled chunks share a colour; order = the stored rows colour by
+ * colour, chunk by chunk, rows ascending, each chunk padded to `chunk` and each colour to a multiple of
+ * 32 entries with -1; segments = the colours' offsets into order (colours + 1 values).  Returns the
+ * length of order (filled when capacity suffices; segments when seg_capacity suffices), or minus a
+ * status code. */
+JXCPR_API int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int chunk, int *order, int capacity,
+                                       int *segments, int seg_capacity);
 
 /* ---- fast path (smoother_order 1) inspection: no reference counterpart ---------------------
  * level_info: smoother (1 multicolour GS, 2 l1-Jacobi, 3 Chebyshev-3; 0 exact path), storage

@@ -206,15 +206,17 @@ void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s) {
 struct ScheduleJob {
     std::vector<int> perm[2], gptr[2], rank[2];
     bool both = false;
+    std::vector<int> chunk_order, chunk_seg;
 };
 
-static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, cudaStream_t s) {
+// chunk > 0: also the stage-2 chunk order of the pattern (level 0 of the fast path)
+static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, int chunk, cudaStream_t s) {
     const int n = L.A.nrows;
     std::vector<int> ia(n + 1), ja(L.A.nnz > 0 ? L.A.nnz : 1);
     L.A.ia.download(ia.data(), n + 1, s);
     L.A.ja.download(ja.data(), L.A.nnz, s);
     JX_CUDA(cudaStreamSynchronize(s));
-    return std::async(std::launch::async, [n, order, ia = std::move(ia), ja = std::move(ja)]() {
+    return std::async(std::launch::async, [n, order, chunk, ia = std::move(ia), ja = std::move(ja)]() {
         ScheduleJob J;
         build_schedule_host(n, ia.data(), ja.data(), order, true, J.perm[0], J.gptr[0], J.rank[0]);
         if (order == ORDER_EXACT) {
@@ -222,6 +224,7 @@ static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, cu
             build_schedule_host(n, ia.data(), ja.data(), order, false, J.perm[1], J.gptr[1], J.rank[1]);
         }
         // multicolour: the backward sweep visits the same classes in reverse order (fwd schedule, reversed)
+        if (chunk > 0) build_chunk_order_host(n, ia.data(), ja.data(), chunk, J.chunk_order, J.chunk_seg);
         return J;
     });
 }
@@ -229,6 +232,8 @@ static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, cu
 static void finish_level_schedules(AmgLevel &L, ScheduleJob J, cudaStream_t s) {
     upload_schedule(J.perm[0], J.gptr[0], J.rank[0], L.fwd, s);
     if (J.both) upload_schedule(J.perm[1], J.gptr[1], J.rank[1], L.bwd, s);
+    L.chunk_order = std::move(J.chunk_order);
+    L.chunk_seg = std::move(J.chunk_seg);
 }
 
 static double now_ms() {
@@ -269,7 +274,9 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         AmgLevel &L = *H.levels[level];
         const int n = L.A.nrows;
         jobs.emplace_back();
-        if (wants_schedule(L, level == 0)) jobs.back() = start_level_schedules(L, H.prm.order, s);
+        if (wants_schedule(L, level == 0))
+            jobs.back() = start_level_schedules(
+                L, H.prm.order, (level == 0 && H.prm.order != ORDER_EXACT) ? H.prm.stage2_chunk : 0, s);
         DevPattern S;
         if (H.prm.theta_for_level) {
             L.theta = H.prm.theta_for_level(level, L.A.view());
@@ -338,7 +345,7 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
     }
     const int n0 = H.levels[0]->A.nrows;
     H.work.alloc((size_t)(n0 > 0 ? n0 : 1) * 2);
-    H.err.alloc(1);
+    H.err.alloc(4);  // [0] error flag, [2..3] grid barrier of the cooperative sweeps
     H.err.zero(s);
     H.log.mark("vectors", s);
     coarse_setup(H, s);

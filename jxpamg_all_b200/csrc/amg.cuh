@@ -53,6 +53,7 @@ struct AmgLevel {
     DeviceCsr R;          // P^T, rows listing fine points ascending
     std::vector<int> cf;  // host copy of the C/F splitting (tests)
     Schedule fwd, bwd;    // Gauss-Seidel schedules
+    std::vector<int> chunk_order, chunk_seg;  // level 0 of the fast path: stage-2 chunk order (host)
     DevBuf<double> f, u;  // right-hand side and iterate of this level
 };
 
@@ -66,6 +67,7 @@ struct AmgParams {
     int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
     double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows go straight to l1-Jacobi
     int rs_range_rows = 0;  // > 0: the coarsening's first pass runs on row ranges of this size (host threads)
+    int stage2_chunk = 0;   // > 0 (fast path): level 0 also gets the stage-2 chunk order (build_chunk_order_host)
     // Optional per-level strength thresholds: called before level l is
     // coarsened with its operator; returns the threshold to use (learned model).
     std::function<double(int level, const CsrView<double> &A)> theta_for_level;
@@ -87,7 +89,7 @@ struct Amg {
     int nc = 0;
     DevBuf<double> Ufac, Lt, Ainv;
     DevBuf<double> work;  // residual of the finest level
-    DevBuf<int> err;      // device error flag of the smoothers
+    DevBuf<int> err;      // [0] device error flag of the smoothers, [2..3] their grid barrier
     int num_levels() const { return (int)levels.size(); }
 };
 
@@ -109,6 +111,10 @@ void build_schedule_host(int n, const int *ia, const int *ja, int order, bool fo
                          std::vector<int> &group_ptr, std::vector<int> &rank);
 void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr, const std::vector<int> &rank,
                      Schedule &S, cudaStream_t s);
+// Stage-2 order of the throughput path: chunks of `chunk` (a divisor of 32) consecutive rows, coloured;
+// order = stored rows (colour by colour, chunk by chunk, -1 padding), seg = colour segment offsets.
+void build_chunk_order_host(int n, const int *ia, const int *ja, int chunk, std::vector<int> &order,
+                            std::vector<int> &seg);
 
 // amg.cu
 void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s);
@@ -122,6 +128,8 @@ void permute_rows_csr(const CsrView<double> &A, const int *perm, DeviceCsr &P, c
 void permute_rows_bsr(const BsrView<double> &A, const int *perm, DeviceBsr &P, cudaStream_t s);
 
 // smoother.cu
+// err: the hierarchy's 4-int device buffer (err[0] the error flag; err[2..3] the grid barrier of the
+// cooperative sweeps, reset by each launch on `s`), so solvers on concurrent streams do not share it.
 // One Gauss-Seidel sweep of A u = f along `sch` (relax_weight = omega = 1,
 // rows with a zero diagonal skipped): jxf_PAMGRelax6's forward or backward
 // pass.

@@ -60,6 +60,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"bf16_level", &p.bf16_level},
                {"fast_smoother", &p.fast_smoother},
                {"stage2_lanes", &p.stage2_lanes},
+               {"stage2_chunk", &p.stage2_chunk},
                {"learned_fallback", &p.learned_fallback},
                {"record_features", &p.record_features},
                {"flexible", &p.flexible},
@@ -73,6 +74,10 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"bilu_upper_iters", &p.bilu_upper_iters}};
     if (!key) return JXCPR_ERROR_ARG;
     if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
+    if (!strcmp(key, "stage2_chunk") && v != 0 && v != 4 && v != 8 && v != 16) {
+        set_error("stage2_chunk must be 0, 4, 8 or 16 (got %d)", v);
+        return JXCPR_ERROR_ARG;
+    }
     for (auto &e : tab)
         if (!strcmp(key, e.k)) {
             *e.f = v;
@@ -95,7 +100,8 @@ int set_real_param(SolverParams &p, const char *key, double v) {
                {"strong_threshold", &p.strong_threshold},
                {"strong_threshold_coarse", &p.strong_threshold_coarse},
                {"cheb_lower", &p.cheb_lower},
-               {"cheb_upper", &p.cheb_upper}};
+               {"cheb_upper", &p.cheb_upper},
+               {"jacobi_mean_row", &p.jacobi_mean_row}};
     if (!key) return JXCPR_ERROR_ARG;
     for (auto &e : tab)
         if (!strcmp(key, e.k)) {
@@ -411,6 +417,24 @@ int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int devic
         JX_CUDA(cudaStreamSynchronize(st));
         return JXCPR_SUCCESS;
     });
+}
+
+int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int chunk, int *order, int capacity,
+                             int *segments, int seg_capacity) {
+    if (nb < 0 || (nb > 0 && (!ia || !ja)) || (chunk != 4 && chunk != 8 && chunk != 16) || capacity < 0) {
+        set_error("stage2_chunk_order: bad arguments");
+        return -JXCPR_ERROR_ARG;
+    }
+    try {
+        std::vector<int> ord, seg;
+        build_chunk_order_host(nb, ia, ja, chunk, ord, seg);
+        if (order && (size_t)capacity >= ord.size()) std::copy(ord.begin(), ord.end(), order);
+        if (segments && (size_t)seg_capacity >= seg.size()) std::copy(seg.begin(), seg.end(), segments);
+        return (int)ord.size();
+    } catch (...) {
+        set_error("stage2_chunk_order: host allocation failed");
+        return -JXCPR_ERROR_MEMORY;
+    }
 }
 
 }  // extern "C"

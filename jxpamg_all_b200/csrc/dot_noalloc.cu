@@ -5,10 +5,18 @@
 // device, or a time-critical loop that forbids allocator calls on its critical
 // path (cudaMalloc can synchronise the device and stall every stream).  jxcpr_dot_dev allocates its per-CTA partial sums on
 // every call, which these callers cannot accept.  This variant keeps the
-// partial sums and the result in a fixed array that the library reserves when
-// it is loaded: JXCPR_NOALLOC_DOT_MAX_PARTIALS doubles of partial sums (one per
-// JXCPR_NOALLOC_DOT_CHUNK elements) plus one result slot, 512 KB per GPU that
-// loads the library, held until the process exits.
+// partial sums and the result in a fixed file-scope device array:
+// JXCPR_NOALLOC_DOT_MAX_PARTIALS doubles of partial sums (one per
+// JXCPR_NOALLOC_DOT_CHUNK elements) plus one result slot, 512 KB per GPU,
+// held until the process exits.
+//
+// When the array comes into being: the library is built one module per source
+// file and CUDA loads modules lazily, so this file's module -- and with it the
+// array -- is loaded on a device by the first call on that device (the
+// cudaGetSymbolAddress below).  That load takes device memory like any other
+// module load.  A caller whose pool will later reserve the whole device makes
+// one warm-up call (n = 0 is enough) on each device before the pool does;
+// every later call allocates nothing.
 //
 // The array is shared by every call on a device and keeps the last call's
 // contents.  Each call writes every partial it reads and overwrites the
@@ -16,8 +24,9 @@
 // GPU (concurrent streams) race on the array and must be serialised by the
 // caller.  Host code cannot use the array's name as a device address: on the
 // first call on each device (that device current) the library resolves the
-// address with cudaGetSymbolAddress and caches it, so that first call should
-// come before any stream capture.
+// address with cudaGetSymbolAddress and caches it.  Every call copies the
+// result to the host and synchronises its stream, so it must not be called
+// while that stream is being captured into a CUDA graph.
 #include <mutex>
 
 #include "common.cuh"
@@ -33,6 +42,8 @@ constexpr int kThreads = 256;
 static __device__ __align__(256) double g_dot_scratch[kMaxPartials + 32];
 
 std::mutex g_mu;
+// Cached per device; a cudaDeviceReset by the application would unload the module and leave the
+// cached address stale (the library assumes the context lives as long as the process).
 double *g_addr[64] = {nullptr};
 
 // Device address of g_dot_scratch for the current device (resolved once).

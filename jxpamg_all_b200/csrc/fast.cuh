@@ -24,8 +24,9 @@
 // colour class over a colour-contiguous row copy), l1-Jacobi (dense levels),
 // or a degree-3 polynomial (Chebyshev) smoother u += p(D^-1 A) D^-1 (f - A u)
 // with per-level coefficients (given intervals, or predicted by the learned
-// model).  Stage 2 is the reference's hybrid block GS (w, omega) in colour
-// order, V lanes per block row.
+// model).  Stage 2 is the reference's hybrid block GS (w, omega) in chunk order
+// (chunks of consecutive block rows visited in natural order, the chunks
+// coloured; fk::hgs_chunk), or in the level-0 colour order (stage2_chunk 0).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -56,6 +57,7 @@ struct LevelMat {
     int E = 1;
     int kind = VAL_F64;
     int sell = 0;
+    int chunk = 0;  // sliced ELL in chunk order (stage 2, fk::hgs_chunk): rows per chunk
     int lanes = 1;
     int nstored = 0;
     const int *perm = nullptr;  // CSR: not owned
@@ -92,6 +94,8 @@ struct FastOptions {
     int smoother = 0;       // 0 colour GS / l1-Jacobi, 1 Chebyshev-3 on the l1-Jacobi levels, 2 on every level
     double cheb_lower = 0.3, cheb_upper = 1.1;  // interval [lower, upper] * lambda_max(D^-1 A)
     int stage2_lanes = 4;      // CSR stage 2 (small systems): lanes per block row
+    int stage2_chunk = 8;      // stage 2 in chunk order (chunks of this many consecutive block rows; 0: the
+                               // level-0 colour order)
     int sell_min_rows = 16384; // without autotuning: sliced ELL for operators with at least this many rows ...
     double sell_max_mean = 40; // ... and at most this mean row length
     int graphs = 1;            // replay each preconditioner application as one captured CUDA graph

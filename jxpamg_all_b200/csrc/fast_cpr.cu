@@ -246,6 +246,51 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
     JX_CUDA(cudaStreamSynchronize(s));
 }
 
+// Stage-2 block matrix in chunk order (fk::hgs_chunk): stored rows = `order` (chunks of `chunk`
+// consecutive rows, -1 padding, colour segments `seg` on slice boundaries), sliced ELL without the
+// length sort, so that every chunk keeps its rows in order at lanes 0..chunk-1 of its slice part.
+void build_chunk_mat(int n, long long nnz, int E, const int *ia, const int *ja, const double *a, int kind,
+                     const std::vector<int> &order, const std::vector<int> &seg, int chunk, LevelMat &M,
+                     cudaStream_t s) {
+    M.n = n;
+    M.m = n;
+    M.nnz = nnz;
+    M.E = E;
+    M.kind = kind;
+    M.sell = 1;
+    M.chunk = chunk;
+    M.seg = seg;
+    M.nstored = (int)order.size();
+    std::vector<int> ia_h(n + 1);
+    JX_CUDA(cudaMemcpyAsync(ia_h.data(), ia, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    const size_t ns = order.size() / 32;
+    std::vector<long long> sp(ns + 1, 0);
+    for (size_t sl = 0; sl < ns; ++sl) {
+        int wd = 0;
+        for (int q = 0; q < 32; ++q) {
+            const int i = order[sl * 32 + q];
+            if (i >= 0) wd = std::max(wd, ia_h[i + 1] - ia_h[i]);
+        }
+        sp[sl + 1] = sp[sl] + 32LL * wd;
+    }
+    M.rows.alloc(order.size() + 1);
+    M.rows.upload(order.data(), order.size(), s);
+    M.sp.alloc(sp.size());
+    M.sp.upload(sp.data(), sp.size(), s);
+    const long long slots = sp.back();
+    M.ja.alloc(slots > 0 ? slots : 1);
+    const long long nv = (slots > 0 ? slots : 1) * E;
+    if (kind == VAL_F64) {
+        M.a64.alloc(nv);
+        sell_fill_launch<double>(M, ia, ja, a, M.a64.get(), nullptr, s);
+    } else {
+        M.a32.alloc(nv);
+        sell_fill_launch<float>(M, ia, ja, a, M.a32.get(), nullptr, s);
+    }
+    JX_CUDA(cudaStreamSynchronize(s));
+}
+
 bool use_sell(const FastOptions &o, int n, long long nnz) {
     return n >= o.sell_min_rows && n > 0 && (double)nnz / n <= o.sell_max_mean;
 }
@@ -647,6 +692,23 @@ struct FastCpr final : FastCprBase {
     template <typename TV, typename TXV, typename TAC>
     void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, TXV *vtp, TAC w,
                        TAC om, int plain, fk::SweepOrder so, cudaStream_t s) {
+        if (M.chunk) {
+            const int grid = div_up(r1 - r0, kThreads);
+#define JX_HGS_CHUNK(BSV, CHV)                                                                              \
+    launch_dep(fk::hgs_chunk<BSV, CHV, TV, TAC, TXV>, dim3(grid), dim3(kThreads), s, r0, r1, M.sp.get(),     \
+               M.ja.get(), a, M.rows.get(), r, z, vtp, w, om, plain, so)
+            if (bs == 2) {
+                if (M.chunk == 4) JX_HGS_CHUNK(2, 4);
+                else if (M.chunk == 16) JX_HGS_CHUNK(2, 16);
+                else JX_HGS_CHUNK(2, 8);
+            } else {
+                if (M.chunk == 4) JX_HGS_CHUNK(3, 4);
+                else if (M.chunk == 16) JX_HGS_CHUNK(3, 16);
+                else JX_HGS_CHUNK(3, 8);
+            }
+#undef JX_HGS_CHUNK
+            return;
+        }
         if (M.sell) {
             const int grid = div_up(r1 - r0, kThreads);
             if (bs == 2)
@@ -949,7 +1011,23 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
         F->vt32.alloc(nv);
         F->vt32.zero(s);
     }
-    if (H0.fwd.ngroups > 0 && A.nb > 0) {
+    if (opt.stage2_chunk > 0 && !H0.chunk_order.empty() && A.nb > 0) {
+        // chunk order: no layout timing (one layout)
+        const std::vector<int> &ord = H0.chunk_order;
+        const std::vector<int> &sg = H0.chunk_seg;
+        std::vector<int> cls(A.nb, 0);
+        for (size_t c = 0; c + 1 < sg.size(); ++c)
+            for (int t = sg[c]; t < sg[c + 1]; ++t)
+                if (ord[t] >= 0) cls[ord[t]] = (int)c;
+        F->st2_cls.alloc(A.nb);
+        F->st2_cls.upload(cls.data(), A.nb, s);
+        const int kind = (fp64 || opt.precision == 3) ? VAL_F64 : VAL_F32;
+        build_chunk_mat(A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, ord, sg, opt.stage2_chunk, F->st2, s);
+        char line[200];
+        snprintf(line, sizeof line, "stage2 rows %d blocks/row %.1f layout chunk%d colours %d", A.nb,
+                 (double)A.nnzb / A.nb, opt.stage2_chunk, (int)sg.size() - 1);
+        F->tune_log.emplace_back(line);
+    } else if (H0.fwd.ngroups > 0 && A.nb > 0) {
         std::vector<int> order = download_ints(H0.fwd.perm.get(), A.nb, s);
         {
             const std::vector<int> &g = H0.fwd.h_group_ptr;

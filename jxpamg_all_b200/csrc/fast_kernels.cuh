@@ -444,6 +444,133 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
     }
 }
 
+// Stage 2 in chunk order (the throughput path's default): block rows are grouped in chunks of CH
+// consecutive rows (natural numbering, chunk = row / CH), the chunks coloured so that no two chunks
+// of one colour are coupled; a sweep visits the colours in turn and each chunk's rows in natural
+// order, i.e. the block update of hgs_color in that sequential order.  Storage: sliced ELL with each
+// colour a run of whole chunks, CH-aligned inside the 32-row slices (lane p of a chunk holds its row
+// p; padding rows -1), rows not sorted by length.
+//   Phase 1, every row at once: the entries outside the row's chunk (earlier colours: current value
+//   and saved start value; later colours: the start value), and the in-chunk entries of higher
+//   index (not updated yet: start value).  Of an in-chunk entry of lower index j only the start-value
+//   term -(1 - omega) A_ij vt_j is added; the first such entry is kept in registers.
+//   Phase 2, CH steps: at step r lane r of every chunk solves its block and writes x; the new value
+//   is shuffled to the chunk's other lanes, whose rows coupled to it add A_ij x_j (the kept entry, or
+//   a re-scan of the row for any further in-chunk lower entry).
+template <int BS, int CH, typename TV, typename TA, typename TXV>
+__global__ void __launch_bounds__(256) hgs_chunk(int r0, int r1, const long long *__restrict__ sp,
+                                                 const int *__restrict__ col, const TV *__restrict__ a,
+                                                 const int *__restrict__ rows, const TXV *__restrict__ b,
+                                                 TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
+    static_assert(32 % CH == 0, "chunks tile the 32-row slices");
+    grid_dep_wait();
+    const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int p = lane % CH;
+    const int i = t < r1 ? __ldg(rows + t) : -1;
+    const bool live = i >= 0;
+    const int cbase = i - p;  // first row of the chunk (row i sits at lane p of its chunk)
+    const TA omo = (TA)1 - omega;
+    TA rhs[BS], xv[BS], D[BS * BS], acc[BS], K[BS * BS];
+    int kq = -1;            // chunk position of the kept in-chunk lower entry
+    unsigned lowmask = 0u;  // chunk positions of every in-chunk lower entry
+    long long o = 0;
+    int wd = 0;
+#pragma unroll
+    for (int q = 0; q < BS; ++q) acc[q] = 0;
+#pragma unroll
+    for (int q = 0; q < BS * BS; ++q) K[q] = 0;
+    if (live) {
+        const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
+        wd = (int)((b1 - b0) >> 5);
+        o = b0 + (t & 31);
+#pragma unroll
+        for (int q = 0; q < BS; ++q) {
+            rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
+            xv[q] = (TA)x[(long long)i * BS + q];
+        }
+        load_block<BS, TV, TA>(a, o, D);
+        for (int k = 1; k < wd; ++k) {
+            const long long pk = o + (long long)k * 32;
+            const int j = __ldg(col + pk);
+            TA B[BS * BS], c[BS];
+            load_block<BS, TV, TA>(a, pk, B);
+            const int dq = j - cbase;
+            if (dq >= 0 && dq < CH) {
+                if (dq > p) {  // later in the chunk: its start value
+#pragma unroll
+                    for (int m = 0; m < BS; ++m) {
+                        const TA xj = (TA)x[(long long)j * BS + m];
+                        c[m] = plain ? xj : xj - omo * xj;
+                    }
+                } else {  // earlier in the chunk: -(1 - omega) A vt_j now, A x_j(new) in phase 2
+                    lowmask |= 1u << dq;
+                    if (kq < 0) {
+                        kq = dq;
+#pragma unroll
+                        for (int q = 0; q < BS * BS; ++q) K[q] = B[q];
+                    }
+#pragma unroll
+                    for (int m = 0; m < BS; ++m) c[m] = plain ? (TA)0 : -omo * (TA)x[(long long)j * BS + m];
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < BS; ++m) {
+                    const TA xj = (TA)x[(long long)j * BS + m];
+                    c[m] = plain ? xj : xj - omo * start_value<TA, TXV>(x, vt, (long long)j * BS + m, j, so);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < BS; ++q)
+#pragma unroll
+                for (int m = 0; m < BS; ++m) acc[q] += B[q * BS + m] * c[m];
+        }
+    }
+    __syncwarp();  // every lane has read its chunk's start values before any lane writes
+    const TA prod = (TA)1 - w * omega;
+    TA xn[BS];
+#pragma unroll
+    for (int q = 0; q < BS; ++q) xn[q] = 0;
+#pragma unroll 1
+    for (int r = 0; r < CH; ++r) {
+        if (live && p == r) {
+            TA r2[BS], out[BS];
+#pragma unroll
+            for (int q = 0; q < BS; ++q) r2[q] = (plain ? (TA)1 : omega) * rhs[q] - acc[q];
+            block_solve<BS, TA>(D, r2, out);
+#pragma unroll
+            for (int q = 0; q < BS; ++q) {
+                const TXV nv = plain ? (TXV)out[q] : (TXV)(prod * xv[q] + w * out[q]);
+                if (!plain && so.save) vt[(long long)i * BS + q] = (TXV)xv[q];
+                x[(long long)i * BS + q] = nv;
+                xn[q] = (TA)nv;
+            }
+        }
+        TA bx[BS];
+#pragma unroll
+        for (int q = 0; q < BS; ++q) bx[q] = __shfl_sync(0xffffffffu, xn[q], (lane & ~(CH - 1)) | r);
+        if (live && p > r && ((lowmask >> r) & 1u)) {
+            if (r == kq) {
+#pragma unroll
+                for (int q = 0; q < BS; ++q)
+#pragma unroll
+                    for (int m = 0; m < BS; ++m) acc[q] += K[q * BS + m] * bx[m];
+            } else {
+                for (int k = 1; k < wd; ++k) {
+                    const long long pk = o + (long long)k * 32;
+                    if (__ldg(col + pk) != cbase + r) continue;
+                    TA B[BS * BS];
+                    load_block<BS, TV, TA>(a, pk, B);
+#pragma unroll
+                    for (int q = 0; q < BS; ++q)
+#pragma unroll
+                        for (int m = 0; m < BS; ++m) acc[q] += B[q * BS + m] * bx[m];
+                }
+            }
+        }
+    }
+}
+
 // ---- sliced-ELL fill ----------------------------------------------------------
 template <typename TV>
 __device__ __forceinline__ TV cvt_val(double v, double sc);

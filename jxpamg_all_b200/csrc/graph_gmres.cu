@@ -116,7 +116,11 @@ __global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const
         s.normdown = rn;
         norms[0] = rn;
     }
+    // stall rule: a full cycle that reduced the true residual by less than stall^k
+    const int ci = s.iter - s.iter0;
+    const bool stalled = P.stall > 0.0 && s.cycles > 1 && ci >= P.k && rn > s.r_norm * pow(P.stall, (double)ci);
     s.r_norm = rn;
+    s.iter0 = s.iter;
     if (!done) {
         if (rn == 0.0 || (rn <= s.epsilon && s.iter >= P.min_iter)) {
             s.converged = 1;
@@ -124,6 +128,9 @@ __global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const
         } else if (s.est_conv && !P.check_restarted) {
             done = true;  // estimate below tolerance, true residual not, no restart allowed
         } else if (s.conv_fail || s.iter >= P.max_iter || s.cycles > P.max_iter + 1) {
+            done = true;
+        } else if (stalled) {
+            s.stalled = 1;
             done = true;
         }
     }
@@ -388,7 +395,7 @@ __global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, double 
 __global__ void summary_kernel(const GgState *st, const int *kerr, const int *aerr, double *out) {
     const GgState &s = *st;
     out[0] = s.iter;
-    out[1] = s.converged;
+    out[1] = s.converged ? 1.0 : (s.stalled ? -1.0 : 0.0);
     out[2] = s.rel;
     out[3] = s.status;
     out[4] = (double)s.t_start;
@@ -520,6 +527,7 @@ void GraphGmres::prepare(Solver &S) {
     P.tol = prm.tol;
     P.a_tol = prm.a_tol;
     P.convfac = prm.convfac_threshold;
+    P.stall = prm.stall_factor;
     JX_CUDA(cudaStreamSynchronize(s));
     reset_graph();
 }
@@ -527,7 +535,7 @@ void GraphGmres::prepare(Solver &S) {
 bool GraphGmres::matches(const SolverParams &prm) const {
     return prm.k_dim == P.k && prm.max_iter == P.max_iter && prm.min_iter == P.min_iter &&
            prm.is_check_restarted == P.check_restarted && prm.tol == P.tol && prm.a_tol == P.a_tol &&
-           prm.convfac_threshold == P.convfac;
+           prm.convfac_threshold == P.convfac && prm.stall_factor == P.stall;
 }
 
 void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
@@ -635,7 +643,8 @@ unsigned long long GraphGmres::kernels_run(int iterations, int cycles) const {
 GmresResult GraphGmres::result_from(const double *sm, cudaStream_t s, bool with_norms) {
     GmresResult res;
     res.iterations = (int)sm[0];
-    res.converged = (int)sm[1];
+    res.converged = sm[1] > 0.5 ? 1 : 0;
+    res.stalled = sm[1] < -0.5 ? 1 : 0;
     res.rel_residual = sm[2];
     res.status = sm[3] != 0.0 ? JXCPR_ERROR_GENERIC : 0;
     if (with_norms) {

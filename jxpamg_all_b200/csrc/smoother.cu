@@ -309,16 +309,10 @@ namespace {
 constexpr int kSweepThreads = 256;
 constexpr int kSmallRows = 12288;
 
-struct BarrierPool {
-    GridBarrier *bar[64] = {nullptr};
-    GridBarrier *get() {
-        int dev = 0;
-        JX_CUDA(cudaGetDevice(&dev));
-        if (!bar[dev]) JX_CUDA(cudaMalloc(&bar[dev], sizeof(GridBarrier)));
-        return bar[dev];
-    }
-};
-BarrierPool g_bars;
+// The grid barrier of a cooperative sweep lives beside the hierarchy's error flag (err[0]) in the
+// same per-hierarchy allocation (err[2..3]), so exact-order sweeps of different solvers on
+// concurrent streams never share a barrier.
+GridBarrier *barrier_of(int *err) { return reinterpret_cast<GridBarrier *>(err + 2); }
 
 template <typename K>
 int coop_grid(K kernel) {
@@ -345,7 +339,7 @@ void gs_sweep(const CsrView<double> &A, const Schedule &sch, const double *f, do
     static int grid = 0;
     if (!grid) grid = coop_grid(gs_sweep_grid_kernel);
     const int blocks = std::min(grid, div_up(sch.max_group, kSweepThreads));
-    GridBarrier *bar = g_bars.get();
+    GridBarrier *bar = barrier_of(err);
     JX_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s));
     int ng = sch.ngroups;
     const int *gp = sch.group_ptr.get(), *pm = sch.perm.get();
@@ -380,7 +374,7 @@ void hgs_pass(const BsrView<double> &A, const Schedule &sch, const double *b, do
     if (!grid3) grid3 = coop_grid(hgs_sweep_grid_kernel<3>);
     const int grid = A.bs == 2 ? grid2 : grid3;
     const int blocks = std::min(grid, div_up(sch.max_group, kSweepThreads));
-    GridBarrier *bar = g_bars.get();
+    GridBarrier *bar = barrier_of(err);
     JX_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBarrier), s));
     int ng = sch.ngroups;
     const int *gp = sch.group_ptr.get(), *pm = sch.perm.get();

@@ -33,6 +33,8 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     amg.prm.order = prm.smoother_order;
     amg.prm.coarse_exact = fast_path ? 0 : prm.coarse_exact;
     amg.prm.max_colors = prm.max_colors;
+    amg.prm.jacobi_mean_row = prm.jacobi_mean_row;
+    amg.prm.stage2_chunk = fast_path ? prm.stage2_chunk : 0;
     amg.prm.rs_range_rows = fast_path ? prm.rs_range_rows : 0;
     amg.prm.strong_threshold = prm.strong_threshold;
     amg.prm.theta_for_level = nullptr;
@@ -71,6 +73,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         opt.cheb_lower = prm.cheb_lower;
         opt.cheb_upper = prm.cheb_upper;
         opt.stage2_lanes = prm.stage2_lanes;
+        opt.stage2_chunk = prm.stage2_chunk;
         opt.autotune = prm.autotune;
         opt.graphs = prm.graphs;
         opt.dep_launch = prm.dep_launch;
@@ -406,6 +409,7 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
     int converged = 0;
     while (iter < prm.max_iter) {
         rs[0] = r_norm;
+        const double cycle_r0 = r_norm;
         if (r_norm == 0.0) {
             res.iterations = iter;
             res.converged = 1;
@@ -524,6 +528,12 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
             }
         }
         if (iter > 1 && conv_factor > prm.convfac_threshold) break;
+        // stall rule: a full cycle that reduced the residual by less than stall_factor^k
+        if (prm.stall_factor > 0.0 && i == k_dim && iter < prm.max_iter &&
+            r_norm > cycle_r0 * pow(prm.stall_factor, (double)k_dim)) {
+            res.stalled = 1;
+            break;
+        }
         for (int j = i; j > 0; --j) {
             rs[j - 1] = -sn[j - 1] * rs[j];
             rs[j] = c[j - 1] * rs[j];
@@ -643,9 +653,15 @@ void Solver::learned_probe(cudaStream_t s) {
 // the learned one, on the already decoupled matrix.
 void Solver::rebuild_plain(cudaStream_t s) {
     const int fs = cpr.prm.fast_smoother;
+    const double ff = cpr.factor_fast, fp = cpr.factor_plain, pb0 = cpr.probe_bytes[0], pb1 = cpr.probe_bytes[1];
     cpr.prm.fast_smoother = 0;
     cpr.ready = false;
     cpr.setup(A.view(), s);
+    // the probe's figures stay reported (learned_status): they are why the plain method runs now
+    cpr.factor_fast = ff;
+    cpr.factor_plain = fp;
+    cpr.probe_bytes[0] = pb0;
+    cpr.probe_bytes[1] = pb1;
     cpr.prm.fast_smoother = fs;
     cpr.learned_used = 0;
     cpr.probe_pending = false;
@@ -653,21 +669,17 @@ void Solver::rebuild_plain(cudaStream_t s) {
     if (ggmres) ggmres->reset_graph();
 }
 
-// Learned settings are kept by a short probe at setup; if the full solve then
-// stalls -- no convergence within a budget of three times the iterations the
-// probe's residual reduction predicts (at least that plus one restart cycle)
-// -- the plain preconditioner (default thresholds, plain smoothers) is built in
-// their place and GMRES continues from the current iterate with the remaining
-// iterations.
+// Learned settings are kept by a short probe at setup.  The full solve then runs with a stall
+// rule: a restart cycle of k iterations that reduces the residual by less than a third (in
+// logarithm) of what the probe's per-iteration factor predicts ends it early.  The plain
+// preconditioner (default thresholds, plain smoothers) is then built in place of the learned one
+// and GMRES continues from the current iterate with the remaining iterations.
 GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
     const bool guard = cpr.fast && cpr.learned_used && prm.learned_fallback && cpr.factor_fast > 0.0 &&
                        cpr.factor_fast < 1.0 && prm.tol > 0.0 && prm.tol < 1.0;
     if (!guard) return solve_once(b_in, x_io, device);
     const SolverParams saved = prm;
-    const double expect = std::ceil(std::log(prm.tol) / std::log(cpr.factor_fast));
-    const double want = std::max(3.0 * expect, expect + prm.k_dim);
-    const int budget = (int)std::min<double>(prm.max_iter, want);
-    prm.max_iter = budget;
+    prm.stall_factor = std::pow(cpr.factor_fast, 1.0 / 3.0);
     GmresResult first;
     try {
         first = solve_once(b_in, x_io, device);
@@ -676,7 +688,7 @@ GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
         throw;
     }
     prm = saved;
-    if (first.converged || first.status || first.iterations < budget || budget >= saved.max_iter) return first;
+    if (!first.stalled || first.status) return first;
     const double ms0 = solve_ms;
     {
         PoolStream scope(stream);

@@ -26,6 +26,9 @@ struct SolverParams {
     double a_tol = 0.0;
     int is_check_restarted = 1;
     double convfac_threshold = 1e4;
+    // Internal (not an option): > 0 ends the solve with `stalled` set when a full restart cycle reduces
+    // the residual by less than stall_factor^k (the learned settings' guard, Solver::solve).
+    double stall_factor = 0.0;
     int print_level = 0;
     int logging = 1;
     // CPR (jxfpamg-0220/csrc/cpr/jxf_cpr.c:151-182, 226-262)
@@ -55,6 +58,7 @@ struct SolverParams {
     int smoother_order = ORDER_EXACT;  // 0 exact order (bit-identical), 1 throughput / mixed path
     int coarse_exact = 1;
     int max_colors = 8;
+    double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows use l1-Jacobi
     // fast path: the coarsening's first pass on row ranges of this many rows, one host thread per
     // range (levels with fewer than twice as many rows, and the exact order always, take one pass)
     int rs_range_rows = 131072;
@@ -74,6 +78,7 @@ struct SolverParams {
     double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
     double cheb_upper = 1.1;
     int stage2_lanes = 4;
+    int stage2_chunk = 8;      // fast path: stage 2 in chunk order (4, 8 or 16 consecutive block rows; 0 colour order)
     int learned_fallback = 1;  // learned mode: keep the plain smoothers when their V-cycle factor is lower
     int record_features = 0;   // fast path: record the per-level features (training data)
 };
@@ -130,6 +135,7 @@ struct CprPrecond {
 struct GmresResult {
     int iterations = 0;
     int converged = 0;
+    int stalled = 0;  // ended by the stall rule (stall_factor)
     double rel_residual = 0.0;
     std::vector<double> norms;
     int status = 0;
@@ -165,13 +171,15 @@ constexpr int kGgMaxK = 64;
 struct GgState {
     int i, m, iter, cycles;
     int converged, done, status, first;
-    int est_conv, conv_fail, cont, pad;
+    int est_conv, conv_fail, cont, stalled;
+    int iter0, pad;  // iterations at the current cycle's start
     double b_norm, r_norm, r_norm0, epsilon, normdown, scale, rel;
     unsigned long long t_start, t_end;  // device global timer (ns) at the solve's start and end
 };
 struct GgParams {
     int k, max_iter, min_iter, check_restarted;
     double tol, a_tol, convfac;
+    double stall;  // SolverParams::stall_factor
 };
 struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
     double *rs, *c, *sn, *h1, *h2, *y, *hh;

@@ -74,6 +74,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_stage2_sweep.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_level_info.argtypes = [P, c_int, P, P, P, P]
     lib.jxcpr_solver_stage2_native.argtypes = [P, c_int]
+    lib.jxcpr_stage2_chunk_order.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]
     lib.jxcpr_solver_bilu_sizes.argtypes = [P, P]
     lib.jxcpr_solver_bilu_factors.argtypes = [P, P, P, P]
     lib.jxcpr_solver_bilu_apply.argtypes = [P, P, P, c_int]

@@ -157,6 +157,27 @@ def ref_bsr_decouple(ia, ja, a, bs, rhs, dtype_code, thermal=False):
     return a2, r2
 
 
+def chunk_colour(ia, ja, chunk):
+    """Colour of each block row's chunk in the throughput path's stage-2 order, and the colour count."""
+    ia, ja = _i32(ia), _i32(ja)
+    nb = len(ia) - 1
+    colour = np.zeros(max(nb, 1), np.int32)
+    nc = orc().orc_chunk_colour(c_int(nb), _p(ia), _p(ja if len(ja) else np.zeros(1, np.int32)), c_int(chunk),
+                                _p(colour))
+    return colour[:nb], int(nc)
+
+
+def hgs_relax_chunked(ia, ja, a, bs, x, b, chunk, w=0.7, omega=0.9):
+    """One stage-2 sweep (the reference's weighted block update) in the chunk order."""
+    nb = len(ia) - 1
+    colour, nc = chunk_colour(ia, ja, chunk)
+    x = _f64(x).copy()
+    keep = (_i32(ia), _i32(ja), _f64(a))
+    orc().orc_hgs_relax_chunked(c_int(nb), c_int(bs), *(_p(v) for v in keep), _p(x), _p(_f64(b)), c_double(w),
+                                c_double(omega), c_int(chunk), _p(colour), c_int(nc))
+    return x
+
+
 # ---- AMG / CPR / GMRES handles ----------------------------------------------------
 class _CprBase:
     """Common accessors for a CPR handle (restatement or reference)."""
@@ -193,7 +214,7 @@ class OracleCPR(_CprBase):
 
     _prefix = "orc_"
 
-    def __init__(self, ia, ja, a, bs, stage2_maxit=3, stage2_type=2):
+    def __init__(self, ia, ja, a, bs, stage2_maxit=3, stage2_type=2, stage2_chunk=0):
         self._lib = orc()
         self._lib.orc_cpr_create.restype = c_void_p
         self.nb, self.bs = len(ia) - 1, bs
@@ -201,6 +222,8 @@ class OracleCPR(_CprBase):
         self.h = self._lib.orc_cpr_create(c_int(self.nb), c_int(bs), *(_p(v) for v in self._keep),
                                           c_int(stage2_maxit))
         self._lib.orc_cpr_set_stage2_type(c_void_p(self.h), c_int(stage2_type))
+        if stage2_chunk:
+            self._lib.orc_cpr_set_stage2_chunk_h(c_void_p(self.h), c_int(stage2_chunk))
 
     def apply(self, r):
         z = np.zeros(self.nb * self.bs)

@@ -37,6 +37,8 @@ typedef struct {
 
 typedef struct {
     int nb, bs, stage2_maxit, stage2_type;
+    int stage2_chunk, ncolour; /* > 0: stage 2 in chunk order (orc_chunk_colour), colour per row */
+    int *colour;
     const int *ia, *ja;
     const double *a;
     double *work; /* stage-2 work vector (nb * bs), zero at setup */
@@ -70,6 +72,10 @@ void orc_hgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a
 void orc_hsgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
                     double *work, double w, double omega);
 void orc_cpr_setup(orc_cpr *C, int nb, int bs, const int *ia, const int *ja, const double *a, int stage2_maxit);
+int orc_chunk_colour(int nb, const int *ia, const int *ja, int chunk, int *colour);
+void orc_hgs_relax_chunked(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                           double w, double omega, int chunk, const int *colour, int ncolour);
+void orc_cpr_set_stage2_chunk(orc_cpr *C, int chunk);
 void orc_cpr_apply(const orc_cpr *C, const double *r, double *z);
 void orc_cpr_free(orc_cpr *C);
 int orc_gmres(int nb, int bs, const int *ia, const int *ja, const double *a, const double *b, double *x, int k_dim,

@@ -44,6 +44,7 @@ void orc_cpr_destroy(void *hv)
 
 /* stage2_type 2: forward HGS sweeps, 3: HSGS (jxf_cpr.c:572-585) */
 void orc_cpr_set_stage2_type(void *hv, int type) { ((orc_cpr_handle *)hv)->cpr.stage2_type = type; }
+void orc_cpr_set_stage2_chunk_h(void *hv, int chunk) { orc_cpr_set_stage2_chunk(&((orc_cpr_handle *)hv)->cpr, chunk); }
 
 void orc_cpr_apply_h(void *hv, const double *r, double *z)
 {

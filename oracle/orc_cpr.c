@@ -146,6 +146,89 @@ void orc_hgs_relax(int nb, int bs, const int *ia, const int *ja, const double *a
     free(vt);
 }
 
+/* Stage-2 chunk order of the throughput path (no reference counterpart; it reorders the natural
+ * sweep of par_relax_bsr.c:193-573 for parallel slack): block rows in chunks of `chunk` consecutive
+ * rows (chunk c = rows [c*chunk, (c+1)*chunk)), chunks coloured greedily in natural order with the
+ * smallest colour that no chunk coupled to it (symmetrised pattern) has; colour[i] gets the colour of
+ * row i's chunk.  Returns the number of colours.  The sweep visits colour 0's chunks, then colour
+ * 1's, ..., chunks ascending, rows ascending inside a chunk. */
+int orc_chunk_colour(int nb, const int *ia, const int *ja, int chunk, int *colour)
+{
+    int nc = (nb + chunk - 1) / chunk, ncol = 0;
+    int *cc = (int *)malloc(sizeof(int) * (nc + 1)), *mark = NULL, nmark = 0;
+    for (int c = 0; c < nc; c++) cc[c] = -1;
+    /* coupling of chunk c: columns of its rows, and rows whose columns fall in it */
+    int *ti = (int *)calloc(nb + 1, sizeof(int)), *tj = (int *)malloc(sizeof(int) * (ia[nb] + 1));
+    for (int k = 0; k < ia[nb]; k++) ti[ja[k] + 1]++;
+    for (int i = 0; i < nb; i++) ti[i + 1] += ti[i];
+    int *pos = (int *)malloc(sizeof(int) * (nb + 1));
+    memcpy(pos, ti, sizeof(int) * nb);
+    for (int i = 0; i < nb; i++)
+        for (int k = ia[i]; k < ia[i + 1]; k++) tj[pos[ja[k]]++] = i;
+    for (int c = 0; c < nc; c++) {
+        /* colours taken by coupled, already coloured chunks */
+        int lo = c * chunk, hi = (c + 1) * chunk < nb ? (c + 1) * chunk : nb;
+        for (int pass = 0; pass < 2; pass++)
+            for (int i = lo; i < hi; i++) {
+                const int *p0 = pass ? tj + ti[i] : ja + ia[i];
+                const int *p1 = pass ? tj + ti[i + 1] : ja + ia[i + 1];
+                for (const int *q = p0; q < p1; q++) {
+                    int d = *q / chunk;
+                    if (d != c && cc[d] >= 0) {
+                        if (cc[d] >= nmark) {
+                            int nm = 2 * cc[d] + 2;
+                            mark = (int *)realloc(mark, sizeof(int) * nm);
+                            for (int t = nmark; t < nm; t++) mark[t] = -1;
+                            nmark = nm;
+                        }
+                        mark[cc[d]] = c;
+                    }
+                }
+            }
+        int col = 0;
+        while (col < nmark && mark[col] == c) col++;
+        cc[c] = col;
+        if (col + 1 > ncol) ncol = col + 1;
+    }
+    for (int i = 0; i < nb; i++) colour[i] = cc[i / chunk];
+    free(cc);
+    free(mark);
+    free(ti);
+    free(tj);
+    free(pos);
+    return ncol;
+}
+
+/* One stage-2 sweep (the jxf_ParBSRHGSRelax update, par_relax_bsr.c:193-573) visiting the block
+ * rows in the chunk order given by colour[] (orc_chunk_colour): x_i <- (1 - w omega) x_i +
+ * w A_ii^-1 (omega b_i + res0 + (1 - omega) res2), res0 = -sum_j A_ij x_j (current values),
+ * res2 = sum_j A_ij vt_j (values at the sweep start). */
+void orc_hgs_relax_chunked(int nb, int bs, const int *ia, const int *ja, const double *a, double *x, const double *b,
+                           double w, double omega, int chunk, const int *colour, int ncolour)
+{
+    const int b2 = bs * bs;
+    double *vt = (double *)malloc(sizeof(double) * (size_t)nb * bs + 8);
+    memcpy(vt, x, sizeof(double) * (size_t)nb * bs);
+    const double prod = 1.0 - w * omega, omo = 1.0 - omega;
+    int nc = (nb + chunk - 1) / chunk;
+    for (int col = 0; col < ncolour; col++)
+        for (int c = 0; c < nc; c++) {
+            if (colour[c * chunk] != col) continue;
+            int hi = (c + 1) * chunk < nb ? (c + 1) * chunk : nb;
+            for (int i = c * chunk; i < hi; i++) {
+                double res0[3] = {0, 0, 0}, res2[3] = {0, 0, 0}, tmp[3], out[3];
+                for (int jj = ia[i] + 1; jj < ia[i + 1]; jj++) {
+                    blk_matvec_stable(-1.0, a + (size_t)jj * b2, x + (size_t)ja[jj] * bs, res0, bs);
+                    blk_matvec_stable(1.0, a + (size_t)jj * b2, vt + (size_t)ja[jj] * bs, res2, bs);
+                }
+                for (int k = 0; k < bs; k++) tmp[k] = omega * b[i * bs + k] + res0[k] + omo * res2[k];
+                blk_inv_matvec(a + (size_t)ia[i] * b2, tmp, out, bs);
+                for (int k = 0; k < bs; k++) x[i * bs + k] = prod * x[i * bs + k] + w * out[k];
+            }
+        }
+    free(vt);
+}
+
 /* jxf_ParBSRHSGSRelax, jxfpamg-0220/csrc/amg/par_relax_bsr.c:579-1062, one
  * rank, one thread: a forward block Gauss-Seidel pass over the rows, then a
  * backward one, both reading the current iterate.  With w = omega = 1 each
@@ -230,14 +313,31 @@ void orc_cpr_apply(const orc_cpr *C, const double *r, double *z)
     orc_prolong(nb, bs, 0, xp, z);
     for (int s = 0; s < C->stage2_maxit; s++) {
         if (C->stage2_type == 3) orc_hsgs_relax(nb, bs, C->ia, C->ja, C->a, z, r, C->work, 0.7, 0.9);
+        else if (C->stage2_chunk > 0)
+            orc_hgs_relax_chunked(nb, bs, C->ia, C->ja, C->a, z, r, 0.7, 0.9, C->stage2_chunk, C->colour,
+                                  C->ncolour);
         else orc_hgs_relax(nb, bs, C->ia, C->ja, C->a, z, r, 0.7, 0.9, 1);
     }
     free(rp);
     free(xp);
 }
 
+void orc_cpr_set_stage2_chunk(orc_cpr *C, int chunk)
+{
+    free(C->colour);
+    C->colour = NULL;
+    C->stage2_chunk = chunk;
+    C->ncolour = 0;
+    if (chunk > 0) {
+        C->colour = (int *)malloc(sizeof(int) * (C->nb + 1));
+        C->ncolour = orc_chunk_colour(C->nb, C->ia, C->ja, chunk, C->colour);
+    }
+}
+
 void orc_cpr_free(orc_cpr *C)
 {
+    free(C->colour);
+    C->colour = NULL;
     free(C->work);
     C->work = NULL;
     orc_amg_free(&C->amg);

@@ -40,11 +40,14 @@ def test_version_and_error_without_gpu():
 INT_KEYS = ["k_dim", "max_iter", "min_iter", "is_check_restarted", "print_level", "logging", "pressure_index",
             "stage1_maxit", "stage2_maxit", "stage1_solver_type", "stage2_solver_type", "decouple", "thermal",
             "consistent_rhs", "smoother_order", "coarse_exact", "max_colors", "rs_range_rows", "dep_launch",
-            "use_tma_spmv", "precision", "bf16_level", "fast_smoother", "stage2_lanes", "learned_fallback",
+            "use_tma_spmv", "precision", "bf16_level", "fast_smoother", "stage2_lanes", "stage2_chunk", "learned_fallback",
             "record_features", "flexible", "autotune", "graphs", "orthog", "graph_gmres", "bilu_sweeps",
             "bilu_ir_iters", "bilu_lower_iters", "bilu_upper_iters"]
 REAL_KEYS = ["tol", "a_tol", "threshold", "convfac_threshold", "stage2_relax_weight", "stage2_omega",
-             "strong_threshold", "strong_threshold_coarse", "cheb_lower", "cheb_upper"]
+             "strong_threshold", "strong_threshold_coarse", "cheb_lower", "cheb_upper", "jacobi_mean_row"]
+
+
+VALID_INT = {"stage2_chunk": 8}
 
 
 def test_option_keys_accepted_and_documented():
@@ -60,11 +63,12 @@ def test_option_keys_accepted_and_documented():
     header = open(os.path.join(ROOT, "include", "jxcpr_b200.h")).read()
     try:
         for k in INT_KEYS:
-            assert so.jxcpr_solver_set_int(h, k.encode(), 1) == 0, k
+            assert so.jxcpr_solver_set_int(h, k.encode(), VALID_INT.get(k, 1)) == 0, k
             assert re.search(r"\b%s\b" % k, header), f"{k} not described in jxcpr_b200.h"
         for k in REAL_KEYS:
             assert so.jxcpr_solver_set_real(h, k.encode(), 0.5) == 0, k
             assert re.search(r"\b%s\b" % k, header), f"{k} not described in jxcpr_b200.h"
+        assert so.jxcpr_solver_set_int(h, b"stage2_chunk", 5) == 4  # chunks must tile the 32-row slices
         assert so.jxcpr_solver_set_int(h, b"no_such_key", 1) == 4
         assert so.jxcpr_solver_set_real(h, b"no_such_key", 1.0) == 4
     finally:

@@ -68,7 +68,7 @@ def test_solve_matches_oracle(systems, name, decouple):
     # only the dot products' summation order differs: histories agree to ~1e-9
     assert np.allclose(G.norms(), ref["norms"], rtol=1e-7, atol=0)
     # x agrees with the oracle's solution far below the solver tolerance
-    assert np.linalg.norm(x - ref["x"]) <= 1e-7 * np.linalg.norm(ref["x"])
+    assert np.linalg.norm(x - ref["x"]) <= 1e-8 * np.linalg.norm(ref["x"])
     # true residual of the decoupled system
     res = oracle.bsr_matvec(s.ia, s.ja, a, s.block_size, x, -1.0, b, 1.0)
     assert np.linalg.norm(res) <= 1e-6 * np.linalg.norm(b) * (1 + 1e-9)
@@ -85,13 +85,13 @@ def test_solve_golden(systems):
         x, it, rel, conv = G.solve(s.b)
         assert it == int(g["gmres_iters"])
         assert np.allclose(G.norms(), g["gmres_norms"], rtol=1e-7, atol=0)
-        assert np.linalg.norm(x - g["gmres_x"]) <= 1e-7 * np.linalg.norm(g["gmres_x"])
+        assert np.linalg.norm(x - g["gmres_x"]) <= 1e-8 * np.linalg.norm(g["gmres_x"])
 
 
 def test_multicolor_mode_converges(systems):
     """The throughput mode (multicolour Gauss-Seidel on level 0, l1-Jacobi on dense
     coarse levels) is a different smoother; it must still converge to the
-    tolerance with an iteration count near the reference's."""
+    tolerance with an iteration count within +-10 % of the reference's."""
     s = systems("c0")
     a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, 1)
     O = oracle.OracleCPR(s.ia, s.ja, a, s.block_size)
@@ -99,6 +99,6 @@ def test_multicolor_mode_converges(systems):
     G = build(s, 1, max_iter=300, smoother_order=1, coarse_exact=0)
     x, it, rel, conv = G.solve(s.b)
     assert conv and rel <= 1e-6
-    assert it <= int(1.35 * ref["iters"]) + 1
+    assert abs(it - ref["iters"]) <= 0.10 * ref["iters"]
     res = oracle.bsr_matvec(s.ia, s.ja, a, s.block_size, x, -1.0, b, 1.0)
     assert np.linalg.norm(res) <= 1e-6 * np.linalg.norm(b) * (1 + 1e-9)

@@ -185,15 +185,53 @@ def _greedy_classes(ia, ja, n):
 
 
 @pytest.mark.parametrize("name", ["small", "c0", "tiny3"])
-@pytest.mark.parametrize("opt", [dict(autotune=0), dict(autotune=1)], ids=["heuristic", "tuned"])
-def test_stage2_sweep_matches_colour_ordered_hgs(systems, name, opt):
-    """One FP64 stage-2 sweep of the fast path (colour classes in order, no start-of-sweep copy)
-    against a direct restatement of the weighted block Gauss-Seidel update with vt = the iterate
-    at the sweep start: x_i <- (1 - w om) vt_i + w D_i^-1 (om b_i - sum_j A_ij (x_j - (1 - om) vt_j))."""
+@pytest.mark.parametrize("chunk", [4, 8, 16])
+@pytest.mark.parametrize("weights", [(0.7, 0.9), (1.0, 1.0), (1.0, 0.8)], ids=["ref", "plain", "mixed"])
+def test_stage2_sweep_matches_chunk_ordered_hgs(systems, name, chunk, weights):
+    """One FP64 stage-2 sweep of the fast path in chunk order (the default) against the oracle's
+    restatement of the reference's weighted block update visited in the same order
+    (oracle.hgs_relax_chunked); only the summation order of each row differs."""
     s = systems(name)
     bs = s.block_size
     a_dec, _ = oracle.bsr_decouple(s.ia, s.ja, s.a, bs, s.b, 1)
-    G, *_ = solve(s, precision=0, fast_smoother=0, **opt)
+    w, om = weights
+    G, *_ = solve(s, precision=0, fast_smoother=0, stage2_chunk=chunk, stage2_relax_weight=w, stage2_omega=om)
+    rng = np.random.default_rng(9)
+    r = rng.standard_normal(s.n)
+    z0 = rng.standard_normal(s.n)
+    got = G.stage2_sweep(r, z0)
+    G.close()
+    want = oracle.hgs_relax_chunked(s.ia, s.ja, a_dec, bs, z0, r, chunk, w=w, omega=om)
+    assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("name", ["c0", "tiny3"])
+def test_stage2_sweep_fp32_chunk_order(systems, name):
+    """The mixed path's FP32 stage-2 sweep in chunk order against the FP64 restatement (FP32 rounding)."""
+    s = systems(name)
+    bs = s.block_size
+    a_dec, _ = oracle.bsr_decouple(s.ia, s.ja, s.a, bs, s.b, 1)
+    G, *_ = solve(s, precision=1, fast_smoother=0, flexible=1)
+    rng = np.random.default_rng(10)
+    r = rng.standard_normal(s.n)
+    z0 = rng.standard_normal(s.n)
+    got = G.stage2_sweep(r, z0)
+    G.close()
+    want = oracle.hgs_relax_chunked(s.ia, s.ja, a_dec, bs, z0, r, 8)
+    assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("name", ["small", "c0", "tiny3"])
+@pytest.mark.parametrize("opt", [dict(autotune=0), dict(autotune=1)], ids=["heuristic", "tuned"])
+def test_stage2_sweep_matches_colour_ordered_hgs(systems, name, opt):
+    """One FP64 stage-2 sweep of the fast path in the level-0 colour order (stage2_chunk 0: colour
+    classes in order, no start-of-sweep copy) against a direct restatement of the weighted block
+    Gauss-Seidel update with vt = the iterate at the sweep start:
+    x_i <- (1 - w om) vt_i + w D_i^-1 (om b_i - sum_j A_ij (x_j - (1 - om) vt_j))."""
+    s = systems(name)
+    bs = s.block_size
+    a_dec, _ = oracle.bsr_decouple(s.ia, s.ja, s.a, bs, s.b, 1)
+    G, *_ = solve(s, precision=0, fast_smoother=0, stage2_chunk=0, **opt)
     rng = np.random.default_rng(8)
     r = rng.standard_normal(s.n)
     z0 = rng.standard_normal(s.n)

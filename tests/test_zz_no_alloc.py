@@ -43,6 +43,31 @@ def test_noalloc_dot_matches_allocating_dot_twice():
         assert abs(got - float(np.dot(x, y))) <= RTOL * scale
 
 
+def test_noalloc_dot_leaves_free_memory_unchanged():
+    """After the first call on the device (which loads the module and its static array),
+    further calls take no device memory: cudaMemGetInfo's free bytes do not move."""
+    import torch
+
+    from gpu_util import dev
+
+    so = lib.load()
+    n = 1 << 20
+    rng = np.random.default_rng(7)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    xd, yd = dev(x), dev(y)
+    st, _ = _dot(so.jxcpr_dot_dev_noalloc, xd, yd, 0)  # warm-up call, as the header asks
+    assert st == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        st, got = _dot(so.jxcpr_dot_dev_noalloc, xd, yd, n)
+        assert st == 0
+        assert abs(got - float(np.dot(x, y))) <= RTOL * max(1.0, float(np.abs(x).dot(np.abs(y))))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_dot_rejects_sizes_beyond_scratch():
     from gpu_util import dev
 
