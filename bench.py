@@ -15,12 +15,12 @@ true residual b - A x in FP64 before it reports convergence).
           learned per-level strength thresholds and Chebyshev intervals, the
           stage-2 weights of the reference's mixed-precision driver, flexible
           FP64 GMRES run on the device as one CUDA graph), seconds;
-          config.plain_fp64_s is the same measurement for the plain FP64 path
+          details.plain_fp64_s is the same measurement for the plain FP64 path
           (the reference's CPR weights, host-driven MGS GMRES) and
-          config.speedup_vs_plain_fp64 their ratio; config.*same_driver* is
+          details.speedup_vs_plain_fp64 their ratio; details.*same_driver* is
           the plain FP64 preconditioner under the measured path's weights and
           GMRES driver (what precision + learned settings alone gain), and
-          config.hybrid_* the reference's hybrid form (FP32 stage 1, FP64
+          details.hybrid_* the reference's hybrid form (FP32 stage 1, FP64
           stage-2 polish).
   e2e   : the measured path through the public C ABI from pinned host buffers,
           timed per step from the host->device upload of the matrix and b,
@@ -30,9 +30,12 @@ The matrix, AMG hierarchy and Krylov basis (~2 GB) exceed L2 (126 MB), so no
 explicit flush is needed between steps.
 
 --impl reference times the reference library (compiled from its own sources
-into oracle/_ref) on the host cores, on a bounded sample: decoupling + CPR
-setup + GMRES runs of 2 and 4 iterations, scaled to the reference's iteration
-count on this system.
+into oracle/_ref) on the host cores: every timed step is one complete run to
+FP64 rel-res 1e-6; value = its GMRES solve phase (setup excluded, as our
+value), e2e = decoupling + setup + solve.  Our arm's cpu_baseline is a
+bounded sample of the same library (decoupling + setup + GMRES runs of 2 and
+4 iterations, scaled to the reference's iteration count) so that the default
+run stays short.
 
 Multi-GPU (torchrun): replicas -- every rank solves its own copy of the
 system; value is the max over ranks of the mean solve time (weak scaling).
@@ -89,6 +92,10 @@ BATCH_METRIC = "batched CPR-GMRES solves per second to 1e-6 FP64 rel-res (64 une
 # batched solves: mixed precision (FP32 preconditioner), Chebyshev-3 on the dense levels, flexible FP64 GMRES
 BATCH_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=1, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8)
 
+
+# the kernel the `roofline` object reports for each workload: the one with the largest share of the
+# measured solve in its launch list (profiles/launches_*): "cheb_level1" or "stage2"
+DOMINANT = {"c1": "cheb_level1", "c4": "stage2"}
 
 # per-workload method choices: the three-phase system is decoupled by True-IMPES and solved with
 # GMRES(60) (with ABF, or with GMRES(30), the reference itself is still short of 1e-6 after 300
@@ -198,9 +205,9 @@ class ClockSampler:
 # reference arm / CPU baseline
 # ---------------------------------------------------------------------------
 def reference_sample(s, threads, cfg):
-    """Reference library on the host: decouple + CPR setup + 2 GMRES iterations.
+    """Reference library on the host, bounded sample: decouple + CPR setup + 2 and 4 GMRES iterations.
 
-    Returns (estimated seconds for the full solve, measured sample seconds,
+    Returns (estimated seconds of the solve phase to 1e-6, measured sample seconds,
     description, kind)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import oracle
@@ -216,10 +223,12 @@ def reference_sample(s, threads, cfg):
         wall = time.perf_counter() - t0
         t_dec, t_setup = r2["times"][0], r2["times"][1]
         per_iter = max(0.0, (r4["times"][2] - r2["times"][2]) / 2.0)
-        est = t_dec + t_setup + r2["times"][2] + per_iter * max(0, iters_full - 2)
+        est = r2["times"][2] + per_iter * max(0, iters_full - 2)
         desc = (f"reference JXFPAMG built from source (FP64), {threads} OpenMP threads: decoupling + CPR setup + "
-                f"GMRES runs of 2 and 4 iterations ({wall:.1f} s in total); the per-iteration time (difference / 2) "
-                f"is scaled to the {iters_full} iterations the reference needs on this system")
+                f"GMRES runs of 2 and 4 iterations ({wall:.1f} s in total); the solve phase (setup excluded, as "
+                f"value) is the 2-iteration run's plus the per-iteration time (difference / 2) scaled to the "
+                f"{iters_full} iterations the reference needs on this system (decoupling {t_dec:.2f} s and setup "
+                f"{t_setup:.2f} s come on top)")
         return est, wall, desc, "reference"
     # fallback: the oracle restatement (single thread)
     sample_iters = 4
@@ -230,13 +239,50 @@ def reference_sample(s, threads, cfg):
     oracle.gmres(s.ia, s.ja, a, s.block_size, b, tol=1e-6, max_iter=sample_iters, cpr=C,
                  k_dim=CONFIG_OPTS.get(cfg, {}).get("k_dim", 30))
     t2 = time.perf_counter()
-    est = (t1 - t0) + (t2 - t1) / sample_iters * iters_full
+    est = (t2 - t1) / sample_iters * iters_full
     desc = (f"oracle C restatement (1 thread): decoupling + CPR setup + {sample_iters} GMRES iterations "
-            f"({t2 - t0:.1f} s), scaled to {iters_full} iterations")
+            f"({t2 - t0:.1f} s); the solve phase scaled to {iters_full} iterations")
     return est, t2 - t0, desc, "port"
 
 
+def common_config(cfg, opts):
+    """The `config` object both arms print (identical keys and values for one workload)."""
+    return {"workload": WORKLOADS[cfg],
+            "decoupling": "True-IMPES" if opts.get("decouple") == 5 else "ABF",
+            "tol": 1e-6, "k_dim": opts.get("k_dim", 30),
+            "l2_flush": "not needed: matrix + hierarchy + Krylov basis > 126 MB L2"}
+
+
+def reference_full_solve(s, threads, cfg):
+    """One complete run of the reference library on the host: decoupling, CPR setup and GMRES to
+    FP64 rel-res 1e-6.  Returns (seconds per phase [decouple, setup, solve], iterations, kind)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    dec = CONFIG_OPTS.get(cfg, {}).get("decouple", 1)
+    kd = CONFIG_OPTS.get(cfg, {}).get("k_dim", 30)
+    mi = CONFIG_OPTS.get(cfg, {}).get("max_iter", 300)
+    if oracle.ref_available():
+        r = oracle.ref_gmres(s.ia, s.ja, s.a, s.block_size, s.b, decouple=dec, tol=1e-6, max_iter=mi, k_dim=kd)
+        if not r["converged"]:
+            raise RuntimeError(f"reference solve did not converge (rel {r['rel']})")
+        return [float(r["times"][0]), float(r["times"][1]), float(r["times"][2])], r["iters"], "reference"
+    t0 = time.perf_counter()
+    a, b = oracle.bsr_decouple(s.ia, s.ja, s.a, s.block_size, s.b, dec)
+    t1 = time.perf_counter()
+    C = oracle.OracleCPR(s.ia, s.ja, a, s.block_size)
+    t2 = time.perf_counter()
+    r = oracle.gmres(s.ia, s.ja, a, s.block_size, b, tol=1e-6, max_iter=mi, cpr=C, k_dim=kd)
+    t3 = time.perf_counter()
+    return [t1 - t0, t2 - t1, t3 - t2], r["iters"], "port"
+
+
 def run_reference(args):
+    """--impl reference: the reference's own CPU implementation of the path (compiled from its sources
+    into oracle/_ref; the oracle restatement where it is absent) on all host threads.  Each timed step is
+    one complete run to convergence; value = the GMRES solve phase (setup excluded, as in our arm's
+    value), e2e = decoupling + CPR setup + solve (as our arm's e2e, which also includes the uploads).
+    Warm-up steps are short runs (two GMRES iterations) that page the library and the system in."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -244,23 +290,41 @@ def run_reference(args):
 
     s = synth.config_system(args.config)
     threads = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        reference_sample(s, threads, args.config)
-    vals = []
-    desc = kind = None
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    dec = CONFIG_OPTS.get(args.config, {}).get("decouple", 1)
+    kd = CONFIG_OPTS.get(args.config, {}).get("k_dim", 30)
+    for _ in range(args.warmup):
+        if oracle.ref_available():
+            oracle.ref_gmres(s.ia, s.ja, s.a, s.block_size, s.b, decouple=dec, tol=1e-6, max_iter=2, k_dim=kd)
+    phases, iters, kind = [], [], None
+    w0 = time.perf_counter()
     for _ in range(args.steps):
-        est, wall, desc, kind = reference_sample(s, threads, args.config)
-        vals.append(est)
-    value = float(np.mean(vals))
+        t, it, kind = reference_full_solve(s, threads, args.config)
+        phases.append(t)
+        iters.append(it)
+    wall = time.perf_counter() - w0
+    ph = np.array(phases)
+    value = float(ph[:, 2].mean())
+    total = float(ph.sum(axis=1).mean())
+    what = ("reference JXFPAMG built from source (FP64)" if kind == "reference"
+            else "oracle C restatement (FP64, the reference library was not built)")
+    desc = (f"{what}, {threads} OpenMP threads, {args.steps} complete runs to FP64 rel-res 1e-6 "
+            f"({iters[0]} GMRES iterations; decoupling {ph[:, 0].mean():.2f} s, CPR setup {ph[:, 1].mean():.2f} s, "
+            f"solve {value:.2f} s per run; {wall:.0f} s in all)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.config],
-                   "decoupling": "True-IMPES" if CONFIG_OPTS.get(args.config, {}).get("decouple") == 5 else "ABF",
-                   "tol": 1e-6, "k_dim": CONFIG_OPTS.get(args.config, {}).get("k_dim", 30)},
+        "config": common_config(args.config, plain_opts(args)),
+        "parallelism": f"1 host process, {threads} OpenMP threads",
+        "details": {"value_definition": "GMRES solve phase of a complete run (decoupling and CPR setup excluded, "
+                                        "reported in e2e)",
+                    "iterations": iters[0], "decouple_s": float(ph[:, 0].mean()), "setup_s": float(ph[:, 1].mean()),
+                    "solve_s": value, "ms_per_step_definition": "one complete run (decoupling + setup + solve)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": total, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -350,6 +414,7 @@ def run_ours(args):
     plain_t, plain_it, plain_rel, _, clk_p = timed(P, "plain FP64")
     x_plain = d_x.cpu().numpy().copy()
     roof_plain = roofline_stage2(P, s, stream, 8, args.config)
+    plain_gbs = iteration_bytes(P, s, plain_opts(args).get("k_dim", 30)) * plain_it / plain_t / 1e9
     P.close()
 
     # ---- the reference's hybrid form (FP32 stage 1 + FP64 polish), for comparison ------
@@ -369,8 +434,15 @@ def run_ours(args):
     per_solve, it_m, rel_m, launches, clocks = timed(G, "mixed+learned")
     x_mixed = d_x.cpu().numpy().copy()
     err_vs_fp64 = float(np.linalg.norm(x_mixed - x_plain) / np.linalg.norm(x_plain))
-    roof = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) in (0, 3) else 4, args.config)
+    vb = 8 if measured_opts.get("precision", 0) == 0 else 4
+    roof_st2 = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) in (0, 3) else 4, args.config)
+    roof_lvl = roofline_level(G, stream, 1, 1, vb, vb, args.config) if G.num_levels() > 2 else None
+    solve_gbs = iteration_bytes(G, s, measured_opts.get("k_dim", 30)) * it_m / per_solve / 1e9
     G.close()
+    roof_spmv = roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, args.config)
+    # the roofline line names the kernel with the largest share of the measured solve (launch list in
+    # profiles/): the level-1 Chebyshev pass where the level has one, else the stage-2 sweep
+    roof = roof_lvl if (roof_lvl is not None and DOMINANT.get(args.config) == "cheb_level1") else roof_st2
     if clk_p.get("reasons"):
         clocks["reasons"] = sorted(set(clocks.get("reasons", [])) | set(clk_p["reasons"]))
 
@@ -421,27 +493,33 @@ def run_ours(args):
             "metric": METRIC, "value": per_solve, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_solve * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.config],
-                       "method": f"CPR-GMRES({measured_opts.get('k_dim', 30)}) to FP64 true rel-res 1e-6, " +
-                                 ("True-IMPES" if measured_opts.get("decouple") == 5 else "ABF") +
-                                 " decoupling, AMG V(1,1) (HMIS, ext+i) "
-                                 "+ 3 block-GS stage-2 sweeps",
-                       "measured_path": measured_path_text(measured_opts, learned),
-                       "options": measured_opts,
-                       "iterations": it_m, "final_rel_res": rel_m,
-                       "plain_fp64_s": plain_t, "plain_fp64_iterations": plain_it, "plain_fp64_rel_res": plain_rel,
-                       "speedup_vs_plain_fp64": plain_t / per_solve,
-                       "hybrid_fp32_fp64_s": hybrid_t, "hybrid_iterations": hybrid_it,
-                       "plain_fp64_same_driver_s": plain_d_t, "plain_fp64_same_driver_iterations": plain_d_it,
-                       "speedup_vs_plain_fp64_same_driver": plain_d_t / per_solve,
-                       "hybrid_speedup_vs_plain_fp64": plain_t / hybrid_t,
-                       "x_rel_diff_vs_plain_fp64": err_vs_fp64,
-                       "learned": learned,
-                       "setup_s": setup_stats["setup_ms"] / 1e3, "plain_setup_s": plain_setup["setup_ms"] / 1e3,
-                       "amg_levels": setup_stats["levels"],
-                       "roofline_plain_fp64_stage2": roof_plain,
-                       "l2_flush": "not needed: matrix + hierarchy + Krylov basis > 126 MB L2",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "config": common_config(args.config, measured_opts),
+            "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+            "details": {"method": f"CPR-GMRES({measured_opts.get('k_dim', 30)}) to FP64 true rel-res 1e-6, " +
+                                  ("True-IMPES" if measured_opts.get("decouple") == 5 else "ABF") +
+                                  " decoupling, AMG V(1,1) (HMIS, ext+i) + 3 block-GS stage-2 sweeps",
+                        "measured_path": measured_path_text(measured_opts, learned),
+                        "options": measured_opts,
+                        "iterations": it_m, "final_rel_res": rel_m,
+                        "solve_gbs": solve_gbs,
+                        "solve_gbs_definition": "modelled bytes per GMRES iteration (preconditioner traffic at its "
+                                                "storage precision + FP64 BSR SpMV + CGS2 orthogonalisation) x "
+                                                "iterations / solve time",
+                        "plain_fp64_s": plain_t, "plain_fp64_iterations": plain_it, "plain_fp64_rel_res": plain_rel,
+                        "plain_fp64_solve_gbs": plain_gbs,
+                        "speedup_vs_plain_fp64": plain_t / per_solve,
+                        "hybrid_fp32_fp64_s": hybrid_t, "hybrid_iterations": hybrid_it,
+                        "plain_fp64_same_driver_s": plain_d_t, "plain_fp64_same_driver_iterations": plain_d_it,
+                        "speedup_vs_plain_fp64_same_driver": plain_d_t / per_solve,
+                        "hybrid_speedup_vs_plain_fp64": plain_t / hybrid_t,
+                        "x_rel_diff_vs_plain_fp64": err_vs_fp64,
+                        "learned": learned,
+                        "setup_s": setup_stats["setup_ms"] / 1e3, "plain_setup_s": plain_setup["setup_ms"] / 1e3,
+                        "amg_levels": setup_stats["levels"],
+                        "roofline_bsr_spmv": roof_spmv,
+                        "roofline_stage2": roof_st2,
+                        "roofline_cheb_level1": roof_lvl,
+                        "roofline_plain_fp64_stage2": roof_plain},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": float(e2e_t.item()), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -458,54 +536,122 @@ def run_ours(args):
     return 0
 
 
-# DRAM traffic of one stage-2 sweep's kernels (both colour launches), from an ncu capture of the same
-# solve (dram__bytes_read.sum + dram__bytes_write.sum, layouts reused through JXCPR_TUNE_CACHE):
-# (workload, value bytes, layout) -> bytes.
-STAGE2_TRAFFIC_BYTES = {("c1", 4, "sell"): 209.4e6}
+# DRAM traffic per launch of the roofline kernels, from ncu captures of the same kernels on the same
+# workload (dram__bytes_read.sum + dram__bytes_write.sum; layouts reused through JXCPR_TUNE_CACHE), each
+# summarised in profiles/: (workload, kernel key) -> bytes.  None where not captured.
+TRAFFIC_BYTES = {}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(p)) if os.path.exists(p) else {}
+    if peaks.get("hbm_gbs"):
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _event_time(stream, body, reps):
+    """Mean device seconds of body() (which queues `reps` launches) between events on `stream`."""
+    import torch
+
+    body(3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    body(reps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def _roof(kernel, alg, sec, cfg, key, extra=None):
+    peak, src = hbm_peak()
+    achieved = alg / sec / 1e9
+    out = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_source": src, "traffic": TRAFFIC_BYTES.get((cfg, key)),
+           "algorithmic_bytes": int(alg), "launch_ms": sec * 1e3}
+    out.update(extra or {})
+    return out
+
+
+def _layout(G, name):
+    for line in G.setup_report().splitlines():
+        if line.startswith("tuned " + name + " ") and " layout " in line:
+            return line.split(" layout ")[1].split()[0]
+    return "?"
 
 
 def roofline_stage2(G, s, stream, value_bytes, cfg="c1"):
-    """Roofline of the stage-2 block Gauss-Seidel sweep (one launch per colour
-    class) in the path's own storage precision: algorithmic bytes of one sweep /
-    mean sweep time (CUDA events on the solver's stream)."""
+    """Stage-2 block Gauss-Seidel sweep (one launch per colour) in the path's own storage precision:
+    algorithmic bytes of one sweep / mean sweep time (CUDA events on the solver's stream)."""
+    from jxpamg_all_b200 import lib
+
+    so = lib.load()
+    reps = 20
+    sec = _event_time(stream, lambda r: lib.check(so.jxcpr_solver_stage2_native(G.h, r)), reps)
+    bs, nb, nnzb, n = s.block_size, s.num_block_rows, s.nnzb, s.n
+    # values + column indices + row pointers; b read, x read and written, the start values of the
+    # colours before the last written to vt and read back by their neighbours (about n in all)
+    alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * value_bytes * 5
+    layout = _layout(G, "stage2")
+    kname = {"sell": f"hgs_sell<{bs}>"}.get(layout, f"hgs_chunk<{bs}>" if layout.startswith("chunk")
+                                               else f"hgs_color<{bs}> ({layout})")
+    return _roof(f"stage-2 block hybrid Gauss-Seidel sweep ({kname}, {'FP64' if value_bytes == 8 else 'FP32'} "
+                 "values, one launch per colour)", alg, sec, cfg, f"stage2/{value_bytes}/{layout}",
+                 {"sweep_ms": sec * 1e3})
+
+
+def roofline_level(G, stream, level, op, value_bytes, vec_bytes, cfg="c1"):
+    """One pass over AMG level `level` (op 1: a Chebyshev step y = c z + D^-1 A x) in the path's storage
+    precision and layout: algorithmic bytes nnz (p_v + 4) + (n + 1) 4 + 4 n p_x (x, z, D^-1 read,
+    y written) / mean launch time (CUDA events on the solver's stream)."""
+    from jxpamg_all_b200 import lib
+
+    so = lib.load()
+    n, _, nnz = G.level_sizes(level, 0)
+    sec = _event_time(stream, lambda r: lib.check(so.jxcpr_solver_level_native(G.h, level, op, r)), 20)
+    alg = nnz * (value_bytes + 4) + (n + 1) * 4 + 4 * n * vec_bytes
+    layout = _layout(G, f"A{level}")
+    fmt = "SellFmt" if layout == "sell" else f"CsrFmt<{layout.split('/')[-1]}>"
+    ty = {8: "double", 4: "float", 2: "bf16"}[value_bytes]
+    return _roof(f"AMG level {level} Chebyshev step (row_kernel<{fmt}<{ty}>, OpCheb>, {n} rows, {nnz} entries)",
+                 alg, sec, cfg, f"cheb/A{level}/{value_bytes}/{layout}", {"level": level})
+
+
+def roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, cfg="c1"):
+    """The FP64 BSR SpMV y = A x of GMRES (bsr_spmv_direct_kernel) on the workload's matrix."""
     import torch
 
     from jxpamg_all_b200 import lib
 
     so = lib.load()
-    peaks = {}
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        peaks = json.load(open(p))
-    peak = peaks.get("hbm_gbs")
-    src = "measured" if peak else "fallback"
-    peak = peak or 6650.0
-    reps = 20
-    lib.check(so.jxcpr_solver_stage2_native(G.h, 3))
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    lib.check(so.jxcpr_solver_stage2_native(G.h, reps))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    sec = e0.elapsed_time(e1) / 1e3 / reps
+    x = torch.ones(s.n, dtype=torch.float64, device="cuda")
+    y = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+
+    def body(r):
+        for _ in range(r):
+            lib.check(so.jxcpr_bsr_matvec_dev(s.num_block_rows, s.block_size, s.nnzb, d_ia.data_ptr(),
+                                              d_ja.data_ptr(), d_a.data_ptr(), 1.0, x.data_ptr(), 0.0,
+                                              y.data_ptr(), 0, ctypes.c_void_p(stream.cuda_stream)))
+
+    sec = _event_time(stream, body, 20)
     bs, nb, nnzb, n = s.block_size, s.num_block_rows, s.nnzb, s.n
-    xb = value_bytes  # the mixed path keeps the stage-2 vectors in FP32 too
-    # values + column indices + row pointers; b read, x read and written, the start values of the
-    # classes before the last written to vt and read back by their neighbours (about n in all)
-    alg = nnzb * (bs * bs * value_bytes + 4) + (nb + 1) * 4 + n * xb * 5
-    achieved = alg / sec / 1e9
-    layout = "?"
-    for line in G.setup_report().splitlines():
-        if line.startswith("tuned stage2") and " layout " in line:
-            layout = line.split(" layout ")[1].split()[0]
-    kname = f"hgs_sell<{bs}>" if layout == "sell" else f"hgs_color<{bs}> ({layout})"
-    return {"bound": "hbm", "kernel": f"stage-2 block hybrid Gauss-Seidel sweep ({kname}, "
-            f"{'FP64' if value_bytes == 8 else 'FP32'} values, one launch per colour class)",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": src, "traffic": STAGE2_TRAFFIC_BYTES.get((cfg, value_bytes, layout)),
-            "traffic_note": "ncu DRAM bytes of the sweep's colour launches; null where not captured",
-            "algorithmic_bytes": int(alg), "sweep_ms": sec * 1e3}
+    alg = nnzb * (bs * bs * 8 + 4) + (nb + 1) * 4 + 2 * n * 8
+    return _roof(f"BSR SpMV y = A x (bsr_spmv_direct_kernel<{bs}, double>, FP64)", alg, sec, cfg, "bsr_spmv/8")
+
+
+def iteration_bytes(G, s, k_dim):
+    """Modelled bytes of one GMRES iteration: the preconditioner application (its modelled traffic), the
+    FP64 BSR SpMV, and the flexible CGS2 orthogonalisation at the mean step of a cycle (two passes over
+    the basis, the update fused with the second products: (2 j + 6) n doubles at step j)."""
+    from jxpamg_all_b200 import lib
+
+    so = lib.load()
+    ab = np.zeros(1)
+    lib.check(so.jxcpr_solver_apply_bytes(G.h, ab.ctypes.data_as(ctypes.c_void_p)))
+    spmv = s.nnzb * (s.block_size ** 2 * 8 + 4) + (s.num_block_rows + 1) * 4 + 2 * s.n * 8
+    jm = (k_dim - 1) / 2.0
+    return float(ab[0]) + spmv + (2 * jm + 6) * s.n * 8
 
 
 # ---------------------------------------------------------------------------

@@ -102,6 +102,14 @@ JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, doubl
 JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *y, double *out_host,
                                     void *stream);
 
+/* ---- dense inverse (coarsest AMG level) ------------------------------------
+ * ainv = a^-1 for a dense n x n row-major FP64 matrix (n <= 8192; device pointers, may not alias) by
+ * blocked Gauss-Jordan elimination without pivoting, as the reference eliminates its coarsest level
+ * (jxf_gselim, jxfpamg-0220/csrc/operation/matops/par_gs.c:20-74, no pivoting): one cooperative kernel,
+ * trailing updates on the FP64 tensor cores.  The fast path's coarse solve is a GEMV with this inverse.
+ * A zero pivot returns JXCPR_ERROR_ARG ("singular without pivoting").  Synchronises `stream`. */
+JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void *stream);
+
 /* ---- solver object ---------------------------------------------------------
  * CPR-GMRES on one GPU: jxcpr_solver_setup copies a BSR matrix (host or
  * device arrays), applies the configured decoupling (jxf_BSRMatrixDecouple,
@@ -209,6 +217,15 @@ JXCPR_API int jxcpr_solver_stage2_native(jxcpr_solver *solver, int sweeps);
  * status code. */
 JXCPR_API int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int chunk, int *order, int capacity,
                                        int *segments, int seg_capacity);
+
+/* Queues `reps` passes over AMG level `level`'s operator (not the coarsest) in the fast path's storage
+ * precision and layout, on the level's own work vectors, asynchronously on the solver's stream (no
+ * reference counterpart; the kernel a roofline measurement times with events on that stream):
+ * op 0 y = A x, 1 one Chebyshev step y = c z + D^-1 A x, 2 the residual r = f - A u. */
+JXCPR_API int jxcpr_solver_level_native(jxcpr_solver *solver, int level, int op, int reps);
+/* Modelled bytes one preconditioner application of the fast path moves (every smoother pass, residual,
+ * transfer, coarse solve and stage-2 sweep at its storage precision); no reference counterpart. */
+JXCPR_API int jxcpr_solver_apply_bytes(jxcpr_solver *solver, double *bytes);
 
 /* ---- fast path (smoother_order 1) inspection: no reference counterpart ---------------------
  * level_info: smoother (1 multicolour GS, 2 l1-Jacobi, 3 Chebyshev-3; 0 exact path), storage

@@ -92,39 +92,6 @@ __global__ void __launch_bounds__(1024) lu_solve_kernel(int n, const double *__r
     for (int i = threadIdx.x; i < n; i += blockDim.x) u[i] = xs[i];
 }
 
-// Explicit inverse (setup of the fast coarse solve): X = I, then the forward
-// and back substitutions of the stored factors applied to every column at
-// once, one launch per elimination step (the same operations per column as a
-// column-by-column substitution).
-__global__ void eye_kernel(int n, double *__restrict__ X) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < (long long)n * n) X[t] = (t / n == t % n) ? 1.0 : 0.0;
-}
-
-// rows j > k: X[j][c] -= L[j][k] X[k][c]
-__global__ void inv_forward_kernel(int n, int k, const double *__restrict__ Lt, double *__restrict__ X) {
-    const int j = k + 1 + blockIdx.y;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n || c >= n) return;
-    const double l = Lt[(long long)k * n + j];
-    if (l != 0.0) X[(long long)j * n + c] -= l * X[(long long)k * n + c];
-}
-
-// rows j < k: X[j][c] -= U[j][k] (X[k][c] / U[k][k]); row k itself is scaled by inv_scale_kernel afterwards
-__global__ void inv_backward_kernel(int n, int k, const double *__restrict__ Ut, double *__restrict__ X) {
-    const int j = blockIdx.y;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= k || c >= n) return;
-    const double v = Ut[(long long)k * n + j];
-    if (v != 0.0) X[(long long)j * n + c] -= (X[(long long)k * n + c] / Ut[(long long)k * n + k]) * v;
-}
-
-__global__ void inv_scale_kernel(int n, int k, const double *__restrict__ Ut, double *__restrict__ X) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) X[(long long)k * n + c] /= Ut[(long long)k * n + k];
-}
-
-
 // u = Ainv f, one warp per row.
 __global__ void dense_gemv_kernel(int n, const double *__restrict__ Ainv, const double *__restrict__ f,
                                   double *__restrict__ u) {
@@ -147,6 +114,12 @@ void coarse_setup(Amg &H, cudaStream_t s) {
         set_error("coarsest level has %d rows (dense solve limited to 8192); coarsening stalled", n);
         throw CudaError{cudaErrorInvalidValue, "coarse size"};
     }
+    if (!H.prm.coarse_exact) {
+        // fast coarse solve: only the inverse is needed (one cooperative DMMA kernel, coarse_mma.cu)
+        H.Ainv.alloc((size_t)n * n);
+        coarse_inverse_mma(L.A.view(), H.Ainv.get(), H.err.get(), s);
+        return;
+    }
     DevBuf<double> M((size_t)n * n);
     M.zero(s);
     dense_assemble_kernel<<<div_up(n, 128), 128, 0, s>>>(n, L.A.ia.get(), L.A.ja.get(), L.A.a.get(), M.get());
@@ -161,24 +134,6 @@ void coarse_setup(Amg &H, cudaStream_t s) {
     H.Ufac.alloc((size_t)n * n);
     transpose_upper_kernel<<<dim3(div_up(n, 256), n), 256, 0, s>>>(n, M.get(), H.Ufac.get());
     JX_LAUNCH_CHECK();
-    if (!H.prm.coarse_exact) {
-        H.Ainv.alloc((size_t)n * n);
-        double *X = H.Ainv.get();
-        eye_kernel<<<div_up((long long)n * n, 256), 256, 0, s>>>(n, X);
-        JX_LAUNCH_CHECK();
-        for (int k = 0; k < n - 1; ++k) {
-            inv_forward_kernel<<<dim3(div_up(n, 256), n - k - 1), 256, 0, s>>>(n, k, H.Lt.get(), X);
-            JX_LAUNCH_CHECK();
-        }
-        for (int k = n - 1; k >= 0; --k) {
-            if (k > 0) {
-                inv_backward_kernel<<<dim3(div_up(n, 256), k), 256, 0, s>>>(n, k, H.Ufac.get(), X);
-                JX_LAUNCH_CHECK();
-            }
-            inv_scale_kernel<<<div_up(n, 256), 256, 0, s>>>(n, k, H.Ufac.get(), X);
-            JX_LAUNCH_CHECK();
-        }
-    }
     JX_CUDA(cudaStreamSynchronize(s));
 }
 

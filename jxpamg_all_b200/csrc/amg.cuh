@@ -116,6 +116,12 @@ void upload_schedule(const std::vector<int> &perm, const std::vector<int> &gptr,
 void build_chunk_order_host(int n, const int *ia, const int *ja, int chunk, std::vector<int> &order,
                             std::vector<int> &seg);
 
+// coarse_mma.cu: explicit inverse by blocked Gauss-Jordan (no pivoting) in one cooperative kernel with
+// FP64 tensor-core (DMMA) trailing updates.  err: 4 device ints (flags, grid barrier); a zero pivot
+// throws std::invalid_argument, a barrier time-out CudaError.
+void coarse_inverse_mma(const CsrView<double> &A, double *Ainv, int *err, cudaStream_t s);
+void dense_inverse_mma(int n, const double *A, double *Ainv, cudaStream_t s);
+
 // amg.cu
 void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s);
 void amg_vcycle(Amg &H, const double *f0, double *u0, cudaStream_t s);  // one V(1,1), u0 in/out

@@ -4,7 +4,9 @@
 // status code (0 = success) and never aborts; jxcpr_last_error() explains a
 // failure.
 #include <mutex>
+#include <stdexcept>
 
+#include "amg.cuh"
 #include "common.cuh"
 #include "jxcpr_b200.h"
 #include "kernels.cuh"
@@ -33,6 +35,8 @@ int guarded(F &&f) {
         return JXCPR_SUCCESS;
     } catch (const CudaError &) {
         return JXCPR_ERROR_DEVICE;
+    } catch (const std::invalid_argument &) {
+        return JXCPR_ERROR_ARG;  // the message was set where it was thrown
     } catch (const std::bad_alloc &) {
         set_error("host allocation failed");
         return JXCPR_ERROR_MEMORY;
@@ -105,6 +109,14 @@ int jxcpr_dot_dev(long long n, const double *x, const double *y, double *out_hos
                                 s));
         JX_CUDA(cudaStreamSynchronize(s));
     });
+}
+
+int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void *stream) {
+    if (n < 0 || n > 8192 || (n > 0 && (!a || !ainv))) {
+        set_error("dense_inverse: n must be in [0, 8192] and the pointers set (n = %d)", n);
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] { dense_inverse_mma(n, a, ainv, (cudaStream_t)stream); });
 }
 
 }  // extern "C"

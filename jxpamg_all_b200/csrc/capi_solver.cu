@@ -419,6 +419,31 @@ int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int devic
     });
 }
 
+int jxcpr_solver_level_native(jxcpr_solver *h, int level, int op, int reps) {
+    if (!h || reps < 0 || op < 0 || op > 2 || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    if (!h->s.cpr.fast) {
+        set_error("level_native needs the fast path (smoother_order 1)");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        if (!h->s.cpr.fast->level_native(level, op, reps, h->s.stream)) {
+            set_error("level_native: level %d has no smoothed operator", level);
+            return JXCPR_ERROR_ARG;
+        }
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_apply_bytes(jxcpr_solver *h, double *bytes) {
+    if (!h || !bytes || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
+    if (!h->s.cpr.fast) {
+        set_error("apply_bytes needs the fast path (smoother_order 1)");
+        return JXCPR_ERROR_ARG;
+    }
+    *bytes = h->s.cpr.fast->apply_bytes();
+    return JXCPR_SUCCESS;
+}
+
 int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int chunk, int *order, int capacity,
                              int *segments, int seg_capacity) {
     if (nb < 0 || (nb > 0 && (!ia || !ja)) || (chunk != 4 && chunk != 8 && chunk != 16) || capacity < 0) {

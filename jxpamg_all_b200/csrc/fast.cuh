@@ -128,6 +128,10 @@ struct FastCprBase {
     // `sweeps` stage-2 sweeps in the preconditioner's own precision on internal
     // vectors (no conversions), queued on s: the kernel the roofline times.
     virtual void stage2_native(int sweeps, cudaStream_t s) = 0;
+    // `reps` passes over level l's operator in its storage precision on the level's own work vectors,
+    // queued on s (what a roofline measurement times): op 0 y = A x, 1 one Chebyshev step
+    // (y = c z + D^-1 A x), 2 the residual r = f - A u.  Returns false if the level has no operator.
+    virtual bool level_native(int level, int op, int reps, cudaStream_t s) = 0;
     // One line per tuned operator: "name rows mean_row layout time_us".
     std::vector<std::string> tune_log;
 };

@@ -870,6 +870,26 @@ struct FastCpr final : FastCprBase {
         }
     }
 
+    bool level_native(int level, int op, int reps, cudaStream_t s) override {
+        if (level < 0 || level + 1 >= (int)lv.size()) return false;
+        FastLevel<TX> &L = *lv[level];
+        if (L.n == 0) return false;
+        DepLaunchScope dep(opt.dep_launch);
+        if (!L.y1.get()) alloc_vec(L.y1, L.n);
+        if (!L.y2.get()) alloc_vec(L.y2, L.n);
+        for (int k = 0; k < reps; ++k) {
+            if (op == 0) {
+                spmv(L.A, L.u.get(), false, L.y1.get(), s);
+            } else if (op == 1) {
+                fk::OpCheb<TX> c1{1, 0, (TX)0.5, L.f.get(), L.dinv.get(), L.u.get(), L.u.get(), L.z.get(), L.y1.get()};
+                launch_rows<TX>(L.A, c1, 0, L.A.nstored, s);
+            } else {
+                residual(L, L.f.get(), L.u.get(), L.r.get(), s);
+            }
+        }
+        return true;
+    }
+
     double apply_bytes() const override {
         auto vb = [](int kind) { return kind == VAL_F64 ? 8.0 : (kind == VAL_F32 ? 4.0 : 2.0); };
         const double xb = sizeof(TX);

@@ -31,6 +31,7 @@ def _declare(lib):
     lib.jxcpr_bsr_matvec_dev_f32.argtypes = lib.jxcpr_bsr_matvec_dev.argtypes
     lib.jxcpr_dot_dev.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.jxcpr_dot_dev_noalloc.argtypes = [c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.jxcpr_dense_inverse_dev.argtypes = [c_int, c_void_p, c_void_p, c_void_p]
     _declare_solver(lib)
     _declare_mlp(lib)
 
@@ -74,6 +75,8 @@ def _declare_solver(lib):
     lib.jxcpr_solver_stage2_sweep.argtypes = [P, P, P, c_int]
     lib.jxcpr_solver_level_info.argtypes = [P, c_int, P, P, P, P]
     lib.jxcpr_solver_stage2_native.argtypes = [P, c_int]
+    lib.jxcpr_solver_level_native.argtypes = [P, c_int, c_int, c_int]
+    lib.jxcpr_solver_apply_bytes.argtypes = [P, P]
     lib.jxcpr_stage2_chunk_order.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]
     lib.jxcpr_solver_bilu_sizes.argtypes = [P, P]
     lib.jxcpr_solver_bilu_factors.argtypes = [P, P, P, P]

@@ -374,6 +374,45 @@ def bilu_solve(ia, ja, a, bs, F, f, ir=5, lower=5, upper=5, u0=None):
     return u
 
 
+def bilu_levels(ia, ja):
+    """Levels of the lower and upper block-triangular DAGs: (lev_l, lev_u, number of lower levels,
+    number of upper levels)."""
+    nb = len(ia) - 1
+    lia, lja, uia, uja = bilu_pattern(ia, ja)
+    lev_l, lev_u = np.zeros(max(nb, 1), np.int32), np.zeros(max(nb, 1), np.int32)
+    nup = np.zeros(1, np.int32)
+    nl = orc().orc_bilu_levels(c_int(nb), _p(lia), _p(lja if len(lja) else np.zeros(1, np.int32)), _p(uia),
+                               _p(uja if len(uja) else np.zeros(1, np.int32)), _p(lev_l), _p(lev_u), _p(nup))
+    return lev_l[:nb], lev_u[:nb], int(nl), int(nup[0])
+
+
+def bilu_setup_exact(ia, ja, a, bs):
+    """Exact block ILU(0) factors (the fixed point of jxf_ILUSetupFGPBILU_v3's sweeps), as bilu_setup."""
+    nb = len(ia) - 1
+    lia, lja, uia, uja = bilu_pattern(ia, ja)
+    bn = bs * bs
+    la = np.zeros(max(len(lja), 1) * bn)
+    ua = np.zeros(max(len(uja), 1) * bn)
+    dinv = np.zeros(nb * bn)
+    orc().orc_bilu_setup_exact(c_int(nb), c_int(bs), _p(_i32(ia)), _p(_i32(ja)), _p(_f64(a)), _p(lia),
+                               _p(lja if len(lja) else np.zeros(1, np.int32)), _p(la), _p(uia),
+                               _p(uja if len(uja) else np.zeros(1, np.int32)), _p(ua), _p(dinv))
+    return dict(lia=lia, lja=lja, la=la[:len(lja) * bn], uia=uia, uja=uja, ua=ua[:len(uja) * bn], dinv=dinv)
+
+
+def bilu_solve_exact(ia, ja, a, bs, F, f, ir=5, u0=None):
+    """u += BILU^-1 (f - A u) with substitution in level order, `ir` refinement loops."""
+    nb = len(ia) - 1
+    u = np.zeros(nb * bs) if u0 is None else _f64(u0).copy()
+    z = np.zeros(1, np.int32)
+    orc().orc_bilu_solve_exact(c_int(nb), c_int(bs), _p(_i32(ia)), _p(_i32(ja)), _p(_f64(a)), _p(F["lia"]),
+                               _p(F["lja"] if len(F["lja"]) else z), _p(F["la"] if len(F["la"]) else np.zeros(1)),
+                               _p(F["uia"]), _p(F["uja"] if len(F["uja"]) else z),
+                               _p(F["ua"] if len(F["ua"]) else np.zeros(1)), _p(F["dinv"]), c_int(ir), _p(_f64(f)),
+                               _p(u))
+    return u
+
+
 def ref_bilu(ia, ja, a, bs, f, sweeps=3, ir=5, lower=5, upper=5):
     """The reference's jxf_BILUSetup + jxf_BILUSolve: (u, la, ua, dinv)."""
     nb = len(ia) - 1

@@ -82,6 +82,13 @@ int orc_gmres(int nb, int bs, const int *ia, const int *ja, const double *a, con
               double tol, int max_iter, const orc_cpr *precond, double *rel, int *converged, double *norms);
 
 /* ---- block ILU(0) restatement (orc_bilu.c) ---- */
+int orc_bilu_levels(int nb, const int *lia, const int *lja, const int *uia, const int *uja, int *lev_l,
+                    int *lev_u, int *nup);
+int orc_bilu_setup_exact(int nb, int bs, const int *ia, const int *ja, const double *a, const int *lia,
+                         const int *lja, double *la, const int *uia, const int *uja, double *ua, double *dinv);
+int orc_bilu_solve_exact(int nb, int bs, const int *ia, const int *ja, const double *a, const int *lia,
+                         const int *lja, const double *la, const int *uia, const int *uja, const double *ua,
+                         const double *dinv, int ir_iters, const double *f, double *u);
 int orc_bilu_pattern(int nb, const int *ia, const int *ja, int *lia, int *lja, int *uia, int *uja);
 int orc_bilu_setup(int nb, int bs, const int *ia, const int *ja, const double *a, int sweeps, const int *lia,
                    const int *lja, double *la, const int *uia, const int *uja, double *ua, double *dinv);

@@ -220,3 +220,151 @@ int orc_bilu_solve(int nb, int bs, const int *ia, const int *ja, const double *a
     free(un);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------
+ * Exact block ILU(0) with level-scheduled triangular solves (the device path's bilu_exact mode).
+ * No reference routine computes it directly; it is the fixed point the reference's FGPBILU sweeps
+ * and Jacobi triangular solves converge to, and every operation below is the one those routines
+ * apply to the final values (par_bilu_setup.c:5459-5609, par_bilu_solve.c:2893-3000), so the
+ * results equal the reference's bit for bit once its sweep and Jacobi counts exceed the levels.
+ * ------------------------------------------------------------------------ */
+
+/* Levels of the lower DAG (row r after every k of its L-row; lev_l) and of the upper DAG (row r
+ * after every c of its U-row; lev_u).  Returns the number of lower levels; *nup gets the upper one. */
+int orc_bilu_levels(int nb, const int *lia, const int *lja, const int *uia, const int *uja, int *lev_l,
+                    int *lev_u, int *nup)
+{
+    int nl = 0, nu = 0;
+    for (int r = 0; r < nb; r++) {
+        int l = 0;
+        for (int k = lia[r]; k < lia[r + 1]; k++)
+            if (lev_l[lja[k]] + 1 > l) l = lev_l[lja[k]] + 1;
+        lev_l[r] = l;
+        if (l + 1 > nl) nl = l + 1;
+    }
+    for (int r = nb - 1; r >= 0; r--) {
+        int l = 0;
+        for (int k = uia[r]; k < uia[r + 1]; k++)
+            if (lev_u[uja[k]] + 1 > l) l = lev_u[uja[k]] + 1;
+        lev_u[r] = l;
+        if (l + 1 > nu) nu = l + 1;
+    }
+    if (nup) *nup = nu;
+    return nl;
+}
+
+/* C_rc = A_rc - sum_{lj in L-row r} L_r,lja[lj] U_lja[lj],col (U found in U-row k), the sweep's sum */
+static void bilu_c_block(int r, int jj, int bs, const int *ja, const double *a, const int *lia, const int *lja,
+                         const double *la, const int *uia, const int *uja, const double *ua, double *Cb)
+{
+    const int bn = bs * bs, col = ja[jj];
+    double tmp[9];
+    memcpy(Cb, a + (size_t)jj * bn, bn * sizeof(double));
+    for (int lj = lia[r]; lj < lia[r + 1]; lj++) {
+        const int k = lja[lj];
+        for (int uj = uia[k]; uj < uia[k + 1]; uj++)
+            if (uja[uj] == col) {
+                blk_matmul(la + (size_t)lj * bn, ua + (size_t)uj * bn, tmp, bs);
+                for (int q = 0; q < bn; q++) Cb[q] -= tmp[q];
+                break;
+            }
+    }
+}
+
+/* Exact factors, rows in natural order (a topological order of the lower DAG): the row's L entries in
+ * ascending column (each needs the L entries of smaller columns), then its diagonal, then its U entries. */
+int orc_bilu_setup_exact(int nb, int bs, const int *ia, const int *ja, const double *a, const int *lia,
+                         const int *lja, double *la, const int *uia, const int *uja, double *ua, double *dinv)
+{
+    const int bn = bs * bs;
+    double C[9], d[9];
+    for (int r = 0; r < nb; r++) {
+        /* L entries by ascending column; pl = their position in L-row r (A's order) */
+        int done = 0, nlr = lia[r + 1] - lia[r];
+        int last = -1;
+        while (done < nlr) {
+            int best = -1, bestc = nb, pl = lia[r], bj = -1;
+            for (int jj = ia[r]; jj < ia[r + 1]; jj++) {
+                if (ja[jj] < r) {
+                    if (ja[jj] > last && ja[jj] < bestc) {
+                        bestc = ja[jj];
+                        best = pl;
+                        bj = jj;
+                    }
+                    pl++;
+                }
+            }
+            bilu_c_block(r, bj, bs, ja, a, lia, lja, la, uia, uja, ua, C);
+            blk_matmul(C, dinv + (size_t)bestc * bn, la + (size_t)best * bn, bs);
+            last = bestc;
+            done++;
+        }
+        int pu = uia[r];
+        for (int jj = ia[r]; jj < ia[r + 1]; jj++) {
+            if (ja[jj] == r) {
+                bilu_c_block(r, jj, bs, ja, a, lia, lja, la, uia, uja, ua, C);
+                diag_update(C, d, dinv + (size_t)r * bn, bs);
+            }
+        }
+        for (int jj = ia[r]; jj < ia[r + 1]; jj++) {
+            if (ja[jj] > r) {
+                bilu_c_block(r, jj, bs, ja, a, lia, lja, la, uia, uja, ua, C);
+                memcpy(ua + (size_t)(pu++) * bn, C, bn * sizeof(double));
+            }
+        }
+    }
+    return 0;
+}
+
+/* u += (I + L)(D + U) solved exactly, `ir_iters` refinement loops as the reference's: ftemp = f - A u;
+ * each loop: y by forward substitution, y_r = -(sum_k L_rk y_k) + ftemp_r; t by backward substitution,
+ * t_r = D_r^-1 y_r + D_r^-1 (-(sum_c U_rc t_c)); ftemp -= A t; u += t.  Sums in stored row order with
+ * the reference BSR product's rounding sequence. */
+int orc_bilu_solve_exact(int nb, int bs, const int *ia, const int *ja, const double *a, const int *lia,
+                         const int *lja, const double *la, const int *uia, const int *uja, const double *ua,
+                         const double *dinv, int ir_iters, const double *f, double *u)
+{
+    const int n = nb * bs, bn = bs * bs;
+    double *ft = malloc(sizeof(double) * n), *yt = malloc(sizeof(double) * n), *ut = malloc(sizeof(double) * n);
+    memcpy(ft, f, sizeof(double) * n);
+    orc_bsr_matvec(nb, bs, ia, ja, a, -1.0, u, 1.0, ft);
+    for (int it = 0; it < ir_iters; it++) {
+        for (int r = 0; r < nb; r++) {
+            double s[3] = {0.0, 0.0, 0.0};
+            for (int k = lia[r]; k < lia[r + 1]; k++)
+                for (int q = 0; q < bs; q++) {
+                    double t = s[q];
+                    for (int m = 0; m < bs; m++) t += la[(size_t)k * bn + q * bs + m] * yt[lja[k] * bs + m];
+                    s[q] = t;
+                }
+            for (int q = 0; q < bs; q++) yt[r * bs + q] = s[q] * -1.0 + ft[r * bs + q];
+        }
+        for (int r = nb - 1; r >= 0; r--) {
+            double s[3] = {0.0, 0.0, 0.0}, un[3], tq[3];
+            for (int k = uia[r]; k < uia[r + 1]; k++)
+                for (int q = 0; q < bs; q++) {
+                    double t = s[q];
+                    for (int m = 0; m < bs; m++) t += ua[(size_t)k * bn + q * bs + m] * ut[uja[k] * bs + m];
+                    s[q] = t;
+                }
+            for (int q = 0; q < bs; q++) un[q] = s[q] * -1.0;
+            const double *D = dinv + (size_t)r * bn;
+            for (int q = 0; q < bs; q++) {
+                double v = 0.0;
+                for (int m = 0; m < bs; m++) v += D[q * bs + m] * un[m];
+                tq[q] = v;
+            }
+            for (int q = 0; q < bs; q++) {
+                double v = 0.0;
+                for (int m = 0; m < bs; m++) v += D[q * bs + m] * yt[r * bs + m];
+                ut[r * bs + q] = v + tq[q];
+            }
+        }
+        orc_bsr_matvec(nb, bs, ia, ja, a, -1.0, ut, 1.0, ft);
+        for (int i = 0; i < n; i++) u[i] = u[i] + 1.0 * ut[i];
+    }
+    free(ft);
+    free(yt);
+    free(ut);
+    return 0;
+}

@@ -46,3 +46,11 @@ def test_measured_path_text_follows_the_options():
     c4 = bench.measured_path_text(bench.solver_opts(SimpleNamespace(config="c4", opt=[])), {"learned_used": False})
     assert "mixed driver's weights 1.0/0.8" in c1 and "(kept)" in c1
     assert "plain CPR's weights 0.7/0.9" in c4 and "no learned settings" in c4
+
+
+def test_both_arms_print_the_same_config():
+    """The reference arm and our arm emit identical `config` objects for a workload, so that a
+    comparison of the two lines is like for like."""
+    for cfg in ("c1", "c4"):
+        args = SimpleNamespace(config=cfg, opt=[])
+        assert bench.common_config(cfg, bench.plain_opts(args)) == bench.common_config(cfg, bench.solver_opts(args))
