@@ -126,7 +126,8 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         pressure_index (0), stage1_maxit (1), stage2_maxit (3),
  *         stage1_solver_type (1 AMG; 0 none), stage2_solver_type (2 HGS; 5 block ILU(0)
  *         correction z += BILU^-1 (r - A z) after CPR without sweeps; bilu_sweeps (3),
- *         bilu_ir_iters (5), bilu_lower_iters (5), bilu_upper_iters (5)),
+ *         bilu_ir_iters (5), bilu_lower_iters (5), bilu_upper_iters (5), bilu_exact (0; 1 exact
+ *         factors and level-scheduled substitutions, FP32 factors in the mixed path)),
  *         decouple (0 none, 1 ABF, 5 True-IMPES), consistent_rhs (0: the
  *         reference's right-hand-side arithmetic, 1: solution-preserving),
  *         smoother_order (0 exact sequential order, 1 multicolour),
@@ -201,6 +202,11 @@ JXCPR_API int jxcpr_solver_stage2_sweep(jxcpr_solver *solver, const double *b, d
 JXCPR_API int jxcpr_solver_bilu_sizes(jxcpr_solver *solver, long long *sizes);
 JXCPR_API int jxcpr_solver_bilu_factors(jxcpr_solver *solver, double *la, double *ua, double *dinv);
 JXCPR_API int jxcpr_solver_bilu_apply(jxcpr_solver *solver, const double *f, double *u, int device);
+/* With bilu_exact 1 (exact BILU(0) factors, the fixed point of the sweeps above, and level-scheduled block
+ * substitutions in place of the Jacobi iterations; no reference routine computes them in one pass): the
+ * level of each block row in the lower DAG (row r after the rows of its L entries) and in the upper DAG
+ * (after the rows of its U entries), host arrays of nb ints, and counts = {lower levels, upper levels}. */
+JXCPR_API int jxcpr_solver_bilu_levels(jxcpr_solver *solver, int *lev_l, int *lev_u, int *counts);
 
 /* Queues `sweeps` stage-2 sweeps in the fast path's own storage precision (FP64, or FP32 in the mixed
  * path) on internal vectors, asynchronously on the solver's stream (no reference counterpart): the

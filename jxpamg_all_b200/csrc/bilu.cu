@@ -297,9 +297,13 @@ void Bilu::setup(const BsrView<double> &A, cudaStream_t s) {
                                                        U.ia.get(), U.a.get());
         JX_LAUNCH_CHECK();
     };
-    diag(A.a);
-    lu(A.a);
-    if (sweeps > 0 && nb) {
+    if (exact) {
+        setup_exact(A, s);
+    } else {
+        diag(A.a);
+        lu(A.a);
+    }
+    if (!exact && sweeps > 0 && nb) {
         DevBuf<double> C((size_t)(A.nnzb > 0 ? A.nnzb : 1) * bn);
         for (int sw = 0; sw < sweeps; ++sw) {
             if (bs == 2)
@@ -330,6 +334,14 @@ void Bilu::solve(const BsrView<double> &A, const double *f, double *u, cudaStrea
     const BsrView<double> Lv = L.view(), Uv = U.view();
     copy_dev(n, f, ft.get(), s);
     bsr_spmv<double, double>(A, -1.0, u, 1.0, ft.get(), nullptr, s, false);
+    if (exact) {
+        for (int it = 0; it < ir_iters; ++it) {
+            substitute(ft.get(), yt.get(), ut.get(), s);
+            bsr_spmv<double, double>(A, -1.0, ut.get(), 1.0, ft.get(), nullptr, s, false);
+            axpy_dev(n, 1.0, ut.get(), u, s);
+        }
+        return;
+    }
     for (int it = 0; it < ir_iters; ++it) {
         JX_CUDA(cudaMemsetAsync(ut.get(), 0, sizeof(double) * n, s));
         JX_CUDA(cudaMemsetAsync(yt.get(), 0, sizeof(double) * n, s));

@@ -71,7 +71,8 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"bilu_sweeps", &p.bilu_sweeps},
                {"bilu_ir_iters", &p.bilu_ir_iters},
                {"bilu_lower_iters", &p.bilu_lower_iters},
-               {"bilu_upper_iters", &p.bilu_upper_iters}};
+               {"bilu_upper_iters", &p.bilu_upper_iters},
+               {"bilu_exact", &p.bilu_exact}};
     if (!key) return JXCPR_ERROR_ARG;
     if (!strcmp(key, "block_size")) return JXCPR_SUCCESS;  // taken from the matrix, as the reference's setup does
     if (!strcmp(key, "stage2_chunk") && v != 0 && v != 4 && v != 8 && v != 16) {
@@ -415,6 +416,24 @@ int jxcpr_solver_vcycle(jxcpr_solver *h, const double *rp, double *xp, int devic
         const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
         JX_CUDA(cudaMemcpyAsync(xp, S.cpr.xp.get(), sizeof(double) * nb, out, st));
         JX_CUDA(cudaStreamSynchronize(st));
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_bilu_levels(jxcpr_solver *h, int *lev_l, int *lev_u, int *counts) {
+    if (!h || !h->s.cpr.bilu) return JXCPR_ERROR_ARG;
+    const Bilu &B = *h->s.cpr.bilu;
+    if (!B.exact) {
+        set_error("bilu_levels: the level schedule exists with bilu_exact 1 only");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        if (counts) {
+            counts[0] = B.nlev_l;
+            counts[1] = B.nlev_u;
+        }
+        if (lev_l && B.nb) JX_CUDA(cudaMemcpy(lev_l, B.lev_l.get(), sizeof(int) * B.nb, cudaMemcpyDeviceToHost));
+        if (lev_u && B.nb) JX_CUDA(cudaMemcpy(lev_u, B.lev_u.get(), sizeof(int) * B.nb, cudaMemcpyDeviceToHost));
         return JXCPR_SUCCESS;
     });
 }

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, double 
     }
 }
 
-__global__ void summary_kernel(const GgState *st, const int *kerr, const int *aerr, double *out) {
+__global__ void summary_kernel(const GgState *st, const int *kerr, const int *aerr, const int *berr, double *out) {
     const GgState &s = *st;
     out[0] = s.iter;
     out[1] = s.converged ? 1.0 : (s.stalled ? -1.0 : 0.0);
@@ -401,7 +401,7 @@ __global__ void summary_kernel(const GgState *st, const int *kerr, const int *ae
     out[4] = (double)s.t_start;
     out[5] = (double)s.t_end;
     out[6] = s.cycles;
-    out[7] = (kerr ? *kerr : 0) + (aerr ? *aerr : 0);
+    out[7] = (kerr ? *kerr : 0) + (aerr ? *aerr : 0) + (berr ? *berr : 0);
 }
 
 // Adds a WHILE node after the nodes captured so far on s and continues the
@@ -599,7 +599,8 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         JX_LAUNCH_CHECK();
         JX_CUDA(cudaStreamEndCapture(s1, &gchk));
         c4 = launch_count();
-        summary_kernel<<<1, 1, 0, s>>>(st, kerr, S.cpr.amg.err.get(), out);
+        summary_kernel<<<1, 1, 0, s>>>(st, kerr, S.cpr.amg.err.get(),
+                                       S.cpr.bilu ? S.cpr.bilu->error_flag() : nullptr, out);
         JX_LAUNCH_CHECK();
     } catch (...) {
         end_capture_quietly(aux[1]);

@@ -110,6 +110,9 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         bilu->ir_iters = prm.bilu_ir_iters;
         bilu->lower_iters = prm.bilu_lower_iters;
         bilu->upper_iters = prm.bilu_upper_iters;
+        bilu->exact = prm.bilu_exact;
+        // the mixed path keeps the exact factors in FP32 for the substitutions
+        bilu->fp32 = prm.bilu_exact && prm.smoother_order != ORDER_EXACT && (prm.precision == 1 || prm.precision == 2);
         bilu->setup(A, s);
         amg.log.mark("bilu_setup", s);
         bres.alloc((size_t)(A.nb > 0 ? A.nb : 1) * A.bs);
@@ -734,10 +737,11 @@ GmresResult Solver::solve_once(const double *b_in, double *x_io, int device) {
         last = ggmres->result_from(sm, s, true);
         count_launches(ggmres->kernels_run(last.iterations, (int)sm[6]));
         if (sm[7] != 0.0) {
-            set_error("device wait timed out (spmv / smoother flags set)");
+            set_error("device wait timed out (spmv / smoother / BILU substitution flags set)");
             last.status = JXCPR_ERROR_DEVICE;
             kerr.zero(s);
             cpr.amg.err.zero(s);
+            if (cpr.bilu && cpr.bilu->error_flag()) JX_CUDA(cudaMemsetAsync(cpr.bilu->error_flag(), 0, sizeof(int), s));
             JX_CUDA(cudaStreamSynchronize(s));
         }
         solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -751,14 +755,18 @@ GmresResult Solver::solve_once(const double *b_in, double *x_io, int device) {
     const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     JX_CUDA(cudaMemcpyAsync(x_io, x.get(), sizeof(double) * n, out, s));
     JX_CUDA(cudaStreamSynchronize(s));
-    int kflag = 0, aflag = 0;
+    int kflag = 0, aflag = 0, bflag = 0;
     JX_CUDA(cudaMemcpy(&kflag, kerr.get(), sizeof(int), cudaMemcpyDeviceToHost));
     JX_CUDA(cudaMemcpy(&aflag, cpr.amg.err.get(), sizeof(int), cudaMemcpyDeviceToHost));
-    if (kflag || aflag) {
-        set_error("device wait timed out (spmv flag %d, smoother flag %d)", kflag, aflag);
+    int *bf = cpr.bilu ? cpr.bilu->error_flag() : nullptr;
+    if (bf) JX_CUDA(cudaMemcpy(&bflag, bf, sizeof(int), cudaMemcpyDeviceToHost));
+    if (kflag || aflag || bflag) {
+        set_error("device wait timed out (spmv flag %d, smoother flag %d, BILU substitution flag %d)", kflag, aflag,
+                  bflag);
         last.status = JXCPR_ERROR_DEVICE;
         kerr.zero(s);
         cpr.amg.err.zero(s);
+        if (bf) JX_CUDA(cudaMemsetAsync(bf, 0, sizeof(int), s));
     }
     solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return last;

@@ -43,6 +43,7 @@ struct SolverParams {
     int bilu_ir_iters = 5;
     int bilu_lower_iters = 5;
     int bilu_upper_iters = 5;
+    int bilu_exact = 0;  // 1: exact BILU(0) factors and level-scheduled triangular solves (bilu_exact.cu)
     double threshold = 1e-15;    // accepted and ignored, as in the reference
     double stage2_relax_weight = 0.7;
     double stage2_omega = 0.9;

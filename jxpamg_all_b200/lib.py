@@ -81,6 +81,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_bilu_sizes.argtypes = [P, P]
     lib.jxcpr_solver_bilu_factors.argtypes = [P, P, P, P]
     lib.jxcpr_solver_bilu_apply.argtypes = [P, P, P, c_int]
+    lib.jxcpr_solver_bilu_levels.argtypes = [P, P, P, P]
     lib.jxcpr_solver_level_features.argtypes = [P, c_int, P]
     lib.jxcpr_solver_learned_status.argtypes = [P, P]
     lib.jxcpr_solver_learned_fallbacks.argtypes = [P]

@@ -192,6 +192,13 @@ class CprGmres:
         _lib.check(self._so.jxcpr_solver_bilu_apply(self.h, _ptr(np.ascontiguousarray(f, np.float64)), _ptr(u), 0))
         return u
 
+    def bilu_levels(self):
+        """bilu_exact 1: (lower levels per block row, upper levels per block row, #lower, #upper)."""
+        lev_l, lev_u = np.zeros(self.nb, np.int32), np.zeros(self.nb, np.int32)
+        cnt = np.zeros(2, np.int32)
+        _lib.check(self._so.jxcpr_solver_bilu_levels(self.h, _ptr(lev_l), _ptr(lev_u), _ptr(cnt)))
+        return lev_l, lev_u, int(cnt[0]), int(cnt[1])
+
     def close(self):
         if getattr(self, "h", None):
             self._so.jxcpr_solver_destroy(self.h)
