@@ -229,13 +229,18 @@ JXCPR_API int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int
  * reference counterpart; the kernel a roofline measurement times with events on that stream):
  * op 0 y = A x, 1 one Chebyshev step y = c z + D^-1 A x, 2 the residual r = f - A u. */
 JXCPR_API int jxcpr_solver_level_native(jxcpr_solver *solver, int level, int op, int reps);
+/* Level `level`'s operator values as the fast path stores them (FP64, FP32, or BF16 times its block scale),
+ * widened to FP64, in the entry order of jxcpr_solver_level_matrix (host array of its nnz values); no
+ * reference counterpart.  Levels without a smoothed operator (the coarsest) return JXCPR_ERROR_ARG. */
+JXCPR_API int jxcpr_solver_level_stored_values(jxcpr_solver *solver, int level, double *values);
 /* Modelled bytes one preconditioner application of the fast path moves (every smoother pass, residual,
  * transfer, coarse solve and stage-2 sweep at its storage precision); no reference counterpart. */
 JXCPR_API int jxcpr_solver_apply_bytes(jxcpr_solver *solver, double *bytes);
 
 /* ---- fast path (smoother_order 1) inspection: no reference counterpart ---------------------
  * level_info: smoother (1 multicolour GS, 2 l1-Jacobi, 3 Chebyshev-3; 0 exact path), storage
- * (0 FP64, 1 FP32, 2 BF16 + row scale), the strength threshold the level was coarsened with and
+ * (0 FP64, 1 FP32, 2 BF16 + a power-of-two FP32 scale per 32 stored values), the strength threshold the
+ * level was coarsened with and
  * cheb[6] = {c0, c1, c2, interval low, interval high, lambda_max(D^-1 A)}.  Returns 0 or -1. */
 JXCPR_API int jxcpr_solver_level_info(jxcpr_solver *solver, int level, int *smoother, int *storage, double *theta,
                                       double *cheb);

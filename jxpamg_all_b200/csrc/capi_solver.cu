@@ -438,6 +438,26 @@ int jxcpr_solver_bilu_levels(jxcpr_solver *h, int *lev_l, int *lev_u, int *count
     });
 }
 
+int jxcpr_solver_level_stored_values(jxcpr_solver *h, int level, double *values) {
+    if (!h || !values || !h->s.cpr.ready || !h->s.cpr.fast) return JXCPR_ERROR_ARG;
+    return guarded([&] {
+        Solver &S = h->s;
+        if (level < 0 || level >= (int)S.cpr.amg.levels.size()) {
+            set_error("level_stored_values: no level %d", level);
+            return JXCPR_ERROR_ARG;
+        }
+        const long long nnz = S.cpr.amg.levels[level]->A.nnz;
+        DevBuf<double> out(nnz > 0 ? nnz : 1);
+        if (!S.cpr.fast->stored_values(level, out.get(), S.stream)) {
+            set_error("level_stored_values: level %d has no smoothed operator", level);
+            return JXCPR_ERROR_ARG;
+        }
+        if (nnz) JX_CUDA(cudaMemcpyAsync(values, out.get(), sizeof(double) * nnz, cudaMemcpyDeviceToHost, S.stream));
+        JX_CUDA(cudaStreamSynchronize(S.stream));
+        return JXCPR_SUCCESS;
+    });
+}
+
 int jxcpr_solver_level_native(jxcpr_solver *h, int level, int op, int reps) {
     if (!h || reps < 0 || op < 0 || op > 2 || !h->s.cpr.ready) return JXCPR_ERROR_ARG;
     if (!h->s.cpr.fast) {

@@ -12,7 +12,7 @@
 //   precision 1: FP32 values / vectors / accumulation throughout the
 //                preconditioner (GMRES, its SpMV, the true residual and the
 //                coarsest dense solve stay FP64);
-//   precision 2: as 1, plus BF16 values with a per-row FP32 scale on levels
+//   precision 2: as 1, plus BF16 values with a per-block FP32 scale on levels
 //                >= bf16_level;
 //   precision 3: the reference's hybrid form (src/test_bsr_cprgmres_hybrid.c:
 //                217-439): restriction, AMG and prolongation in FP32, the
@@ -50,7 +50,8 @@ enum FastSmoother { FS_COLOR_GS = 1, FS_L1_JACOBI = 2, FS_CHEB = 3 };
 // Stored row t maps to vector row perm[t] (CSR; nullptr = identity) or rows[t]
 // (sliced ELL; -1 = padding).  Segments (colour classes) are contiguous stored
 // rows [seg[c], seg[c+1]).  E values per entry (1 scalar, bs*bs blocks).
-// BF16 rows carry an FP32 scale (a = rscale * val, rscale = max |a| of the row).
+// BF16 values carry one power-of-two FP32 scale per block of 32 consecutive stored values
+// (a = bscale[k / 32] * val[k]; in sliced ELL a block is one slot of a 32-row slice).
 struct LevelMat {
     int n = 0, m = 0;
     long long nnz = 0;
@@ -68,7 +69,7 @@ struct LevelMat {
     DevBuf<double> a64;
     DevBuf<float> a32;
     DevBuf<__nv_bfloat16> a16;
-    DevBuf<float> rscale;
+    DevBuf<float> bscale;
 };
 
 // One level of the fast hierarchy (vectors in TX = double or float).
@@ -78,6 +79,7 @@ struct FastLevel {
     int smoother = FS_L1_JACOBI;  // in use
     int smoother_cfg = FS_L1_JACOBI, smoother_plain = FS_L1_JACOBI;  // configured / plain settings
     LevelMat A;          // colour classes as segments (FS_COLOR_GS) or one segment
+    const int *src_ia = nullptr;  // row pointer of the hierarchy's CSR operator (not owned)
     int last_color = -1;
     LevelMat P, R;       // interpolation from level+1 / restriction to it
     DevBuf<TX> dinv;     // 1/a_ii (GS, Chebyshev); 0 skips the row
@@ -132,6 +134,9 @@ struct FastCprBase {
     // queued on s (what a roofline measurement times): op 0 y = A x, 1 one Chebyshev step
     // (y = c z + D^-1 A x), 2 the residual r = f - A u.  Returns false if the level has no operator.
     virtual bool level_native(int level, int op, int reps, cudaStream_t s) = 0;
+    // Level l's operator values as stored (FP64, FP32, or BF16 times its block scale), widened to FP64 in
+    // the entry order of the hierarchy's CSR operator (out: device, nnz values).  False if no operator.
+    virtual bool stored_values(int level, double *out, cudaStream_t s) = 0;
     // One line per tuned operator: "name rows mean_row layout time_us".
     std::vector<std::string> tune_log;
 };

@@ -42,7 +42,7 @@ void alloc_vec(DevBuf<T> &b, long long n) {
 // ---- launch of a row operation over stored rows [r0, r1) -------------------------
 template <typename TX, int V, typename TV, class Op>
 void launch_csr(const LevelMat &M, const TV *a, const Op &op, int r0, int r1, cudaStream_t s) {
-    fk::CsrFmt<V, TV> f{M.ia.get(), M.ja.get(), a, M.rscale.get(), M.perm};
+    fk::CsrFmt<V, TV> f{M.ia.get(), M.ja.get(), a, M.bscale.get(), M.perm};
     const long long threads = (long long)(r1 - r0) * V;
     launch_dep(fk::row_kernel<fk::CsrFmt<V, TV>, Op, TX>, dim3(div_up(threads, kThreads)), dim3(kThreads), s,
                f, op, r0, r1);
@@ -54,7 +54,7 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
     with_values<TX>(M, [&](auto a) {
         using TV = typename std::remove_cv<typename std::remove_pointer<decltype(a)>::type>::type;
         if (M.sell) {
-            fk::SellFmt<TV> f{M.sp.get(), M.ja.get(), a, M.rscale.get(), M.rows.get()};
+            fk::SellFmt<TV> f{M.sp.get(), M.ja.get(), a, M.bscale.get(), M.rows.get()};
             launch_dep(fk::row_kernel<fk::SellFmt<TV>, Op, TX>, dim3(div_up(r1 - r0, kThreads)), dim3(kThreads), s,
                        f, op, r0, r1);
             return;
@@ -142,11 +142,11 @@ void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, cons
 }
 
 template <typename TV>
-void sell_fill_launch(LevelMat &M, const int *ia, const int *ja, const double *a, TV *val, float *rscale,
+void sell_fill_launch(LevelMat &M, const int *ia, const int *ja, const double *a, TV *val, float *bscale,
                       cudaStream_t s) {
     if (!M.nstored) return;
     fk::sell_fill<TV><<<div_up(M.nstored, kThreads), kThreads, 0, s>>>(M.nstored, M.rows.get(), M.sp.get(), ia, ja,
-                                                                      a, M.E, M.ja.get(), val, rscale);
+                                                                      a, M.E, M.ja.get(), val, bscale);
     JX_LAUNCH_CHECK();
 }
 
@@ -192,8 +192,8 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
             sell_fill_launch<float>(M, ia, ja, a, M.a32.get(), nullptr, s);
         } else {
             M.a16.alloc(nv);
-            M.rscale.alloc(M.nstored > 0 ? M.nstored : 1);
-            sell_fill_launch<__nv_bfloat16>(M, ia, ja, a, M.a16.get(), M.rscale.get(), s);
+            M.bscale.alloc((size_t)(slots > 0 ? slots : 1) / 32 + 1);
+            sell_fill_launch<__nv_bfloat16>(M, ia, ja, a, M.a16.get(), M.bscale.get(), s);
         }
         JX_CUDA(cudaStreamSynchronize(s));
         return;
@@ -237,9 +237,9 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
         }
     } else {
         M.a16.alloc(nv);
-        M.rscale.alloc(n > 0 ? n : 1);
-        if (n) {
-            fk::to_bf16_rows<<<div_up(n, kThreads), kThreads, 0, s>>>(n, src_ia, src_a, M.rscale.get(), M.a16.get());
+        M.bscale.alloc((size_t)(nnz > 0 ? nnz : 1) / 32 + 1);
+        if (nnz) {
+            fk::to_bf16_blocks<<<div_up(nnz, kThreads), kThreads, 0, s>>>(nnz, src_a, M.bscale.get(), M.a16.get());
             JX_LAUNCH_CHECK();
         }
     }
@@ -447,6 +447,32 @@ std::vector<int> download_ints(const int *d, int n, cudaStream_t s) {
         JX_CUDA(cudaStreamSynchronize(s));
     }
     return h;
+}
+
+// stored values back to the source CSR's entry order (inspection): sliced ELL, stored row t = row rows[t]
+template <typename TV>
+__global__ void unpack_sell_kernel(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
+                                   const int *__restrict__ src_ia, const TV *__restrict__ val,
+                                   const float *__restrict__ bsc, double *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nstored) return;
+    const int i = rows[t];
+    if (i < 0) return;
+    const long long o = sp[t >> 5] + (t & 31);
+    const int d = src_ia[i], len = src_ia[i + 1] - d;
+    for (int k = 0; k < len; ++k) out[d + k] = (double)fk::ldvs(val, bsc, o + (long long)k * 32);
+}
+
+// CSR copy: stored row t = row perm[t] (identity without perm), entries in the source order
+template <typename TV>
+__global__ void unpack_csr_kernel(int n, const int *__restrict__ perm, const int *__restrict__ ia,
+                                  const int *__restrict__ src_ia, const TV *__restrict__ val,
+                                  const float *__restrict__ bsc, double *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = perm ? perm[t] : t;
+    const int d = src_ia[i];
+    for (int k = ia[t]; k < ia[t + 1]; ++k) out[d + (k - ia[t])] = (double)fk::ldvs(val, bsc, k);
 }
 
 template <typename TX>
@@ -890,6 +916,23 @@ struct FastCpr final : FastCprBase {
         return true;
     }
 
+    bool stored_values(int level, double *out, cudaStream_t s) override {
+        if (level < 0 || level + 1 >= (int)lv.size()) return false;
+        const FastLevel<TX> &L = *lv[level];
+        const LevelMat &M = L.A;
+        if (L.n == 0 || !L.src_ia) return false;
+        with_values<TX>(M, [&](auto a) {
+            if (M.sell)
+                unpack_sell_kernel<<<div_up(M.nstored, kThreads), kThreads, 0, s>>>(
+                    M.nstored, M.rows.get(), M.sp.get(), L.src_ia, a, M.bscale.get(), out);
+            else
+                unpack_csr_kernel<<<div_up(M.n, kThreads), kThreads, 0, s>>>(M.n, M.perm, M.ia.get(), L.src_ia, a,
+                                                                             M.bscale.get(), out);
+        });
+        JX_LAUNCH_CHECK();
+        return true;
+    }
+
     double apply_bytes() const override {
         auto vb = [](int kind) { return kind == VAL_F64 ? 8.0 : (kind == VAL_F32 ? 4.0 : 2.0); };
         const double xb = sizeof(TX);
@@ -968,6 +1011,7 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
             Lv.smoother = Lv.smoother_cfg = sm;
             Lv.smoother_plain = (opt.smoother == 2) ? FS_CHEB : plain_sm;
             const CsrView<double> Av = HL.A.view();
+            Lv.src_ia = Av.ia;
             const std::string nm = "A" + std::to_string(l);
             if (sm == FS_COLOR_GS) {
                 std::vector<int> order = download_ints(HL.fwd.perm.get(), n, s);

@@ -1,7 +1,7 @@
 // Device kernels of the fast (throughput / mixed-precision) CPR path.
 //
 // Every kernel is templated on the value storage type TV (double, float or
-// __nv_bfloat16 with a per-row scale) and the vector type TX (double or float;
+// __nv_bfloat16 with a per-block scale) and the vector type TX (double or float;
 // arithmetic is done in TX).  Rows are reduced by V lanes of a warp (V a power
 // of two <= 32): lane l takes entries kb+l, kb+l+V, ... and the V partial sums
 // are combined with xor-shuffles, so every lane of a group must reach the
@@ -18,6 +18,13 @@ namespace fk {
 __device__ __forceinline__ double ldv(const double *p, long long k) { return __ldg(p + k); }
 __device__ __forceinline__ float ldv(const float *p, long long k) { return __ldg(p + k); }
 __device__ __forceinline__ float ldv(const __nv_bfloat16 *p, long long k) { return __bfloat162float(__ldg(p + k)); }
+// Value k of an operator's storage: BF16 values carry one power-of-two FP32 scale per 32 consecutive
+// stored values (bsc[k / 32]; a block scale, exact to apply), FP64 / FP32 values none.
+__device__ __forceinline__ double ldvs(const double *p, const float *, long long k) { return __ldg(p + k); }
+__device__ __forceinline__ float ldvs(const float *p, const float *, long long k) { return __ldg(p + k); }
+__device__ __forceinline__ float ldvs(const __nv_bfloat16 *p, const float *bsc, long long k) {
+    return __bfloat162float(__ldg(p + k)) * __ldg(bsc + (k >> 5));
+}
 
 template <int V, typename TA>
 __device__ __forceinline__ TA group_sum(TA v) {
@@ -29,29 +36,29 @@ __device__ __forceinline__ TA group_sum(TA v) {
 // sum_{k in [kb, ke)} a_k x_{ja_k}, reduced over the V lanes of the group.
 // Two entries per lane per trip keep more loads in flight.
 template <int V, typename TA, typename TV, typename TX>
-__device__ __forceinline__ TA row_sum(const int *__restrict__ ja, const TV *__restrict__ a, int kb, int ke,
-                                      const TX *x, int lane) {
+__device__ __forceinline__ TA row_sum(const int *__restrict__ ja, const TV *__restrict__ a, const float *bsc, int kb,
+                                      int ke, const TX *x, int lane) {
     TA s0 = 0, s1 = 0;
     int k = kb + lane;
     for (; k + V < ke; k += 2 * V) {
         const int j0 = __ldg(ja + k), j1 = __ldg(ja + k + V);
-        const TA a0 = (TA)ldv(a, k), a1 = (TA)ldv(a, k + V);
+        const TA a0 = (TA)ldvs(a, bsc, k), a1 = (TA)ldvs(a, bsc, k + V);
         s0 += a0 * (TA)x[j0];
         s1 += a1 * (TA)x[j1];
     }
-    if (k < ke) s0 += (TA)ldv(a, k) * (TA)x[__ldg(ja + k)];
+    if (k < ke) s0 += (TA)ldvs(a, bsc, k) * (TA)x[__ldg(ja + k)];
     return group_sum<V, TA>(s0 + s1);
 }
 
 // ---- matrix formats -----------------------------------------------------------
 // CSR with V lanes per row.  Stored row t maps to vector row perm[t] (perm ==
-// nullptr: identity); rscale (BF16 storage) is per stored row.
+// nullptr: identity); bscale (BF16 storage): one scale per 32 consecutive stored values.
 template <int V_, typename TV>
 struct CsrFmt {
     static constexpr int V = V_;
     const int *ia, *ja;
     const TV *a;
-    const float *rscale;
+    const float *bscale;
     const int *perm;
     __device__ __forceinline__ int row(int t) const { return perm ? __ldg(perm + t) : t; }
     template <typename TA, typename TX>
@@ -59,9 +66,8 @@ struct CsrFmt {
         const int e = live ? __ldg(ia + t + 1) : 0;
         int d = live ? __ldg(ia + t) + kstart : 0;
         if (d > e) d = e;
-        return row_sum<V, TA>(ja, a, d, e, x, lane);
+        return row_sum<V, TA>(ja, a, bscale, d, e, x, lane);
     }
-    __device__ __forceinline__ float scale(int t) const { return rscale ? __ldg(rscale + t) : 1.0f; }
 };
 
 // Sliced ELL: 32-row slices stored slot-major, entry k of stored row t at
@@ -74,7 +80,7 @@ struct SellFmt {
     const long long *sp;
     const int *col;
     const TV *a;
-    const float *rscale;
+    const float *bscale;  // BF16: one scale per 32 stored values (one slot of a slice)
     const int *rows;
     __device__ __forceinline__ int row(int t) const { return __ldg(rows + t); }
     template <typename TA, typename TX>
@@ -89,7 +95,8 @@ struct SellFmt {
             const long long p = o + (long long)k * 32;
             const int j0 = __ldg(col + p), j1 = __ldg(col + p + 32), j2 = __ldg(col + p + 64),
                       j3 = __ldg(col + p + 96);
-            const TA a0 = (TA)ldv(a, p), a1 = (TA)ldv(a, p + 32), a2 = (TA)ldv(a, p + 64), a3 = (TA)ldv(a, p + 96);
+            const TA a0 = (TA)ldvs(a, bscale, p), a1 = (TA)ldvs(a, bscale, p + 32), a2 = (TA)ldvs(a, bscale, p + 64),
+                     a3 = (TA)ldvs(a, bscale, p + 96);
             s0 += a0 * (TA)x[j0];
             s1 += a1 * (TA)x[j1];
             s2 += a2 * (TA)x[j2];
@@ -97,11 +104,10 @@ struct SellFmt {
         }
         for (; k < w; ++k) {
             const long long p = o + (long long)k * 32;
-            s0 += (TA)ldv(a, p) * (TA)x[__ldg(col + p)];
+            s0 += (TA)ldvs(a, bscale, p) * (TA)x[__ldg(col + p)];
         }
         return (s0 + s1) + (s2 + s3);
     }
-    __device__ __forceinline__ float scale(int t) const { return rscale ? __ldg(rscale + t) : 1.0f; }
 };
 
 // ---- row operations (prologue loads issued before the row sum) -----------------
@@ -214,10 +220,7 @@ __global__ void __launch_bounds__(256) row_kernel(Fmt fmt, Op op, int r0, int r1
     if (own) op.load(i, pre);
     TX s = 0;
     if (op.need_sum()) s = fmt.template sum<TX, TX>(t, i >= 0, lane, op.x(), Op::kstart);
-    if (own) {
-        if (fmt.rscale) s *= (TX)fmt.scale(t);
-        op.store(i, s, pre);
-    }
+    if (own) op.store(i, s, pre);
 }
 
 template <typename TX>
@@ -583,29 +586,46 @@ __device__ __forceinline__ __nv_bfloat16 cvt_val<__nv_bfloat16>(double v, double
     return __float2bfloat16_rn((float)(v / sc));
 }
 
-// Stored row t receives the entries of CSR/BSR row rows[t] (E values per
-// entry, E = 1 or bs*bs) in slot-major order; rscale != nullptr: BF16 row scale.
+// The power of two 2^e with max/2^e in [0.5, 1) (1 for max = 0): the block scale of BF16 storage.
+__device__ __forceinline__ double pow2_scale(double m) {
+    if (!(m > 0.0)) return 1.0;
+    int e = 0;
+    frexp(m, &e);
+    return ldexp(1.0, e);
+}
+
+// max over the 32 lanes of a warp (every lane takes part)
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Stored row t receives the entries of CSR/BSR row rows[t] (E values per entry, E = 1 or bs*bs) in
+// slot-major order.  A warp covers one 32-row slice, so each slot of the slice is one block of 32
+// stored values; bscale != nullptr (BF16, E = 1): that block's power-of-two scale goes to
+// bscale[p / 32] and the values are stored divided by it.
 template <typename TV>
 __global__ void sell_fill(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
                           const int *__restrict__ ia, const int *__restrict__ ja, const double *__restrict__ a,
-                          int E, int *__restrict__ col, TV *__restrict__ val, float *__restrict__ rscale) {
+                          int E, int *__restrict__ col, TV *__restrict__ val, float *__restrict__ bscale) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nstored) return;
-    const int i = rows[t];
+    if (t >= ((nstored + 31) & ~31)) return;  // whole slices: every lane of a slice's warp stays
+    const bool in = t < nstored;
+    const int i = in ? rows[t] : -1;
     const long long b0 = sp[t >> 5], b1 = sp[(t >> 5) + 1];
     const int w = (int)((b1 - b0) >> 5);
     const long long o = b0 + (t & 31);
     const int d = i >= 0 ? ia[i] : 0;
     const int len = i >= 0 ? ia[i + 1] - d : 0;
-    double sc = 1.0;
-    if (rscale) {
-        double m = 0.0;
-        for (long long q = (long long)d * E; q < (long long)(d + len) * E; ++q) m = fmax(m, fabs(a[q]));
-        sc = m > 0.0 ? m : 1.0;
-        rscale[t] = (float)sc;
-    }
     for (int k = 0; k < w; ++k) {
         const long long p = o + (long long)k * 32;
+        double sc = 1.0;
+        if (bscale) {  // warp-uniform
+            sc = pow2_scale(warp_max(k < len ? fabs(a[(long long)(d + k) * E]) : 0.0));
+            if ((t & 31) == 0) bscale[p >> 5] = (float)sc;
+        }
+        if (!in) continue;
         if (k < len) {
             col[p] = ja[d + k];
             for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(a[(long long)(d + k) * E + q], sc);
@@ -622,16 +642,16 @@ __global__ void to_f32(long long n, const double *__restrict__ in, float *__rest
     if (i < n) out[i] = (float)in[i];
 }
 
-// BF16 values scaled per row by max |a_ij| (kept in FP32).
-__global__ void to_bf16_rows(int n, const int *__restrict__ ia, const double *__restrict__ a,
-                             float *__restrict__ rscale, __nv_bfloat16 *__restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double m = 0.0;
-    for (int k = ia[i]; k < ia[i + 1]; ++k) m = fmax(m, fabs(a[k]));
-    const double sc = m > 0.0 ? m : 1.0;
-    rscale[i] = (float)sc;
-    for (int k = ia[i]; k < ia[i + 1]; ++k) out[k] = __float2bfloat16_rn((float)(a[k] / sc));
+// BF16 values of a CSR operator, one power-of-two FP32 scale per 32 consecutive stored values (a warp
+// per block).
+__global__ void to_bf16_blocks(long long nnz, const double *__restrict__ a, float *__restrict__ bscale,
+                               __nv_bfloat16 *__restrict__ out) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((k & ~31LL) >= nnz) return;  // whole warps
+    const double v = k < nnz ? a[k] : 0.0;
+    const double sc = pow2_scale(warp_max(fabs(v)));
+    if ((k & 31) == 0) bscale[k >> 5] = (float)sc;
+    if (k < nnz) out[k] = __float2bfloat16_rn((float)(v / sc));
 }
 
 // 1 / a_ii where the diagonal is the first stored entry, else 0 (row skipped).

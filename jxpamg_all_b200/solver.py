@@ -192,6 +192,13 @@ class CprGmres:
         _lib.check(self._so.jxcpr_solver_bilu_apply(self.h, _ptr(np.ascontiguousarray(f, np.float64)), _ptr(u), 0))
         return u
 
+    def level_stored_values(self, lev):
+        """Level lev's operator values as the fast path stores them, in level_matrix's entry order."""
+        nnz = self.level_sizes(lev, 0)[2]
+        out = np.zeros(max(nnz, 1))
+        _lib.check(self._so.jxcpr_solver_level_stored_values(self.h, lev, _ptr(out)))
+        return out[:nnz]
+
     def bilu_levels(self):
         """bilu_exact 1: (lower levels per block row, upper levels per block row, #lower, #upper)."""
         lev_l, lev_u = np.zeros(self.nb, np.int32), np.zeros(self.nb, np.int32)

@@ -125,3 +125,21 @@ def test_c1_mixed_measured_path(c1):
     it, err = _fast_solve(c1, bench.SOLVER_OPTS, fewer_ok=True)
     assert err <= 1e-2, err
     print(f"mixed + learned path: {it} iterations, x vs the reference's FP64 solution {err:.2e}")
+
+
+def test_c1_bf16_coarse_levels_path(c1):
+    """The BF16 form (coarse levels in BF16 with per-block scales, FP32 level 0 and stage 2, FP64 GMRES and
+    coarsest solve): converges to the true FP64 residual; its iterations and its distance from the
+    reference's FP64 solution are stated."""
+    import bench
+
+    s, a, b, g = c1
+    G = CprGmres(**dict(bench.SOLVER_OPTS, precision=2)).setup(s.ia, s.ja, s.a, s.block_size)
+    x, it, rel, conv = G.solve(s.b)
+    G.close()
+    assert conv and rel <= 1e-6
+    assert _true_rel_res(s, a, b, x) <= 1e-6 * (1 + 1e-9)
+    err = _x_error(x, g)
+    assert err <= 1e-2, err
+    print(f"BF16 coarse levels: {it} iterations (reference {int(g['gmres_iters'])}), x vs the reference's FP64 "
+          f"solution {err:.2e}")

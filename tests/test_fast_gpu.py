@@ -254,3 +254,30 @@ def test_stage2_sweep_matches_colour_ordered_hgs(systems, name, opt):
             x[i] = (1 - w * om) * vt[i] + w * out
     want = x.reshape(-1)
     assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("name", ["c0", "tiny3", "slab_small"])
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_stored_level_values_against_fp64(systems, name, precision):
+    """Every smoothed level's operator as the fast path stores it, against the FP64 hierarchy: FP64 exact,
+    FP32 within FP32 rounding, BF16 (precision 2, levels >= 1) within BF16 rounding of each value -- its
+    per-block power-of-two FP32 scale is exact, so each entry is the BF16 rounding of a_ij."""
+    s = systems(name) if name != "slab_small" else synth.reservoir_system(30, 110, 12, seed=21, phases=2,
+                                                                         channelised_layers=7)
+    G = CprGmres(**dict(BASE, precision=precision, fast_smoother=1, flexible=1)).setup(s.ia, s.ja, s.a,
+                                                                                       s.block_size)
+    for lev in range(G.num_levels() - 1):
+        ia, ja, a, _ = G.level_matrix(lev, 0)
+        got = G.level_stored_values(lev)
+        kind = G.level_info(lev)["storage"]
+        assert kind == (0 if precision == 0 else (2 if precision == 2 and lev >= 1 else 1))
+        if kind == 0:
+            assert np.array_equal(got, a)
+        elif kind == 1:
+            assert np.array_equal(got, a.astype(np.float32).astype(np.float64))
+        else:
+            assert np.all(np.abs(got - a) <= 2.0 ** -8 * np.abs(a)), lev
+            # the BF16 rounding of each value: at most 8 significant bits
+            m, _ = np.frexp(got[got != 0])
+            assert np.all(np.abs(m * 256 - np.round(m * 256)) == 0)
+    G.close()
