@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_LIB = os.path.join(HERE, "liborc.so")
 REF_LIB = os.path.join(HERE, "_ref", "libjxf_ref64.so")
-REF_TREE = "/root/reference"
+# the reference source tree the checker library is compiled from (build step only)
+REF_TREE = os.environ.get("JXF_REFERENCE_TREE", "")
 
 _orc = None
 _ref = None
@@ -36,8 +37,9 @@ def _p(a):
 def build(reference: bool = True, jobs: int = 8) -> None:
     """Compile the restatement; also the reference library when its tree exists."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if reference and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-f", os.path.join(HERE, "ref.mk"), f"REF={REF_TREE}", f"-j{jobs}"],
+    tree = os.environ.get("JXF_REFERENCE_TREE", REF_TREE)
+    if reference and tree and os.path.isdir(tree):
+        subprocess.run(["make", "-s", "-f", os.path.join(HERE, "ref.mk"), f"REF={tree}", f"-j{jobs}"],
                        check=True, cwd=os.path.dirname(HERE))
 
 
