@@ -145,9 +145,9 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         levels needing more colours use l1-Jacobi), flexible (0), graphs (1),
  *         graph_gmres (0), orthog (0 modified, 1 one-pass classical
  *         Gram-Schmidt), autotune (1; 2 shared per shape class), stage2_lanes
- *         (4: CSR stage 2 without autotuning), stage2_chunk (8: stage 2 visits
+ *         (4: CSR stage 2 without autotuning), stage2_chunk (4: stage 2 visits
  *         chunks of this many consecutive block rows in natural order, the
- *         chunks coloured for parallelism; 4 or 16 also accepted; 0: the
+ *         chunks coloured for parallelism; 8 or 16 also accepted; 0: the
  *         level-0 colour order), learned_fallback (1: the probe
  *         and the stall guard may replace the learned settings),
  *         record_features (0), thermal (0)
@@ -252,10 +252,9 @@ JXCPR_API int jxcpr_solver_level_features(jxcpr_solver *solver, int level, float
  * hierarchy, modelled bytes per GMRES iteration with each}.  The setup keeps the learned settings
  * unless their residual reduction per byte is worse. */
 JXCPR_API int jxcpr_solver_learned_status(jxcpr_solver *solver, double *out);
-/* Solves since the last setup in which the learned settings stalled (no convergence within three times
- * the iterations the probe's residual reduction predicts, and at least that plus one restart cycle) and
- * the plain preconditioner (default strength thresholds, plain smoothers) was built in their place for
- * the rest of the solve and for later solves.  When the setup probe rejects the learned settings, the
+/* Solves since the last setup in which the learned settings stalled (a full restart cycle reduced the
+ * residual by less than a factor 10) and the plain preconditioner (default strength thresholds, plain
+ * smoothers) was built in their place for the rest of the solve and for later solves.  When the setup probe rejects the learned settings, the
  * same plain preconditioner is built at once (learned_status reports them unused). */
 JXCPR_API int jxcpr_solver_learned_fallbacks(jxcpr_solver *solver);
 

@@ -96,7 +96,7 @@ struct FastOptions {
     int smoother = 0;       // 0 colour GS / l1-Jacobi, 1 Chebyshev-3 on the l1-Jacobi levels, 2 on every level
     double cheb_lower = 0.3, cheb_upper = 1.1;  // interval [lower, upper] * lambda_max(D^-1 A)
     int stage2_lanes = 4;      // CSR stage 2 (small systems): lanes per block row
-    int stage2_chunk = 8;      // stage 2 in chunk order (chunks of this many consecutive block rows; 0: the
+    int stage2_chunk = 4;      // stage 2 in chunk order (chunks of this many consecutive block rows; 0: the
                                // level-0 colour order)
     int sell_min_rows = 16384; // without autotuning: sliced ELL for operators with at least this many rows ...
     double sell_max_mean = 40; // ... and at most this mean row length

@@ -9,6 +9,7 @@
 #include <numeric>
 #include <map>
 #include <mutex>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -250,8 +251,12 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
 // consecutive rows, -1 padding, colour segments `seg` on slice boundaries), sliced ELL without the
 // length sort, so that every chunk keeps its rows in order at lanes 0..chunk-1 of its slice part.
 void build_chunk_mat(int n, long long nnz, int E, const int *ia, const int *ja, const double *a, int kind,
-                     const std::vector<int> &order, const std::vector<int> &seg, int chunk, LevelMat &M,
-                     cudaStream_t s) {
+                     const std::vector<int> &order, const std::vector<int> &seg, int chunk, const int *cls_dev,
+                     LevelMat &M, cudaStream_t s) {
+    if (n >= (1 << 30)) {
+        set_error("stage 2 in chunk order: %d block rows exceed the 30-bit column words", n);
+        throw std::invalid_argument("chunk order size");
+    }
     M.n = n;
     M.m = n;
     M.nnz = nnz;
@@ -287,6 +292,11 @@ void build_chunk_mat(int n, long long nnz, int E, const int *ia, const int *ja, 
     } else {
         M.a32.alloc(nv);
         sell_fill_launch<float>(M, ia, ja, a, M.a32.get(), nullptr, s);
+    }
+    if (M.nstored) {
+        fk::chunk_col_flags<<<div_up(M.nstored, kThreads), kThreads, 0, s>>>(
+            M.nstored, M.rows.get(), M.sp.get(), ia, cls_dev, chunk, reinterpret_cast<unsigned *>(M.ja.get()));
+        JX_LAUNCH_CHECK();
     }
     JX_CUDA(cudaStreamSynchronize(s));
 }
@@ -722,7 +732,7 @@ struct FastCpr final : FastCprBase {
             const int grid = div_up(r1 - r0, kThreads);
 #define JX_HGS_CHUNK(BSV, CHV)                                                                              \
     launch_dep(fk::hgs_chunk<BSV, CHV, TV, TAC, TXV>, dim3(grid), dim3(kThreads), s, r0, r1, M.sp.get(),     \
-               M.ja.get(), a, M.rows.get(), r, z, vtp, w, om, plain, so)
+               reinterpret_cast<const unsigned *>(M.ja.get()), a, M.rows.get(), r, z, vtp, w, om, plain, so.save)
             if (bs == 2) {
                 if (M.chunk == 4) JX_HGS_CHUNK(2, 4);
                 else if (M.chunk == 16) JX_HGS_CHUNK(2, 16);
@@ -1086,7 +1096,8 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
         F->st2_cls.alloc(A.nb);
         F->st2_cls.upload(cls.data(), A.nb, s);
         const int kind = (fp64 || opt.precision == 3) ? VAL_F64 : VAL_F32;
-        build_chunk_mat(A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, ord, sg, opt.stage2_chunk, F->st2, s);
+        build_chunk_mat(A.nb, A.nnzb, A.bs * A.bs, A.ia, A.ja, A.a, kind, ord, sg, opt.stage2_chunk,
+                        F->st2_cls.get(), F->st2, s);
         char line[200];
         snprintf(line, sizeof line, "stage2 rows %d blocks/row %.1f layout chunk%d colours %d", A.nb,
                  (double)A.nnzb / A.nb, opt.stage2_chunk, (int)sg.size() - 1);

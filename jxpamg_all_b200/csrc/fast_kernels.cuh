@@ -453,18 +453,59 @@ __global__ void __launch_bounds__(256) hgs_sell(int r0, int r1, const long long 
 // order, i.e. the block update of hgs_color in that sequential order.  Storage: sliced ELL with each
 // colour a run of whole chunks, CH-aligned inside the 32-row slices (lane p of a chunk holds its row
 // p; padding rows -1), rows not sorted by length.
-//   Phase 1, every row at once: the entries outside the row's chunk (earlier colours: current value
-//   and saved start value; later colours: the start value), and the in-chunk entries of higher
-//   index (not updated yet: start value).  Of an in-chunk entry of lower index j only the start-value
-//   term -(1 - omega) A_ij vt_j is added; the first such entry is kept in registers.
-//   Phase 2, CH steps: at step r lane r of every chunk solves its block and writes x; the new value
-//   is shuffled to the chunk's other lanes, whose rows coupled to it add A_ij x_j (the kept entry, or
-//   a re-scan of the row for any further in-chunk lower entry).
+//   Phase 1, every row at once: D_i^-1, and the sum over the entries outside the row's chunk
+//   (earlier colours: current value and saved start value; later colours: the start value) and over
+//   its in-chunk entries of higher index (not updated yet: the start value); of an in-chunk entry of
+//   lower index j only the start-value term -(1 - omega) A_ij vt_j.  Then u_i = D_i^-1 (omega b_i -
+//   sum) and, for the first in-chunk lower entry, G = D_i^-1 A_ij.
+//   Phase 2, CH steps: at step r lane r of every chunk forms out = u - (sum of G x_j(new)), updates
+//   and writes x; the new value is shuffled to the chunk's other lanes, whose rows coupled to it add
+//   G x_j (the kept entry; any further in-chunk lower entry is re-read and multiplied by D_i^-1).
+//   The chain from one row to the next is one shuffle and a BS x BS product.
+template <int BS, typename TA>
+__device__ __forceinline__ void block_inverse(const TA D[BS * BS], TA Di[BS * BS]) {
+    if (BS == 2) {
+        const TA det = D[0] * D[3] - D[1] * D[2];
+        const TA inv = det != (TA)0 ? (TA)1 / det : (TA)0;
+        Di[0] = D[3] * inv;
+        Di[1] = -D[1] * inv;
+        Di[2] = -D[2] * inv;
+        Di[3] = D[0] * inv;
+    } else {
+        const TA c00 = D[4] * D[8] - D[5] * D[7], c01 = D[5] * D[6] - D[3] * D[8], c02 = D[3] * D[7] - D[4] * D[6];
+        const TA det = D[0] * c00 + D[1] * c01 + D[2] * c02;
+        const TA inv = det != (TA)0 ? (TA)1 / det : (TA)0;
+        const TA c10 = D[2] * D[7] - D[1] * D[8], c11 = D[0] * D[8] - D[2] * D[6], c12 = D[1] * D[6] - D[0] * D[7];
+        const TA c20 = D[1] * D[5] - D[2] * D[4], c21 = D[2] * D[3] - D[0] * D[5], c22 = D[0] * D[4] - D[1] * D[3];
+        Di[0] = c00 * inv; Di[1] = c10 * inv; Di[2] = c20 * inv;
+        Di[3] = c01 * inv; Di[4] = c11 * inv; Di[5] = c21 * inv;
+        Di[6] = c02 * inv; Di[7] = c12 * inv; Di[8] = c22 * inv;
+    }
+}
+
+template <int BS, typename TA>
+__device__ __forceinline__ void block_matvec(const TA M[BS * BS], const TA v[BS], TA out[BS]) {
+#pragma unroll
+    for (int q = 0; q < BS; ++q) {
+        TA t = 0;
+#pragma unroll
+        for (int m = 0; m < BS; ++m) t += M[q * BS + m] * v[m];
+        out[q] = t;
+    }
+}
+
+// Column words of the chunk-ordered stage-2 matrix: the column in the low 30 bits, bit 30 set when the
+// neighbour's colour comes earlier in the sweep (its start value is in vt), bit 31 when it lies in the
+// row's own chunk.  The sweep order is fixed at setup, so the relation is stored, not looked up.
+constexpr unsigned kChunkColMask = 0x3fffffffu, kChunkEarlier = 1u << 30, kChunkSame = 1u << 31;
+
+// FP32 arithmetic: at least 5 blocks of 256 threads per SM (<= 51 registers), so that enough rows'
+// loads are in flight; FP64: 3 (<= 85 registers)
 template <int BS, int CH, typename TV, typename TA, typename TXV>
-__global__ void __launch_bounds__(256) hgs_chunk(int r0, int r1, const long long *__restrict__ sp,
-                                                 const int *__restrict__ col, const TV *__restrict__ a,
+__global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0, int r1, const long long *__restrict__ sp,
+                                                 const unsigned *__restrict__ col, const TV *__restrict__ a,
                                                  const int *__restrict__ rows, const TXV *__restrict__ b,
-                                                 TXV *x, TXV *vt, TA w, TA omega, int plain, SweepOrder so) {
+                                                 TXV *x, TXV *vt, TA w, TA omega, int plain, int save) {
     static_assert(32 % CH == 0, "chunks tile the 32-row slices");
     grid_dep_wait();
     const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -474,32 +515,35 @@ __global__ void __launch_bounds__(256) hgs_chunk(int r0, int r1, const long long
     const bool live = i >= 0;
     const int cbase = i - p;  // first row of the chunk (row i sits at lane p of its chunk)
     const TA omo = (TA)1 - omega;
-    TA rhs[BS], xv[BS], D[BS * BS], acc[BS], K[BS * BS];
+    TA xv[BS], Di[BS * BS], u[BS], G[BS * BS];
     int kq = -1;            // chunk position of the kept in-chunk lower entry
     unsigned lowmask = 0u;  // chunk positions of every in-chunk lower entry
     long long o = 0;
     int wd = 0;
 #pragma unroll
-    for (int q = 0; q < BS; ++q) acc[q] = 0;
+    for (int q = 0; q < BS * BS; ++q) G[q] = 0;
 #pragma unroll
-    for (int q = 0; q < BS * BS; ++q) K[q] = 0;
+    for (int q = 0; q < BS; ++q) u[q] = xv[q] = 0;
     if (live) {
         const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
         wd = (int)((b1 - b0) >> 5);
         o = b0 + (t & 31);
+        TA rhs[BS], acc[BS], D[BS * BS], K[BS * BS];
 #pragma unroll
         for (int q = 0; q < BS; ++q) {
             rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
             xv[q] = (TA)x[(long long)i * BS + q];
+            acc[q] = 0;
         }
+#pragma unroll
+        for (int q = 0; q < BS * BS; ++q) K[q] = 0;
         load_block<BS, TV, TA>(a, o, D);
-        for (int k = 1; k < wd; ++k) {
-            const long long pk = o + (long long)k * 32;
-            const int j = __ldg(col + pk);
-            TA B[BS * BS], c[BS];
-            load_block<BS, TV, TA>(a, pk, B);
-            const int dq = j - cbase;
-            if (dq >= 0 && dq < CH) {
+        // one off-diagonal entry: its contribution c (A_ij c added to acc) and the in-chunk bookkeeping
+        auto entry = [&](unsigned cw, const TA B[BS * BS]) {
+            const int j = (int)(cw & kChunkColMask);
+            TA c[BS];
+            if (cw & kChunkSame) {
+                const int dq = j - cbase;
                 if (dq > p) {  // later in the chunk: its start value
 #pragma unroll
                     for (int m = 0; m < BS; ++m) {
@@ -517,36 +561,74 @@ __global__ void __launch_bounds__(256) hgs_chunk(int r0, int r1, const long long
                     for (int m = 0; m < BS; ++m) c[m] = plain ? (TA)0 : -omo * (TA)x[(long long)j * BS + m];
                 }
             } else {
+                const bool earlier = (cw & kChunkEarlier) != 0u;
 #pragma unroll
                 for (int m = 0; m < BS; ++m) {
-                    const TA xj = (TA)x[(long long)j * BS + m];
-                    c[m] = plain ? xj : xj - omo * start_value<TA, TXV>(x, vt, (long long)j * BS + m, j, so);
+                    const long long oj = (long long)j * BS + m;
+                    const TA xj = (TA)x[oj];
+                    c[m] = plain ? xj : xj - omo * (earlier ? (TA)__ldg(vt + oj) : xj);
                 }
             }
 #pragma unroll
             for (int q = 0; q < BS; ++q)
 #pragma unroll
                 for (int m = 0; m < BS; ++m) acc[q] += B[q * BS + m] * c[m];
+        };
+        int k = 1;
+        for (; k + 3 < wd; k += 4) {
+            const long long p0 = o + (long long)k * 32;
+            unsigned cw[4];
+            TA B[4][BS * BS];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                cw[e] = __ldg(col + p0 + 32 * e);
+                load_block<BS, TV, TA>(a, p0 + 32 * e, B[e]);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) entry(cw[e], B[e]);
+        }
+        for (; k < wd; ++k) {
+            const long long p0 = o + (long long)k * 32;
+            TA B0[BS * BS];
+            load_block<BS, TV, TA>(a, p0, B0);
+            entry(__ldg(col + p0), B0);
+        }
+        block_inverse<BS, TA>(D, Di);
+        TA r2[BS];
+#pragma unroll
+        for (int q = 0; q < BS; ++q) r2[q] = (plain ? (TA)1 : omega) * rhs[q] - acc[q];
+        block_matvec<BS, TA>(Di, r2, u);
+        if (kq >= 0) {
+#pragma unroll
+            for (int q = 0; q < BS; ++q)
+#pragma unroll
+                for (int m = 0; m < BS; ++m) {
+                    TA g = 0;
+#pragma unroll
+                    for (int l = 0; l < BS; ++l) g += Di[q * BS + l] * K[l * BS + m];
+                    G[q * BS + m] = g;
+                }
         }
     }
-    __syncwarp();  // every lane has read its chunk's start values before any lane writes
     const TA prod = (TA)1 - w * omega;
-    TA xn[BS];
+    TA gx[BS];    // sum of G x_j(new) over the row's in-chunk lower entries
+    TXV mine[BS];  // this row's new value, written after the chunk is done
 #pragma unroll
-    for (int q = 0; q < BS; ++q) xn[q] = 0;
+    for (int q = 0; q < BS; ++q) {
+        gx[q] = 0;
+        mine[q] = 0;
+    }
 #pragma unroll 1
     for (int r = 0; r < CH; ++r) {
-        if (live && p == r) {
-            TA r2[BS], out[BS];
+        TA xn[BS];
 #pragma unroll
-            for (int q = 0; q < BS; ++q) r2[q] = (plain ? (TA)1 : omega) * rhs[q] - acc[q];
-            block_solve<BS, TA>(D, r2, out);
+        for (int q = 0; q < BS; ++q) xn[q] = 0;
+        if (live && p == r) {
 #pragma unroll
             for (int q = 0; q < BS; ++q) {
-                const TXV nv = plain ? (TXV)out[q] : (TXV)(prod * xv[q] + w * out[q]);
-                if (!plain && so.save) vt[(long long)i * BS + q] = (TXV)xv[q];
-                x[(long long)i * BS + q] = nv;
-                xn[q] = (TA)nv;
+                const TA out = u[q] - gx[q];
+                mine[q] = plain ? (TXV)out : (TXV)(prod * xv[q] + w * out);
+                xn[q] = (TA)mine[q];
             }
         }
         TA bx[BS];
@@ -557,20 +639,49 @@ __global__ void __launch_bounds__(256) hgs_chunk(int r0, int r1, const long long
 #pragma unroll
                 for (int q = 0; q < BS; ++q)
 #pragma unroll
-                    for (int m = 0; m < BS; ++m) acc[q] += K[q * BS + m] * bx[m];
+                    for (int m = 0; m < BS; ++m) gx[q] += G[q * BS + m] * bx[m];
             } else {
                 for (int k = 1; k < wd; ++k) {
                     const long long pk = o + (long long)k * 32;
-                    if (__ldg(col + pk) != cbase + r) continue;
-                    TA B[BS * BS];
+                    if ((int)(__ldg(col + pk) & kChunkColMask) != cbase + r) continue;
+                    TA B[BS * BS], v[BS], dv[BS];
                     load_block<BS, TV, TA>(a, pk, B);
+                    block_matvec<BS, TA>(B, bx, v);
+                    block_matvec<BS, TA>(Di, v, dv);
 #pragma unroll
-                    for (int q = 0; q < BS; ++q)
-#pragma unroll
-                        for (int m = 0; m < BS; ++m) acc[q] += B[q * BS + m] * bx[m];
+                    for (int q = 0; q < BS; ++q) gx[q] += dv[q];
                 }
             }
         }
+    }
+    // every lane of the warp has read its chunk's start values in phase 1 (before the shuffles above)
+    if (live) {
+#pragma unroll
+        for (int q = 0; q < BS; ++q) {
+            if (!plain && save) vt[(long long)i * BS + q] = (TXV)xv[q];
+            x[(long long)i * BS + q] = mine[q];
+        }
+    }
+}
+
+// Column words of the chunk-ordered stage-2 matrix (see kChunkSame): stored row t = block row rows[t]
+// of colour cls[rows[t]]; the relation of each stored neighbour to the row goes into its top bits.
+__global__ void chunk_col_flags(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
+                                const int *__restrict__ ia, const int *__restrict__ cls, int chunk,
+                                unsigned *__restrict__ col) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nstored) return;
+    const int i = rows[t];
+    if (i < 0) return;
+    const long long o = sp[t >> 5] + (t & 31);
+    const int len = ia[i + 1] - ia[i], ci = cls[i];
+    for (int k = 0; k < len; ++k) {
+        const long long p = o + (long long)k * 32;
+        const int j = (int)col[p];
+        unsigned f = 0u;
+        if (j / chunk == i / chunk) f = kChunkSame;
+        else if (cls[j] < ci) f = kChunkEarlier;
+        col[p] = (unsigned)j | f;
     }
 }
 

@@ -116,9 +116,9 @@ __global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const
         s.normdown = rn;
         norms[0] = rn;
     }
-    // stall rule: a full cycle that reduced the true residual by less than stall^k
+    // stall rule: a full cycle whose true residual ratio (end / start) stayed above P.stall
     const int ci = s.iter - s.iter0;
-    const bool stalled = P.stall > 0.0 && s.cycles > 1 && ci >= P.k && rn > s.r_norm * pow(P.stall, (double)ci);
+    const bool stalled = P.stall > 0.0 && s.cycles > 1 && ci >= P.k && rn > s.r_norm * P.stall;
     s.r_norm = rn;
     s.iter0 = s.iter;
     if (!done) {
@@ -527,7 +527,7 @@ void GraphGmres::prepare(Solver &S) {
     P.tol = prm.tol;
     P.a_tol = prm.a_tol;
     P.convfac = prm.convfac_threshold;
-    P.stall = prm.stall_factor;
+    P.stall = prm.stall_ratio;
     JX_CUDA(cudaStreamSynchronize(s));
     reset_graph();
 }
@@ -535,7 +535,7 @@ void GraphGmres::prepare(Solver &S) {
 bool GraphGmres::matches(const SolverParams &prm) const {
     return prm.k_dim == P.k && prm.max_iter == P.max_iter && prm.min_iter == P.min_iter &&
            prm.is_check_restarted == P.check_restarted && prm.tol == P.tol && prm.a_tol == P.a_tol &&
-           prm.convfac_threshold == P.convfac && prm.stall_factor == P.stall;
+           prm.convfac_threshold == P.convfac && prm.stall_ratio == P.stall;
 }
 
 void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {

@@ -531,9 +531,8 @@ GmresResult Gmres::solve(const BsrView<double> &A, CprPrecond *M, const double *
             }
         }
         if (iter > 1 && conv_factor > prm.convfac_threshold) break;
-        // stall rule: a full cycle that reduced the residual by less than stall_factor^k
-        if (prm.stall_factor > 0.0 && i == k_dim && iter < prm.max_iter &&
-            r_norm > cycle_r0 * pow(prm.stall_factor, (double)k_dim)) {
+        // stall rule: a full cycle whose residual ratio (end / start) stayed above stall_ratio
+        if (prm.stall_ratio > 0.0 && i == k_dim && iter < prm.max_iter && r_norm > cycle_r0 * prm.stall_ratio) {
             res.stalled = 1;
             break;
         }
@@ -673,16 +672,18 @@ void Solver::rebuild_plain(cudaStream_t s) {
 }
 
 // Learned settings are kept by a short probe at setup.  The full solve then runs with a stall
-// rule: a restart cycle of k iterations that reduces the residual by less than a third (in
-// logarithm) of what the probe's per-iteration factor predicts ends it early.  The plain
-// preconditioner (default thresholds, plain smoothers) is then built in place of the learned one
-// and GMRES continues from the current iterate with the remaining iterations.
+// rule: a full restart cycle of k iterations that reduces the residual by less than a factor
+// 1 / kStallCycleRatio ends it early (the probe's 8 iterations measure the fast early reduction and
+// cannot predict a stall; a learned hierarchy that stalls does so within its first cycle).  The plain
+// preconditioner (default thresholds, plain smoothers) is then built in place of the learned one and
+// GMRES continues from the current iterate with the remaining iterations.
+static constexpr double kStallCycleRatio = 0.1;
 GmresResult Solver::solve(const double *b_in, double *x_io, int device) {
     const bool guard = cpr.fast && cpr.learned_used && prm.learned_fallback && cpr.factor_fast > 0.0 &&
                        cpr.factor_fast < 1.0 && prm.tol > 0.0 && prm.tol < 1.0;
     if (!guard) return solve_once(b_in, x_io, device);
     const SolverParams saved = prm;
-    prm.stall_factor = std::pow(cpr.factor_fast, 1.0 / 3.0);
+    prm.stall_ratio = kStallCycleRatio;
     GmresResult first;
     try {
         first = solve_once(b_in, x_io, device);

@@ -26,9 +26,9 @@ struct SolverParams {
     double a_tol = 0.0;
     int is_check_restarted = 1;
     double convfac_threshold = 1e4;
-    // Internal (not an option): > 0 ends the solve with `stalled` set when a full restart cycle reduces
-    // the residual by less than stall_factor^k (the learned settings' guard, Solver::solve).
-    double stall_factor = 0.0;
+    // Internal (not an option): > 0 ends the solve with `stalled` set when a full restart cycle leaves
+    // a residual ratio (end / start) above stall_ratio (the learned settings' guard, Solver::solve).
+    double stall_ratio = 0.0;
     int print_level = 0;
     int logging = 1;
     // CPR (jxfpamg-0220/csrc/cpr/jxf_cpr.c:151-182, 226-262)
@@ -79,7 +79,7 @@ struct SolverParams {
     double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
     double cheb_upper = 1.1;
     int stage2_lanes = 4;
-    int stage2_chunk = 8;      // fast path: stage 2 in chunk order (4, 8 or 16 consecutive block rows; 0 colour order)
+    int stage2_chunk = 4;      // fast path: stage 2 in chunk order (4, 8 or 16 consecutive block rows; 0 colour order)
     int learned_fallback = 1;  // learned mode: keep the plain smoothers when their V-cycle factor is lower
     int record_features = 0;   // fast path: record the per-level features (training data)
 };
@@ -136,7 +136,7 @@ struct CprPrecond {
 struct GmresResult {
     int iterations = 0;
     int converged = 0;
-    int stalled = 0;  // ended by the stall rule (stall_factor)
+    int stalled = 0;  // ended by the stall rule (stall_ratio)
     double rel_residual = 0.0;
     std::vector<double> norms;
     int status = 0;
@@ -180,7 +180,7 @@ struct GgState {
 struct GgParams {
     int k, max_iter, min_iter, check_restarted;
     double tol, a_tol, convfac;
-    double stall;  // SolverParams::stall_factor
+    double stall;  // SolverParams::stall_ratio
 };
 struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
     double *rs, *c, *sn, *h1, *h2, *y, *hh;
