@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const
     }
     // stall rule: a full cycle whose true residual ratio (end / start) stayed above P.stall
     const int ci = s.iter - s.iter0;
-    const bool stalled = P.stall > 0.0 && s.cycles > 1 && ci >= P.k && rn > s.r_norm * P.stall;
+    const bool stalled = P.stall > 0.0 && s.cycles > 1 && ci >= P.k && rn > s.r_cycle * P.stall;
+    s.r_cycle = rn;
     s.r_norm = rn;
     s.iter0 = s.iter;
     if (!done) {

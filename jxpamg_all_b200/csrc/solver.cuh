@@ -175,6 +175,7 @@ struct GgState {
     int est_conv, conv_fail, cont, stalled;
     int iter0, pad;  // iterations at the current cycle's start
     double b_norm, r_norm, r_norm0, epsilon, normdown, scale, rel;
+    double r_cycle;  // true residual norm at the current cycle's start (stall rule)
     unsigned long long t_start, t_end;  // device global timer (ns) at the solve's start and end
 };
 struct GgParams {
