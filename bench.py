@@ -95,7 +95,7 @@ BATCH_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=1, flexible=1, stage2_r
 
 # the kernel the `roofline` object reports for each workload: the one with the largest share of the
 # measured solve in its launch list (profiles/launches_*): "cheb_level1" or "stage2"
-DOMINANT = {"c1": "cheb_level1", "c4": "stage2"}
+DOMINANT = {"c1": "stage2", "c4": "stage2"}
 
 # per-workload method choices: the three-phase system is decoupled by True-IMPES and solved with
 # GMRES(60) (with ABF, or with GMRES(30), the reference itself is still short of 1e-6 after 300
@@ -103,10 +103,10 @@ DOMINANT = {"c1": "cheb_level1", "c4": "stage2"}
 CONFIG_OPTS = {"c4": dict(decouple=5, k_dim=60, max_iter=1000)}
 # the three-phase system under the measured path's driver: the stage-2 weights of the reference's
 # mixed-precision driver (1.0 / 0.8) leave GMRES(60) near 5e-5 after 1,000 iterations there, its
-# plain CPR weights (0.7 / 0.9) converge in ~250; the learned model (trained on two-phase systems)
-# is left out -- its stall guard fires on this system and the rebuild costs more than it saves
+# plain CPR weights (0.7 / 0.9) converge in ~250; the learned settings (a network trained on two- and
+# three-phase systems) are kept: 0.387 s against 0.404 s with the default Chebyshev intervals
 DRIVER_CONFIG_OPTS = {"c4": dict(stage2_relax_weight=0.7, stage2_omega=0.9)}
-MEASURED_CONFIG_OPTS = {"c4": dict(DRIVER_CONFIG_OPTS["c4"], fast_smoother=1)}
+MEASURED_CONFIG_OPTS = {"c4": dict(DRIVER_CONFIG_OPTS["c4"], fast_smoother=2)}
 
 
 def measured_path_text(opts, learned):
@@ -366,6 +366,46 @@ def run_ours(args):
         return G.solve(d_b.data_ptr(), d_x.data_ptr(), device=True)
 
     measured_opts = solver_opts(args)
+    if args.profile_kernels:
+        # the roofline kernels alone inside a profiler range (ncu --profile-from-start off): one stage-2
+        # sweep, two level-1 Chebyshev steps, one FP64 BSR SpMV, the dense inverse of a seeded 1,024 x
+        # 1,024 diagonally dominant matrix (the coarse-level kernel); --path bilu: one exact block-ILU(0)
+        # application (level-scheduled substitutions) of the plain FP64 path instead
+        if args.path == "bilu":
+            G = make(dict(plain_opts(args), stage2_solver_type=5, bilu_exact=1, bilu_ir_iters=1))
+        else:
+            G = make(plain_opts(args) if args.path == "plain" else measured_opts)
+        x1 = torch.ones(s.n, dtype=torch.float64, device="cuda")
+        y1 = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+        gen = torch.Generator(device="cuda").manual_seed(3)
+        nd = 1024
+        dm = -torch.rand((nd, nd), dtype=torch.float64, device="cuda", generator=gen) * 0.01
+        dm += torch.diag(dm.abs().sum(dim=1) + 1.0)
+        dinv = torch.empty_like(dm)
+
+        def kernels():
+            if args.path == "bilu":
+                lib.check(so.jxcpr_solver_bilu_apply(G.h, ctypes.c_void_p(x1.data_ptr()),
+                                                     ctypes.c_void_p(y1.data_ptr()), 1))
+                return
+            lib.check(so.jxcpr_solver_stage2_native(G.h, 1))
+            if G.num_levels() > 2:
+                lib.check(so.jxcpr_solver_level_native(G.h, 1, 1, 2))
+            lib.check(so.jxcpr_bsr_matvec_dev(s.num_block_rows, s.block_size, s.nnzb, d_ia.data_ptr(),
+                                              d_ja.data_ptr(), d_a.data_ptr(), 1.0, x1.data_ptr(), 0.0,
+                                              y1.data_ptr(), 0, ctypes.c_void_p(stream.cuda_stream)))
+            lib.check(so.jxcpr_dense_inverse_dev(nd, dm.data_ptr(), dinv.data_ptr(),
+                                                 ctypes.c_void_p(stream.cuda_stream)))
+
+        kernels()  # warm
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        kernels()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_kernels": args.config, "path": args.path}))
+        G.close()
+        return 0
     if args.profile_solve:
         # one solve inside a profiler range (ncu --profile-from-start off), nothing else
         G = make(plain_opts(args) if args.path == "plain" else measured_opts)
@@ -440,6 +480,7 @@ def run_ours(args):
     solve_gbs = iteration_bytes(G, s, measured_opts.get("k_dim", 30)) * it_m / per_solve / 1e9
     G.close()
     roof_spmv = roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, args.config)
+    roof_spmv_tma = roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, args.config, staged=1)
     # the roofline line names the kernel with the largest share of the measured solve (launch list in
     # profiles/): the level-1 Chebyshev pass where the level has one, else the stage-2 sweep
     roof = roof_lvl if (roof_lvl is not None and DOMINANT.get(args.config) == "cheb_level1") else roof_st2
@@ -517,6 +558,7 @@ def run_ours(args):
                         "setup_s": setup_stats["setup_ms"] / 1e3, "plain_setup_s": plain_setup["setup_ms"] / 1e3,
                         "amg_levels": setup_stats["levels"],
                         "roofline_bsr_spmv": roof_spmv,
+                        "roofline_bsr_spmv_tma_staged": roof_spmv_tma,
                         "roofline_stage2": roof_st2,
                         "roofline_cheb_level1": roof_lvl,
                         "roofline_plain_fp64_stage2": roof_plain},
@@ -536,10 +578,15 @@ def run_ours(args):
     return 0
 
 
-# DRAM traffic per launch of the roofline kernels, from ncu captures of the same kernels on the same
-# workload (dram__bytes_read.sum + dram__bytes_write.sum; layouts reused through JXCPR_TUNE_CACHE), each
-# summarised in profiles/: (workload, kernel key) -> bytes.  None where not captured.
-TRAFFIC_BYTES = {}
+# DRAM traffic of the roofline kernels per timed unit (a stage-2 sweep = its colour launches, a Chebyshev
+# step, one SpMV), from an ncu capture of `bench.py --profile-kernels` (dram__bytes_read.sum +
+# dram__bytes_write.sum; layouts reused through JXCPR_TUNE_CACHE), each summarised in profiles/:
+# (workload, kernel key) -> bytes.  None where not captured.
+TRAFFIC_BYTES = {
+    ("c1", "stage2/4/chunk4"): 210_227_968,    # hgs_chunk<2,4,float>: 100,754,432 + 109,473,536 (2 colours)
+    ("c1", "cheb/A1/4/csr/4"): 103_513_600,    # row_kernel<CsrFmt<4,float>, OpCheb>: mean of 2 launches
+    ("c1", "bsr_spmv/8"): 318_746_624,         # bsr_spmv_direct_kernel<2, double>
+}
 
 
 def hbm_peak():
@@ -618,8 +665,9 @@ def roofline_level(G, stream, level, op, value_bytes, vec_bytes, cfg="c1"):
                  alg, sec, cfg, f"cheb/A{level}/{value_bytes}/{layout}", {"level": level})
 
 
-def roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, cfg="c1"):
-    """The FP64 BSR SpMV y = A x of GMRES (bsr_spmv_direct_kernel) on the workload's matrix."""
+def roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, cfg="c1", staged=0):
+    """The FP64 BSR SpMV y = A x of GMRES on the workload's matrix: bsr_spmv_direct_kernel (the solve's
+    kernel), or with staged = 1 the TMA-staged bsr_spmv_tma_kernel for comparison."""
     import torch
 
     from jxpamg_all_b200 import lib
@@ -632,12 +680,13 @@ def roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, cfg="c1"):
         for _ in range(r):
             lib.check(so.jxcpr_bsr_matvec_dev(s.num_block_rows, s.block_size, s.nnzb, d_ia.data_ptr(),
                                               d_ja.data_ptr(), d_a.data_ptr(), 1.0, x.data_ptr(), 0.0,
-                                              y.data_ptr(), 0, ctypes.c_void_p(stream.cuda_stream)))
+                                              y.data_ptr(), staged, ctypes.c_void_p(stream.cuda_stream)))
 
     sec = _event_time(stream, body, 20)
     bs, nb, nnzb, n = s.block_size, s.num_block_rows, s.nnzb, s.n
     alg = nnzb * (bs * bs * 8 + 4) + (nb + 1) * 4 + 2 * n * 8
-    return _roof(f"BSR SpMV y = A x (bsr_spmv_direct_kernel<{bs}, double>, FP64)", alg, sec, cfg, "bsr_spmv/8")
+    kname = f"bsr_spmv_tma_kernel<{bs}>" if staged else f"bsr_spmv_direct_kernel<{bs}, double>"
+    return _roof(f"BSR SpMV y = A x ({kname}, FP64)", alg, sec, cfg, "bsr_spmv_tma/8" if staged else "bsr_spmv/8")
 
 
 def iteration_bytes(G, s, k_dim):
@@ -917,9 +966,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override a solver option of the measured path (repeatable)")
-    ap.add_argument("--path", default="mixed", choices=["mixed", "plain"], help="path --profile-solve runs")
+    ap.add_argument("--path", default="mixed", choices=["mixed", "plain", "bilu"],
+                    help="path --profile-solve / --profile-kernels runs (bilu: --profile-kernels only)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="set up, run --warmup solves, then one solve inside a profiler range, and exit")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="set up, then the roofline kernels (stage-2 sweep, level-1 Chebyshev steps, BSR SpMV) "
+                         "once inside a profiler range, and exit")
     args = ap.parse_args()
     if args.config == "c3":
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)

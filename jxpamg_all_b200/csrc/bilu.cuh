@@ -21,7 +21,7 @@ struct Bilu {
     DevBuf<double> D, Dinv;
     DevBuf<double> ft, ut, yt, un;
     // exact mode: per-row levels of the lower / upper DAGs, rows bucketed by level (ptr, rows)
-    int nlev_l = 0, nlev_u = 0;
+    int nlev_l = 0, nlev_u = 0, widest = 1;  // level counts, rows of the widest level
     DevBuf<int> lev_l, lev_u, lptr, lrows, uptr, urows;
     std::vector<int> h_lptr, h_uptr;
     DevBuf<float> la32, ua32, dinv32;

@@ -383,6 +383,11 @@ void Bilu::setup_exact(const BsrView<double> &A, cudaStream_t s) {
     DevBuf<int> err(4);
     nlev_l = level_schedule(nb, L.ia.get(), L.ja.get(), lev_l, lptr, lrows, h_lptr, err.get(), s);
     nlev_u = level_schedule(nb, U.ia.get(), U.ja.get(), lev_u, uptr, urows, h_uptr, err.get(), s);
+    // the widest level bounds the threads a level can use: grids of that size keep the per-level grid
+    // barrier (hundreds of levels on a reservoir grid) among as few blocks as possible
+    widest = 1;
+    for (size_t k = 0; k + 1 < h_lptr.size(); ++k) widest = std::max(widest, h_lptr[k + 1] - h_lptr[k]);
+    for (size_t k = 0; k + 1 < h_uptr.size(); ++k) widest = std::max(widest, h_uptr[k + 1] - h_uptr[k]);
     // the upper levels are counted from the last row: level 0 rows have no U entries and come first
     if (nb) {
         JX_CUDA(cudaMemsetAsync(err.get(), 0, 4 * sizeof(int), s));
@@ -395,7 +400,7 @@ void Bilu::setup_exact(const BsrView<double> &A, cudaStream_t s) {
         int *pe = err.get();
         void *args[] = {&nl, &lp, &lr, &aia, &aja, &aa, &llia, &llja, &pla, &luia, &luja, &pua, &pd, &pdi, &bar, &pe};
         void *fn = bs == 2 ? (void *)factor_kernel<2> : (void *)factor_kernel<3>;
-        const int grid = bs == 2 ? coop_grid_for(factor_kernel<2>, nb) : coop_grid_for(factor_kernel<3>, nb);
+        const int grid = bs == 2 ? coop_grid_for(factor_kernel<2>, widest) : coop_grid_for(factor_kernel<3>, widest);
         JX_CUDA(cudaLaunchCooperativeKernel(fn, grid, kT, args, 0, s));
         count_launch();
         check_flags(err.get(), s, "factorisation");
@@ -432,14 +437,14 @@ void Bilu::substitute(const double *f, double *y, double *t, cudaStream_t s) {
         void *args[] = {&nl, &lp, &lr, &nu, &up, &ur, &llia, &llja, &pla, &luia, &luja, &pua, &pdi,
                         (void *)&f, &y, &t, &bar, &pe};
         fn = bs == 2 ? (void *)subst_kernel<2, float> : (void *)subst_kernel<3, float>;
-        grid = bs == 2 ? coop_grid_for(subst_kernel<2, float>, nb) : coop_grid_for(subst_kernel<3, float>, nb);
+        grid = bs == 2 ? coop_grid_for(subst_kernel<2, float>, widest) : coop_grid_for(subst_kernel<3, float>, widest);
         JX_CUDA(cudaLaunchCooperativeKernel(fn, grid, kT, args, 0, s));
     } else {
         const double *pla = L.a.get(), *pua = U.a.get(), *pdi = Dinv.get();
         void *args[] = {&nl, &lp, &lr, &nu, &up, &ur, &llia, &llja, &pla, &luia, &luja, &pua, &pdi,
                         (void *)&f, &y, &t, &bar, &pe};
         fn = bs == 2 ? (void *)subst_kernel<2, double> : (void *)subst_kernel<3, double>;
-        grid = bs == 2 ? coop_grid_for(subst_kernel<2, double>, nb) : coop_grid_for(subst_kernel<3, double>, nb);
+        grid = bs == 2 ? coop_grid_for(subst_kernel<2, double>, widest) : coop_grid_for(subst_kernel<3, double>, widest);
         JX_CUDA(cudaLaunchCooperativeKernel(fn, grid, kT, args, 0, s));
     }
     count_launch();

@@ -2,10 +2,13 @@
 
 Systems: seeded variants of the config-0/config-1 reservoir Jacobians (2x2
 BSR): grids drawn from 16x16x8 .. 60x110x40 (capped in cell count, half of
-them with a channelised lower part), 60x220 slabs of the config-1 geometry, and
-full 60x220x85 config-1 geometries with other seeds than the benchmark's.  Each system is solved by the mixed
-CPR-GMRES path (FP32 + BF16 coarse levels, flexible GMRES, Chebyshev-3 on the
-dense levels) once per candidate setting (18) -- strength threshold of level 0,
+them with a channelised lower part), 60x220 slabs of the config-1 geometry,
+full 60x220x85 config-1 geometries with other seeds than the benchmark's, and
+three-phase black-oil variants (3x3 BSR, the config-4 family: True-IMPES
+decoupling, GMRES(60), the plain CPR stage-2 weights) on the small grids.  Each
+system is solved by the mixed CPR-GMRES path of the measured configuration
+(FP32 preconditioner, flexible GMRES, chunk-ordered stage 2, Chebyshev-3 on
+the dense levels) once per candidate setting (18) -- strength threshold of level 0,
 strength threshold of the coarser levels, Chebyshev interval -- and once with
 the plain smoothers.  The label of a system is the candidate with the lowest
 cost = iterations x modelled bytes per iteration (bytes moved by the
@@ -24,12 +27,21 @@ from ..solver import CprGmres
 # predictions to these values (csrc/learned.cu), so the two lists must agree
 CANDIDATES = [(t0, tc, lo, hi) for t0 in (0.25, 0.5) for tc in (0.25, 0.5, 0.7)
               for (lo, hi) in ((0.1, 1.2), (0.3, 1.1), (0.5, 1.2))]
+# the measured path's preconditioner (FP32 storage, the reference mixed driver's stage-2 weights);
+# layouts not autotuned and graphs off, so that a training solve sets up quickly
 MIXED = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, smoother_order=1, coarse_exact=0,
-             precision=2, flexible=1, autotune=0, graphs=0)
+             precision=1, flexible=1, autotune=0, graphs=0, stage2_relax_weight=1.0, stage2_omega=0.8)
+# the three-phase family's method (True-IMPES, GMRES(60), the plain CPR stage-2 weights)
+MIXED3 = dict(MIXED, decouple=5, k_dim=60, max_iter=1000, stage2_relax_weight=0.7, stage2_omega=0.9)
 MAX_CELLS = 100_000
 
 
-SLAB_BASE, FULL_BASE = 20000, 30000
+SLAB_BASE, FULL_BASE, THREE_BASE = 20000, 30000, 40000
+
+
+def variant_options(idx):
+    """The solver options of system idx's family."""
+    return MIXED3 if THREE_BASE <= idx < THREE_BASE + 10000 else MIXED
 
 
 def system_variant(idx, base_seed=20240):
@@ -37,9 +49,18 @@ def system_variant(idx, base_seed=20240):
 
     idx < 20000: config-0-like grids (16..60 x 16..110 x 8..40, <= MAX_CELLS cells);
     20000 <= idx < 30000: config-1 slabs, 60 x 220 x (10..40) with a channelised lower part;
-    idx >= 30000: full config-1 geometry (60 x 220 x 85, 50 channelised layers) with other seeds.
+    30000 <= idx < 40000 or idx >= 50000: full config-1 geometry (60 x 220 x 85, 50 channelised layers)
+    with other seeds;
+    40000 <= idx < 50000: three-phase grids drawn as the config-0-like ones (Sg, gas viscosity of config 4).
     """
     rng = np.random.default_rng(base_seed + idx)
+    if THREE_BASE <= idx < THREE_BASE + 10000:
+        while True:
+            nx, ny, nz = int(rng.integers(16, 61)), int(rng.integers(16, 111)), int(rng.integers(8, 31))
+            if nx * ny * nz <= MAX_CELLS:
+                break
+        ch = int(round(nz * rng.uniform(0.3, 0.7))) if rng.random() < 0.5 else 0
+        return synth.reservoir_system(nx, ny, nz, seed=base_seed + 7919 * idx, phases=3, channelised_layers=ch)
     if idx >= FULL_BASE:
         return synth.reservoir_system(60, 220, 85, seed=base_seed + 7919 * idx, phases=2, channelised_layers=50)
     if idx >= SLAB_BASE:
@@ -54,7 +75,7 @@ def system_variant(idx, base_seed=20240):
     return synth.reservoir_system(nx, ny, nz, seed=base_seed + 7919 * idx, phases=2, channelised_layers=ch)
 
 
-def iteration_bytes(G, s, precision=2):
+def iteration_bytes(G, s, precision=2, k_dim=30):
     """Modelled bytes one GMRES iteration moves with the hierarchy of G."""
     xb = 8 if precision == 0 else 4
     tb = 8 if precision == 0 else 4
@@ -75,7 +96,7 @@ def iteration_bytes(G, s, precision=2):
     vb2 = 8 if precision == 0 else 4
     total += 3 * (nnzb * (bs * bs * vb2 + 4) + nb * bs * 8 * 4)   # stage 2
     total += nnzb * (bs * bs * 8 + 4) + 2 * s.n * 8                # GMRES SpMV
-    total += 15 * 4 * s.n * 8                                       # average MGS passes
+    total += (k_dim // 2) * 4 * s.n * 8                             # average orthogonalisation passes
     return total
 
 
@@ -93,7 +114,7 @@ def solve_case(s, dev, options):
     L = G.num_levels()
     feats = [G.level_features(lev) for lev in range(L - 1)]
     thetas = [G.level_info(lev)["theta"] for lev in range(L - 1)]
-    cost = it * iteration_bytes(G, s, options.get("precision", 0)) if conv else float("inf")
+    cost = it * iteration_bytes(G, s, options.get("precision", 0), options.get("k_dim", 30)) if conv else float("inf")
     status = G.learned_status() if options.get("fast_smoother") == 2 else None
     G.close()
     return dict(iters=int(it), converged=bool(conv), rel=float(rel), cost=float(cost),
@@ -107,10 +128,10 @@ def upload(s):
     return dict(ia=d(s.ia), ja=d(s.ja), a=d(s.a), b=d(s.b), x=torch.zeros(s.n, dtype=torch.float64, device="cuda"))
 
 
-def candidate_options(c):
+def candidate_options(c, base=None):
     t0, tc, lo, hi = c
-    return dict(MIXED, fast_smoother=1, strong_threshold=float(t0), strong_threshold_coarse=float(tc),
-                cheb_lower=float(lo), cheb_upper=float(hi), record_features=1)
+    return dict(MIXED if base is None else base, fast_smoother=1, strong_threshold=float(t0),
+                strong_threshold_coarse=float(tc), cheb_lower=float(lo), cheb_upper=float(hi), record_features=1)
 
 
 def generate(indices, log=print):
@@ -118,13 +139,14 @@ def generate(indices, log=print):
     records = []
     for idx in indices:
         s = system_variant(idx)
+        base = variant_options(idx)
         dev = upload(s)
         res = []
         for c in CANDIDATES:
-            r = solve_case(s, dev, candidate_options(c))
+            r = solve_case(s, dev, candidate_options(c, base))
             r["candidate"] = list(c)
             res.append(r)
-        plain = solve_case(s, dev, dict(MIXED, fast_smoother=0, record_features=1))
+        plain = solve_case(s, dev, dict(base, fast_smoother=0, record_features=1))
         best = int(np.argmin([r["cost"] for r in res]))
         records.append(dict(index=int(idx), shape=[s.nx, s.ny, s.nz], cells=s.num_block_rows, results=res,
                             plain=plain, best=best))

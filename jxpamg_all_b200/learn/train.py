@@ -1,6 +1,7 @@
 """Train the learned-settings MLP on the GPU and export its weights.
 
-    python -m jxpamg_all_b200.learn.train --systems 110 --holdout 16 --out-dir DIR
+    python -m jxpamg_all_b200.learn.train --systems 110 --slabs 40 --full 8 --three 40 \
+        --holdout 8 --holdout-three 6 --holdout-full 4 --out-dir DIR
 
 1. datagen.generate: every training system is solved with each candidate
    setting (18 candidates + the plain smoothers: 19 solves per system);
@@ -69,15 +70,16 @@ def evaluate(indices, weights, log=print):
     out = []
     for idx in indices:
         s = datagen.system_variant(idx)
+        base = datagen.variant_options(idx)
         dev = datagen.upload(s)
-        learned = datagen.solve_case(s, dev, dict(datagen.MIXED, fast_smoother=2))
-        cheb = datagen.solve_case(s, dev, dict(datagen.MIXED, fast_smoother=1, record_features=1))
-        plain = datagen.solve_case(s, dev, dict(datagen.MIXED, fast_smoother=0, record_features=1))
+        learned = datagen.solve_case(s, dev, dict(base, fast_smoother=2))
+        cheb = datagen.solve_case(s, dev, dict(base, fast_smoother=1, record_features=1))
+        plain = datagen.solve_case(s, dev, dict(base, fast_smoother=0, record_features=1))
         rec = dict(index=int(idx), cells=s.num_block_rows, learned=learned, chebyshev_default=cheb, plain=plain)
         out.append(rec)
-        log(f"holdout {idx}: cost learned/plain {learned['cost'] / plain['cost']:.3f} "
-            f"cheb/plain {cheb['cost'] / plain['cost']:.3f} iters {learned['iters']}/{cheb['iters']}/{plain['iters']}"
-            f" learned used {learned['learned']}")
+        log(f"holdout {idx}: cost learned/cheb {learned['cost'] / cheb['cost']:.3f} "
+            f"learned/plain {learned['cost'] / plain['cost']:.3f} iters {learned['iters']}/{cheb['iters']}/"
+            f"{plain['iters']} learned used {learned['learned']}")
     return out
 
 
@@ -91,6 +93,9 @@ def main(argv=None):
     ap.add_argument("--runs", help="start from the training runs of an earlier generation (runs.npz)")
     ap.add_argument("--slabs", type=int, default=0, help="60x220 slabs of the config-1 geometry to add")
     ap.add_argument("--full", type=int, default=0, help="full config-1 geometries (other seeds) to add")
+    ap.add_argument("--three", type=int, default=0, help="three-phase (3x3, config-4 family) systems to add")
+    ap.add_argument("--holdout-three", type=int, default=0, help="held-out three-phase systems")
+    ap.add_argument("--holdout-full", type=int, default=0, help="held-out full config-1 geometries")
     args = ap.parse_args(argv)
     import torch
 
@@ -104,6 +109,7 @@ def main(argv=None):
     indices = list(range(args.systems)) if not args.runs else []
     indices += [datagen.SLAB_BASE + i for i in range(args.slabs)]
     indices += [datagen.FULL_BASE + i for i in range(args.full)]
+    indices += [datagen.THREE_BASE + i for i in range(args.three)]
     if indices:
         new = datagen.compact(datagen.generate(indices))
         runs = new if runs is None else datagen.merge(runs, new)
@@ -112,20 +118,27 @@ def main(argv=None):
     t_data = time.time() - t0
     w, hist = train_mlp(X, T, steps=args.steps, lr=args.lr)
     t_train = time.time() - t0 - t_data
-    holdout = evaluate(range(100000, 100000 + args.holdout), w)
+    # held-out systems (never in the training runs): config-0-like grids, three-phase grids, full
+    # config-1 geometries
+    hold_idx = [5000 + i for i in range(args.holdout)]
+    hold_idx += [datagen.THREE_BASE + 5000 + i for i in range(args.holdout_three)]
+    hold_idx += [100000 + i for i in range(args.holdout_full)]
+    holdout = evaluate(hold_idx, w)
     np.savez(os.path.join(args.out_dir, "weights.npz"), w=w)
     n_sys = int(runs["cost"].shape[0])
     n_solves = n_sys * (runs["cost"].shape[1] + 1)
     write_weights_inc(os.path.join(args.out_dir, "learned_weights.inc"), w,
-                      f"Trained on {n_sys} seeded config-0/1 variants ({n_solves} solves), {X.shape[0]} "
+                      f"Trained on {n_sys} seeded config-0/1/4-family variants ({n_solves} solves), {X.shape[0]} "
                       f"level samples, {args.steps} full-batch Adam steps; final loss {hist[-1][1]:.5f}.")
     ratio = lambda key: float(np.mean([h[key]["cost"] / h["plain"]["cost"] for h in holdout]))  # noqa: E731
+    vs_cheb = [h["learned"]["cost"] / h["chebyshev_default"]["cost"] for h in holdout]
     best = np.min(runs["cost"], axis=1)
     report = dict(systems=n_sys, solves=n_solves,
                   train_mean_best_cost_ratio_vs_plain=float(np.mean(best / runs["plain_cost"])), samples=int(X.shape[0]), outputs=N_OUT,
                   loss_history=hist, data_seconds=t_data, train_seconds=t_train,
                   holdout_mean_cost_ratio_learned_vs_plain=ratio("learned"),
                   holdout_mean_cost_ratio_cheb_default_vs_plain=ratio("chebyshev_default"),
+                  holdout_mean_cost_ratio_learned_vs_cheb_default=float(np.mean(vs_cheb)),
                   holdout_learned_used=int(sum(bool(h["learned"]["learned"]["learned_used"]) for h in holdout)),
                   holdout=[dict(index=h["index"], cells=h["cells"],
                                 iters=[h["learned"]["iters"], h["chebyshev_default"]["iters"], h["plain"]["iters"]],

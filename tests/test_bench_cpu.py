@@ -31,7 +31,7 @@ def test_c4_measured_and_plain_options():
     m, p = bench.solver_opts(args), bench.plain_opts(args)
     for o in (m, p):
         assert o["decouple"] == 5 and o["k_dim"] == 60 and o["max_iter"] == 1000
-    assert (m["stage2_relax_weight"], m["stage2_omega"]) == (0.7, 0.9) and m["fast_smoother"] == 1
+    assert (m["stage2_relax_weight"], m["stage2_omega"]) == (0.7, 0.9) and m["fast_smoother"] == 2
     assert "stage2_relax_weight" not in p
 
 
@@ -45,7 +45,10 @@ def test_measured_path_text_follows_the_options():
     c1 = bench.measured_path_text(bench.solver_opts(SimpleNamespace(config="c1", opt=[])), {"learned_used": True})
     c4 = bench.measured_path_text(bench.solver_opts(SimpleNamespace(config="c4", opt=[])), {"learned_used": False})
     assert "mixed driver's weights 1.0/0.8" in c1 and "(kept)" in c1
-    assert "plain CPR's weights 0.7/0.9" in c4 and "no learned settings" in c4
+    assert "plain CPR's weights 0.7/0.9" in c4 and "rejected by the probe" in c4
+    c4d = bench.measured_path_text(bench.solver_opts(SimpleNamespace(config="c4", opt=["fast_smoother=1"])),
+                                   {"learned_used": False})
+    assert "no learned settings" in c4d
 
 
 def test_both_arms_print_the_same_config():

@@ -96,27 +96,34 @@ def test_training_loop_reduces_loss():
     assert np.array_equal(w[:32], np.concatenate([X.mean(0), X.std(0) + 1e-3]).astype(np.float32))
 
 
-def test_trained_network_gain_over_plain_settings():
-    """Held-out systems (never in the training runs): the mixed path with the
-    learned settings against the same path with the plain smoother settings.
-    Reports the modelled-cost ratio; the probe-based fallback must keep the
-    learned mode from regressing beyond noise."""
+# held-out systems (never in the training runs): config-0-like grids, three-phase grids (the config-4
+# family's method), full config-1 geometries with other seeds
+HELD_OUT = ([5000 + i for i in range(8)] + [datagen.THREE_BASE + 5000 + i for i in range(6)] +
+            [100000 + i for i in range(4)])
+
+
+def test_trained_network_gain_over_default_chebyshev():
+    """What the network adds: on held-out two- and three-phase systems, the learned settings (strength
+    thresholds and Chebyshev intervals per level, with the probe / stall fallback) against the same
+    mixed path with the default thresholds and Chebyshev intervals (fast_smoother 1), by the modelled cost
+    (iterations x modelled bytes per iteration).  The learned settings must cost less on average by more
+    than 3 % (the training report of the compiled weights: 0.968)."""
     ratios, used = [], 0
-    for idx in range(100000, 100004):
+    for idx in HELD_OUT:
         s = datagen.system_variant(idx)
+        base = datagen.variant_options(idx)
         dev = datagen.upload(s)
-        # the measured configuration of bench.py: FP32 preconditioner, flexible GMRES
-        learned = datagen.solve_case(s, dev, dict(datagen.MIXED, precision=1, fast_smoother=2))
-        plain = datagen.solve_case(s, dev, dict(datagen.MIXED, precision=1, fast_smoother=0, record_features=1))
-        assert learned["converged"] and plain["converged"]
-        ratios.append(learned["cost"] / plain["cost"])
+        learned = datagen.solve_case(s, dev, dict(base, fast_smoother=2))
+        cheb = datagen.solve_case(s, dev, dict(base, fast_smoother=1, record_features=1))
+        assert learned["converged"] and cheb["converged"]
+        ratios.append(learned["cost"] / cheb["cost"])
         used += learned["learned"]["learned_used"]
         st = learned["learned"]
         assert 0 < st["factor_learned"] < 1 and 0 < st["factor_plain"] < 1
     mean = float(np.mean(ratios))
-    print(f"learned / plain modelled cost on held-out systems: {np.round(ratios, 3)} mean {mean:.3f}, "
+    print(f"learned / default Chebyshev modelled cost on held-out systems: {np.round(ratios, 3)} mean {mean:.3f}, "
           f"learned settings kept on {used} of {len(ratios)}")
-    assert mean <= 1.05
+    assert mean < 0.97
 
 
 def test_rejected_learned_settings_fall_back_to_the_plain_method():
