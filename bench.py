@@ -79,9 +79,10 @@ PLAIN_OPTS = dict(decouple=1, k_dim=30, max_iter=300, tol=1e-6, stage2_maxit=3, 
                   precision=0, fast_smoother=0)
 # measured path: FP32 preconditioner + learned settings, the stage-2 weights of the reference's
 # mixed-precision driver (1.0 / 0.8, src/test_bsr_cprgmres_hybrid.c:373-374; its plain CPR uses
-# 0.7 / 0.9, jxf_cpr.c:547-548), flexible FP64 GMRES run on the device as one CUDA graph
+# 0.7 / 0.9, jxf_cpr.c:547-548), flexible FP64 GMRES run on the device as one CUDA graph with its
+# Krylov basis stored in FP32 (products, norms, rotations and x in FP64)
 SOLVER_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=2, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8,
-                   graph_gmres=1)
+                   graph_gmres=1, krylov_fp32=1)
 # ablation: the plain FP64 preconditioner with the measured path's stage-2 weights and GMRES driver,
 # so that what precision + learned settings alone gain is visible
 PLAIN_SAME_DRIVER_OPTS = dict(PLAIN_OPTS, flexible=1, stage2_relax_weight=1.0, stage2_omega=0.8, graph_gmres=1)
@@ -118,8 +119,9 @@ def measured_path_text(opts, learned):
     else:
         tuned = "default strength threshold, Chebyshev-3 on the dense levels (no learned settings)"
     return (f"mixed: FP32 preconditioner storage/arithmetic (AMG levels, transfers, stage 2 with {src} weights "
-            f"{w}/{om}), FP64 flexible GMRES run on the device as one CUDA graph / SpMV / true residual / coarsest "
-            f"solve; {tuned}; the plain FP64 path is the reference's CPR (weights 0.7/0.9) with its host-driven "
+            f"{w}/{om}), FP64 flexible GMRES run on the device as one CUDA graph"
+            f"{' (Krylov basis stored in FP32)' if opts.get('krylov_fp32') else ''} / SpMV / true residual / "
+            f"coarsest solve; {tuned}; the plain FP64 path is the reference's CPR (weights 0.7/0.9) with its host-driven "
             "MGS GMRES")
 
 
@@ -369,8 +371,9 @@ def run_ours(args):
     if args.profile_kernels:
         # the roofline kernels alone inside a profiler range (ncu --profile-from-start off): one stage-2
         # sweep, two level-1 Chebyshev steps, one FP64 BSR SpMV, the dense inverse of a seeded 1,024 x
-        # 1,024 diagonally dominant matrix (the coarse-level kernel); --path bilu: one exact block-ILU(0)
-        # application (level-scheduled substitutions) of the plain FP64 path instead
+        # 1,024 diagonally dominant matrix (the coarse-level kernel) and, on the measured path, one
+        # device-GMRES orthogonalisation step at the mid-cycle basis size after a solve; --path bilu: one
+        # exact block-ILU(0) application (level-scheduled substitutions) of the plain FP64 path instead
         if args.path == "bilu":
             G = make(dict(plain_opts(args), stage2_solver_type=5, bilu_exact=1, bilu_ir_iters=1))
         else:
@@ -396,6 +399,15 @@ def run_ours(args):
                                               y1.data_ptr(), 0, ctypes.c_void_p(stream.cuda_stream)))
             lib.check(so.jxcpr_dense_inverse_dev(nd, dm.data_ptr(), dinv.data_ptr(),
                                                  ctypes.c_void_p(stream.cuda_stream)))
+
+        if args.path == "mixed" and measured_opts.get("graph_gmres"):
+            solve_device(G)  # the orthogonalisation kernels run on the basis a solve leaves
+            m_kry = (measured_opts.get("k_dim", 30) + 1) // 2
+            base_kernels = kernels
+
+            def kernels():
+                base_kernels()
+                lib.check(so.jxcpr_solver_krylov_native(G.h, m_kry, 1))
 
         kernels()  # warm
         torch.cuda.synchronize()
@@ -454,7 +466,7 @@ def run_ours(args):
     plain_t, plain_it, plain_rel, _, clk_p = timed(P, "plain FP64")
     x_plain = d_x.cpu().numpy().copy()
     roof_plain = roofline_stage2(P, s, stream, 8, args.config)
-    plain_gbs = iteration_bytes(P, s, plain_opts(args).get("k_dim", 30)) * plain_it / plain_t / 1e9
+    plain_gbs = iteration_bytes(P, s, plain_opts(args)) * plain_it / plain_t / 1e9
     P.close()
 
     # ---- the reference's hybrid form (FP32 stage 1 + FP64 polish), for comparison ------
@@ -477,7 +489,8 @@ def run_ours(args):
     vb = 8 if measured_opts.get("precision", 0) == 0 else 4
     roof_st2 = roofline_stage2(G, s, stream, 8 if measured_opts.get("precision", 0) in (0, 3) else 4, args.config)
     roof_lvl = roofline_level(G, stream, 1, 1, vb, vb, args.config) if G.num_levels() > 2 else None
-    solve_gbs = iteration_bytes(G, s, measured_opts.get("k_dim", 30)) * it_m / per_solve / 1e9
+    solve_gbs = iteration_bytes(G, s, measured_opts) * it_m / per_solve / 1e9
+    roof_kry = roofline_krylov(G, s, stream, measured_opts, args.config) if measured_opts.get("graph_gmres") else None
     G.close()
     roof_spmv = roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, args.config)
     roof_spmv_tma = roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, args.config, staged=1)
@@ -544,8 +557,9 @@ def run_ours(args):
                         "iterations": it_m, "final_rel_res": rel_m,
                         "solve_gbs": solve_gbs,
                         "solve_gbs_definition": "modelled bytes per GMRES iteration (preconditioner traffic at its "
-                                                "storage precision + FP64 BSR SpMV + CGS2 orthogonalisation) x "
-                                                "iterations / solve time",
+                                                "storage precision + FP64 BSR SpMV + orthogonalisation: three "
+                                                "CGS2 passes over the basis at its storage precision, or one MGS "
+                                                "pass per vector on the host-driven path) x iterations / solve time",
                         "plain_fp64_s": plain_t, "plain_fp64_iterations": plain_it, "plain_fp64_rel_res": plain_rel,
                         "plain_fp64_solve_gbs": plain_gbs,
                         "speedup_vs_plain_fp64": plain_t / per_solve,
@@ -559,6 +573,7 @@ def run_ours(args):
                         "amg_levels": setup_stats["levels"],
                         "roofline_bsr_spmv": roof_spmv,
                         "roofline_bsr_spmv_tma_staged": roof_spmv_tma,
+                        "roofline_krylov_step": roof_kry,
                         "roofline_stage2": roof_st2,
                         "roofline_cheb_level1": roof_lvl,
                         "roofline_plain_fp64_stage2": roof_plain},
@@ -689,18 +704,47 @@ def roofline_bsr_spmv(d_ia, d_ja, d_a, s, stream, cfg="c1", staged=0):
     return _roof(f"BSR SpMV y = A x ({kname}, FP64)", alg, sec, cfg, "bsr_spmv_tma/8" if staged else "bsr_spmv/8")
 
 
-def iteration_bytes(G, s, k_dim):
+def roofline_krylov(G, s, stream, opts, cfg="c1"):
+    """One device-GMRES orthogonalisation step at the mid-cycle basis size m = (k + 1) // 2: the first
+    Gram products, the fused update + second products and the final update (four launches, one of them a
+    one-block reduction), timed together with CUDA events on the solver's stream after a solve.
+    Algorithmic bytes: three passes over m basis vectors at p_b bytes an entry, w read three times and
+    written once, v_m written: (3 m p_b + 32 + p_b) n."""
+    from jxpamg_all_b200 import lib
+
+    so = lib.load()
+    m = (opts.get("k_dim", 30) + 1) // 2
+    pb = 4 if opts.get("krylov_fp32", 0) else 8
+    sec = _event_time(stream, lambda r: lib.check(so.jxcpr_solver_krylov_native(G.h, m, r)), 20)
+    alg = (3 * m * pb + 32 + pb) * s.n
+    ty = "float" if pb == 4 else "double"
+    return _roof(f"CGS2 orthogonalisation step, m = {m} (dots_kernel<{ty}> + update_dots_kernel<{ty}> + "
+                 f"final_kernel<{ty}>, basis in {'FP32' if pb == 4 else 'FP64'})", alg, sec, cfg,
+                 f"krylov/{pb}/{m}", {"m": m})
+
+
+def iteration_bytes(G, s, opts):
     """Modelled bytes of one GMRES iteration: the preconditioner application (its modelled traffic), the
-    FP64 BSR SpMV, and the flexible CGS2 orthogonalisation at the mean step of a cycle (two passes over
-    the basis, the update fused with the second products: (2 j + 6) n doubles at step j)."""
+    FP64 BSR SpMV, and the orthogonalisation at the mean basis size m = (k + 1) / 2 of a cycle.
+    - Device GMRES (graph_gmres 1, CGS2), with p_b bytes per basis entry (8, or 4 with krylov_fp32):
+      three passes over the basis (first products; the first update fused with the second products;
+      the final update) plus w, the new vector, and the copies in and out of the preconditioner. That
+      is (3 m p_b + 48 + 3 p_b) n bytes, and 8 n more when an FP32 basis rounds the direction in place.
+    - Host GMRES (modified Gram-Schmidt): one pass per basis vector. Each pass reads w and v_j and
+      writes w, giving (32 m + 16) n bytes."""
     from jxpamg_all_b200 import lib
 
     so = lib.load()
     ab = np.zeros(1)
     lib.check(so.jxcpr_solver_apply_bytes(G.h, ab.ctypes.data_as(ctypes.c_void_p)))
     spmv = s.nnzb * (s.block_size ** 2 * 8 + 4) + (s.num_block_rows + 1) * 4 + 2 * s.n * 8
-    jm = (k_dim - 1) / 2.0
-    return float(ab[0]) + spmv + (2 * jm + 6) * s.n * 8
+    m = (opts.get("k_dim", 30) + 1) / 2.0
+    if opts.get("graph_gmres", 0):
+        pb = 4 if opts.get("krylov_fp32", 0) else 8
+        orth = (3 * m * pb + 48 + 3 * pb + (8 if pb == 4 else 0)) * s.n
+    else:
+        orth = (32 * m + 16) * s.n
+    return float(ab[0]) + spmv + orth
 
 
 # ---------------------------------------------------------------------------

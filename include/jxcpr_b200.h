@@ -143,7 +143,11 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         fast_smoother (0 colour GS / l1-Jacobi, 1 Chebyshev-3 on the dense
  *         levels, 2 learned settings, 3 Chebyshev-3 everywhere), max_colors (8:
  *         levels needing more colours use l1-Jacobi), flexible (0), graphs (1),
- *         graph_gmres (0), orthog (0 modified, 1 one-pass classical
+ *         graph_gmres (0), krylov_fp32 (0; 1 with graph_gmres: the Krylov
+ *         basis and the flexible directions stored in FP32, every product,
+ *         norm, rotation, residual and x in FP64), selective_reorth (0; 1
+ *         with graph_gmres: the second classical Gram-Schmidt pass only when
+ *         the first removed more than half of ||w||^2), orthog (0 modified, 1 one-pass classical
  *         Gram-Schmidt), autotune (1; 2 shared per shape class), stage2_lanes
  *         (4: CSR stage 2 without autotuning), stage2_chunk (4: stage 2 visits
  *         chunks of this many consecutive block rows in natural order, the
@@ -229,6 +233,13 @@ JXCPR_API int jxcpr_stage2_chunk_order(int nb, const int *ia, const int *ja, int
  * reference counterpart; the kernel a roofline measurement times with events on that stream):
  * op 0 y = A x, 1 one Chebyshev step y = c z + D^-1 A x, 2 the residual r = f - A u. */
 JXCPR_API int jxcpr_solver_level_native(jxcpr_solver *solver, int level, int op, int reps);
+/* Queues `reps` times the orthogonalisation kernels of one device-GMRES Arnoldi step with m basis
+ * vectors (1 <= m <= k_dim): the first Gram products, the fused first update + second products and
+ * the final update into v_m, outside the solve's graph, on the basis the last solve left and the
+ * solver's work vector, asynchronously on the solver's stream (no reference counterpart; the CGS2
+ * kernels a roofline measurement or a profiler captures).  Needs a solve with graph_gmres 1 first;
+ * the next solve starts from scratch. */
+JXCPR_API int jxcpr_solver_krylov_native(jxcpr_solver *solver, int m, int reps);
 /* Level `level`'s operator values as the fast path stores them (FP64, FP32, or BF16 times its block scale),
  * widened to FP64, in the entry order of jxcpr_solver_level_matrix (host array of its nnz values); no
  * reference counterpart.  Levels without a smoothed operator (the coarsest) return JXCPR_ERROR_ARG. */

@@ -68,6 +68,8 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"graphs", &p.graphs},
                {"orthog", &p.orthog},
                {"graph_gmres", &p.graph_gmres},
+               {"krylov_fp32", &p.krylov_fp32},
+               {"selective_reorth", &p.selective_reorth},
                {"bilu_sweeps", &p.bilu_sweeps},
                {"bilu_ir_iters", &p.bilu_ir_iters},
                {"bilu_lower_iters", &p.bilu_lower_iters},
@@ -469,6 +471,18 @@ int jxcpr_solver_level_native(jxcpr_solver *h, int level, int op, int reps) {
             set_error("level_native: level %d has no smoothed operator", level);
             return JXCPR_ERROR_ARG;
         }
+        return JXCPR_SUCCESS;
+    });
+}
+
+int jxcpr_solver_krylov_native(jxcpr_solver *h, int m, int reps) {
+    if (!h || reps < 0) return JXCPR_ERROR_ARG;
+    if (!h->s.ggmres || !h->s.ggmres->exec) {
+        set_error("krylov_native needs a solve with graph_gmres 1 first");
+        return JXCPR_ERROR_ARG;
+    }
+    return guarded([&] {
+        h->s.ggmres->orth_native(m, reps, h->s.gmres.w.get(), h->s.stream);
         return JXCPR_SUCCESS;
     });
 }

@@ -26,6 +26,10 @@
 // instead of MGS (i + 1 passes).  The norm of the new vector comes from Pythagoras,
 // ||w - V h2||^2 = ||w||^2 - ||h2||^2, as in delayed CGS2 (Swirydowicz et al.,
 // 2020).  Flexible: the preconditioned directions z_i are kept and x += Z y.
+// Options: the basis and the z_i stored in FP32 (krylov_fp32; every product,
+// norm and update still in FP64), and the second pass taken only where the
+// first cancelled more than half of ||w||^2 (selective_reorth, the Daniel-
+// Gragg-Kaufman-Stewart test): a step without it reads the basis twice.
 #include <cmath>
 #include <stdexcept>
 
@@ -37,7 +41,7 @@ namespace gg {
 constexpr int kThreads = 256;
 constexpr int kRedThreads = 1024;
 constexpr int kSlice = 2048;  // elements per block of the Gram products
-constexpr int kSlice2 = 512;  // elements per block of the fused update + second Gram products
+constexpr int kSlice2 = 1024;  // elements per block of the fused update + second Gram products
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -154,57 +158,162 @@ __global__ void __launch_bounds__(kRedThreads) restart_kernel(GgState *st, const
     }
 }
 
-// v_0 = r * scale (skipped once the solve is done)
+// v_0 = r * scale (skipped once the solve is done).  TB: the basis' storage type (double, or float
+// with every product, norm and update still formed in FP64)
+template <typename TB>
 __global__ void __launch_bounds__(kThreads) scale0_kernel(long long n, const double *__restrict__ r,
-                                                          double *const *__restrict__ V, const GgState *st) {
+                                                          TB *const *__restrict__ V, const GgState *st) {
     if (st->done) return;
     const double sc = st->scale;
-    double *v0 = V[0];
+    TB *v0 = V[0];
     for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
-        v0[e] = r[e] * sc;
+        v0[e] = (TB)(r[e] * sc);
 }
 
 // dst = V[i] (the preconditioner's input buffer)
-__global__ void __launch_bounds__(kThreads) gather_kernel(long long n, const double *const *__restrict__ V,
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) gather_kernel(long long n, const TB *const *__restrict__ V,
                                                           const GgState *st, double *__restrict__ dst) {
-    const double *src = V[st->i];
+    const TB *src = V[st->i];
     for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
-        dst[e] = src[e];
+        dst[e] = (double)src[e];
 }
 
-// Z[i] = src (the preconditioner's output, kept for the flexible update)
-__global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, const double *__restrict__ src,
-                                                           double *const *__restrict__ Z, const GgState *st) {
-    double *dst = Z[st->i];
-    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
-        dst[e] = src[e];
+// Z[i] = src (the preconditioner's output, kept for the flexible update).  With an FP32 basis and
+// round_src set, src is replaced by its FP32 rounding too, so that the product A z_i that follows and
+// the update x += Z y use the same direction (a preconditioner with FP32 output needs no rounding).
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, double *__restrict__ src,
+                                                           TB *const *__restrict__ Z, const GgState *st, int round_src) {
+    TB *dst = Z[st->i];
+    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
+        const TB v = (TB)src[e];
+        dst[e] = v;
+        if (round_src) src[e] = (double)v;
+    }
 }
 
-// Block x: partial <V[k], w> over the x-th slice of kSlice elements for every
-// k <= i.  The slice of w is staged in shared memory once and each basis
-// vector is streamed past it; warps reduce with shuffles and combine through
-// shared memory once at the end.
-__global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const double *const *__restrict__ V,
+// Four consecutive entries (a quad) of a basis vector, of w or of x as FP64 values; every vector
+// starts on a 32-byte boundary, so a quad at an index divisible by 4 is one float4 or two double2.
+__device__ __forceinline__ void ld4(const double *p, double v[4]) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const float *p, double v[4]) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+}
+__device__ __forceinline__ void st4(double *p, const double v[4]) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(float *p, const double v[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
+// Quad q of a vector of n entries; the entries past n of the last, partial quad read as 0.
+template <typename T>
+__device__ __forceinline__ void ld4n(const T *p, long long q, long long n, double v[4]) {
+    if (4 * q + 3 < n) {
+        ld4(p + 4 * q, v);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) v[r] = 4 * q + r < n ? (double)p[4 * q + r] : 0.0;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st4n(T *p, long long q, long long n, const double v[4]) {
+    if (4 * q + 3 < n) {
+        st4(p + 4 * q, v);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (4 * q + r < n) p[4 * q + r] = (T)v[r];
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// sum of row[0..G) over one warp (the result in every lane)
+__device__ __forceinline__ double warp_row_sum(const double *__restrict__ row, int G, int lane) {
+    double v = 0.0;
+    for (int j = lane; j < G; j += 32) v += row[j];
+    return warp_sum(v);
+}
+
+// Block x: partial <V[k], w> over the x-th slice of kSlice elements for every k <= i.  Each thread
+// keeps its two quads of w in registers and streams the same quads of every basis vector past them,
+// two vectors at a time (eight loads in flight); warps reduce with shuffles and combine through shared
+// memory once at the end.
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const TB *const *__restrict__ V,
                                                         const GgState *st, const double *__restrict__ w,
                                                         double *__restrict__ partials) {
-    __shared__ double ws[kSlice];
+    static_assert(kSlice == kThreads * 8, "two quads per thread");
     __shared__ double part[kGgMaxK + 2][kThreads / 32];
-    const long long e0 = (long long)blockIdx.x * kSlice;
-    const int len = (int)min((long long)kSlice, n - e0);
-    for (int j = threadIdx.x; j < len; j += kThreads) ws[j] = w[e0 + j];
-    __syncthreads();
-    const int m = st->i + 1, kend = m;
+    const long long q0 = (long long)blockIdx.x * (kSlice / 4) + threadIdx.x, q1 = q0 + kThreads;
+    double w0[4], w1[4];
+    ld4n(w, q0, n, w0);
+    ld4n(w, q1, n, w1);
+    const int m = st->i + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < kend; ++k) {
-        const double *v = V[k] + e0;
-        double acc = 0.0;
-        for (int j = threadIdx.x; j < len; j += kThreads) acc = fma(v[j], ws[j], acc);
+    int k = 0;
+    for (; k + 1 < m; k += 2) {
+        double a0[4], a1[4], b0[4], b1[4];
+        ld4n(V[k], q0, n, a0);
+        ld4n(V[k], q1, n, a1);
+        ld4n(V[k + 1], q0, n, b0);
+        ld4n(V[k + 1], q1, n, b1);
+        double sa = 0.0, sb = 0.0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) part[k][warp] = acc;
+        for (int r = 0; r < 4; ++r) {
+            sa = fma(a0[r], w0[r], sa);
+            sb = fma(b0[r], w0[r], sb);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            sa = fma(a1[r], w1[r], sa);
+            sb = fma(b1[r], w1[r], sb);
+        }
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            part[k][warp] = sa;
+            part[k + 1][warp] = sb;
+        }
+    }
+    if (k < m) {
+        double a0[4], a1[4];
+        ld4n(V[k], q0, n, a0);
+        ld4n(V[k], q1, n, a1);
+        double sa = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) sa = fma(a0[r], w0[r], sa);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) sa = fma(a1[r], w1[r], sa);
+        sa = warp_sum(sa);
+        if (lane == 0) part[k][warp] = sa;
+    }
+    {  // row m: <w, w> (the selective second pass compares it with the first pass' projection)
+        double sw = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) sw = fma(w0[r], w0[r], sw);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) sw = fma(w1[r], w1[r], sw);
+        sw = warp_sum(sw);
+        if (lane == 0) part[m][warp] = sw;
     }
     __syncthreads();
-    if (threadIdx.x < kend) {
+    if (threadIdx.x <= m) {
         double v = 0.0;
 #pragma unroll
         for (int q = 0; q < kThreads / 32; ++q) v += part[threadIdx.x][q];
@@ -212,60 +321,122 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const doubl
     }
 }
 
-// h[k] = sum of partials row k, k <= i (one warp per row)
+// h1[k] = sum of partials row k, k <= i (one warp per row), and ||w||^2 (row i + 1).  With the
+// selective second pass (P.selective) the step skips it when the first pass kept more than half of
+// ||w||^2, i.e. ||w - V h1||^2 = ||w||^2 - ||h1||^2 > ||w||^2 / 2 (the Daniel-Gragg-Kaufman-Stewart
+// criterion with eta = 1/sqrt(2)): then h2 = h1, h1 = 0 and sig = ||w||^2, so that the Arnoldi and
+// final kernels (which use h1 + h2, sig - ||h2||^2 and w - V h2) finish the step from the first pass.
 __global__ void __launch_bounds__(kRedThreads) reduce_h_kernel(const double *__restrict__ partials, int G,
-                                                               const GgState *st, double *__restrict__ h) {
+                                                               GgState *st, GgParams P, GgWork W) {
+    __shared__ double ww;
     const int m = st->i + 1, lane = threadIdx.x & 31;
-    for (int k = threadIdx.x >> 5; k < m; k += kRedThreads / 32) {
-        double v = 0.0;
-        for (int j = lane; j < G; j += 32) v += partials[(long long)k * G + j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) h[k] = v;
+    for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
+        const double v = warp_row_sum(partials + (long long)k * G, G, lane);
+        if (lane == 0) {
+            if (k < m) W.h1[k] = v;
+            else ww = v;
+        }
     }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    int skip = 0;
+    if (P.selective) {
+        double ss = 0.0;
+        for (int k = 0; k < m; ++k) ss += W.h1[k] * W.h1[k];
+        const double e2 = ww - ss;
+        skip = e2 > 0.5 * ww ? 1 : 0;
+        if (skip) {
+            for (int k = 0; k < m; ++k) {
+                W.h2[k] = W.h1[k];
+                W.h1[k] = 0.0;
+            }
+            st->sig = ww;
+        }
+    }
+    st->skip = skip;
 }
 
 // The first update and the second Gram products in one pass over the basis:
 // w -= sum_{k <= i} h[k] V[k], then partial <V[k], w> (k <= i) and <w, w> of
-// the updated w over the block's slice of kSlice2 elements.  A thread handles
-// one element at a time: it reads that element of every V[k] for the update
-// and again for the products right after, from L1 / L2, so the basis crosses
-// HBM once (the separate update and product kernels read it twice).
-__global__ void __launch_bounds__(kThreads) update_dots_kernel(long long n, const double *const *__restrict__ V,
+// the updated w over the block's slice of kSlice2 elements (one quad per thread).
+// The update reads the quad of every V[k], two vectors at a time, and the
+// products read it again right after, from L1 / L2, so the basis crosses HBM
+// once (separate update and product kernels would read it twice); the products
+// of two vectors are reduced over the warp together.
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) update_dots_kernel(long long n, const TB *const *__restrict__ V,
                                                                const GgState *st, const double *__restrict__ h,
                                                                double *__restrict__ w, double *__restrict__ partials) {
-    __shared__ const double *vs[kGgMaxK + 2];
+    static_assert(kSlice2 == kThreads * 4, "one quad per thread");
+    __shared__ const TB *vs[kGgMaxK + 2];
     __shared__ double hs[kGgMaxK + 2];
     __shared__ double part[kGgMaxK + 2][kThreads / 32];
+    if (st->skip) return;  // the selective rule kept the first pass
     const int m = st->i + 1;
     for (int k = threadIdx.x; k < m; k += kThreads) {
         vs[k] = V[k];
         hs[k] = h[k];
     }
-    for (int q = threadIdx.x; q < (m + 1) * (kThreads / 32); q += kThreads) part[q / (kThreads / 32)][q % (kThreads / 32)] = 0.0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long e0 = (long long)blockIdx.x * kSlice2;
-    for (int r = 0; r < kSlice2 / kThreads; ++r) {
-        const long long e = e0 + (long long)r * kThreads + threadIdx.x;
-        const bool live = e < n;
-        double sv = live ? w[e] : 0.0;
-        if (live) {
-            for (int k = 0; k < m; ++k) sv = fma(-hs[k], vs[k][e], sv);
-            w[e] = sv;
-        }
-        for (int k = 0; k <= m; ++k) {  // uniform trip count: every lane takes part in the shuffles
-            double v = live ? (k < m ? vs[k][e] : sv) * sv : 0.0;
+    const long long q = (long long)blockIdx.x * (kSlice2 / 4) + threadIdx.x;
+    const bool live = 4 * q < n;
+    double sv[4] = {0.0, 0.0, 0.0, 0.0};
+    if (live) {
+        ld4n(w, q, n, sv);
+        int k = 0;
+        for (; k + 1 < m; k += 2) {
+            double a[4], b[4];
+            ld4n(vs[k], q, n, a);
+            ld4n(vs[k + 1], q, n, b);
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) part[k][warp] += v;
+            for (int r = 0; r < 4; ++r) sv[r] = fma(-hs[k], a[r], sv[r]);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) sv[r] = fma(-hs[k + 1], b[r], sv[r]);
+        }
+        if (k < m) {
+            double a[4];
+            ld4n(vs[k], q, n, a);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) sv[r] = fma(-hs[k], a[r], sv[r]);
+        }
+        st4n(w, q, n, sv);
+    }
+    for (int k = 0; k <= m; k += 2) {  // uniform trip count: every lane takes part in the shuffles
+        double v0 = 0.0, v1 = 0.0;
+        if (live) {
+            double a[4], b[4];
+            if (k < m)
+                ld4n(vs[k], q, n, a);
+            else
+#pragma unroll
+                for (int r = 0; r < 4; ++r) a[r] = sv[r];
+            if (k + 1 < m)
+                ld4n(vs[k + 1], q, n, b);
+            else
+#pragma unroll
+                for (int r = 0; r < 4; ++r) b[r] = k + 1 == m ? sv[r] : 0.0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                v0 = fma(a[r], sv[r], v0);
+                v1 = fma(b[r], sv[r], v1);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+            v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        }
+        if (lane == 0) {
+            part[k][warp] = v0;
+            if (k + 1 <= m) part[k + 1][warp] = v1;
         }
     }
     __syncthreads();
     if (threadIdx.x <= m) {
         double v = 0.0;
 #pragma unroll
-        for (int q = 0; q < kThreads / 32; ++q) v += part[threadIdx.x][q];
+        for (int qq = 0; qq < kThreads / 32; ++qq) v += part[threadIdx.x][qq];
         partials[(long long)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
 }
@@ -277,15 +448,16 @@ __global__ void __launch_bounds__(kRedThreads) arnoldi_kernel(const double *__re
                                                               cudaGraphConditionalHandle h_in) {
     __shared__ double sig;
     const int i0 = st->i, m = i0 + 1, lane = threadIdx.x & 31;
-    // second-pass coefficients h2[k], k < m, and ||w||^2 (row m)
-    for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
-        double v = 0.0;
-        for (int j = lane; j < G; j += 32) v += partials[(long long)k * G + j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) {
-            if (k < m) W.h2[k] = v;
-            else sig = v;
+    if (st->skip) {  // no second pass: h2 and ||w||^2 come from the first (reduce_h_kernel)
+        if (threadIdx.x == 0) sig = st->sig;
+    } else {
+        // second-pass coefficients h2[k], k < m, and ||w||^2 (row m)
+        for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
+            const double v = warp_row_sum(partials + (long long)k * G, G, lane);
+            if (lane == 0) {
+                if (k < m) W.h2[k] = v;
+                else sig = v;
+            }
         }
     }
     __syncthreads();
@@ -351,33 +523,56 @@ __global__ void __launch_bounds__(kRedThreads) arnoldi_kernel(const double *__re
     cudaGraphSetConditional(h_in, end ? 0u : 1u);
 }
 
-// v_{m} = (w - sum_{k < m} h2[k] V[k]) * scale, skipped at a cycle end
-__global__ void __launch_bounds__(kThreads) final_kernel(long long n, double *const *__restrict__ V,
+// v_{m} = (w - sum_{k < m} h2[k] V[k]) * scale, skipped at a cycle end; a quad per thread and trip,
+// two basis vectors per step of the sum
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) final_kernel(long long n, TB *const *__restrict__ V,
                                                          const GgState *st, const double *__restrict__ h,
                                                          const double *__restrict__ w) {
-    __shared__ const double *vs[kGgMaxK + 2];
+    __shared__ const TB *vs[kGgMaxK + 2];
     __shared__ double hs[kGgMaxK + 2];
     if (!st->cont) return;
     const int m = st->m;
     const double sc = st->scale;
-    double *dst = V[m];
+    TB *dst = V[m];
     for (int k = threadIdx.x; k < m; k += kThreads) {
         vs[k] = V[k];
         hs[k] = h[k];
     }
     __syncthreads();
-    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
-        double s = w[e];
-        for (int k = 0; k < m; ++k) s = fma(-hs[k], vs[k][e], s);
-        dst[e] = s * sc;
+    const long long nq = (n + 3) / 4;
+    for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < nq; q += (long long)gridDim.x * kThreads) {
+        double s[4];
+        ld4n(w, q, n, s);
+        int k = 0;
+        for (; k + 1 < m; k += 2) {
+            double a[4], b[4];
+            ld4n(vs[k], q, n, a);
+            ld4n(vs[k + 1], q, n, b);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) s[r] = fma(-hs[k], a[r], s[r]);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) s[r] = fma(-hs[k + 1], b[r], s[r]);
+        }
+        if (k < m) {
+            double a[4];
+            ld4n(vs[k], q, n, a);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) s[r] = fma(-hs[k], a[r], s[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) s[r] *= sc;
+        st4n(dst, q, n, s);
     }
 }
 
-// x += sum_{j < i} y[j] Z[j] (latest direction first, as the host update)
-__global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, double *const *__restrict__ Z,
+// x += sum_{j < i} y[j] Z[j] (latest direction first, as the host update); a quad per thread and trip,
+// four directions per step of the sum
+template <typename TB>
+__global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, TB *const *__restrict__ Z,
                                                             const GgState *st, const double *__restrict__ y,
                                                             double *__restrict__ x) {
-    __shared__ const double *zs[kGgMaxK];
+    __shared__ const TB *zs[kGgMaxK];
     __shared__ double ys[kGgMaxK];
     const int i = st->i;
     if (i == 0) return;
@@ -386,10 +581,27 @@ __global__ void __launch_bounds__(kThreads) update_x_kernel(long long n, double 
         ys[k] = y[k];
     }
     __syncthreads();
-    for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
-        double xe = x[e];
-        for (int j = i - 1; j >= 0; --j) xe = fma(ys[j], zs[j][e], xe);
-        x[e] = xe;
+    const long long nq = (n + 3) / 4;
+    for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < nq; q += (long long)gridDim.x * kThreads) {
+        double xe[4];
+        ld4n(x, q, n, xe);
+        int j = i - 1;
+        for (; j >= 3; j -= 4) {
+            double a[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ld4n(zs[j - u], q, n, a[u]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) xe[r] = fma(ys[j - u], a[u][r], xe[r]);
+        }
+        for (; j >= 0; --j) {
+            double a[4];
+            ld4n(zs[j], q, n, a);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) xe[r] = fma(ys[j], a[r], xe[r]);
+        }
+        st4n(x, q, n, xe);
     }
 }
 
@@ -480,6 +692,7 @@ void GraphGmres::prepare(Solver &S) {
     G = div_up(nn, gg::kSlice);  // blocks of the Gram products and norms: one slice each
     G2 = div_up(nn, gg::kSlice2);  // blocks of the fused update + second products
     G1 = std::max(1, std::min(8 * sm_count(), div_up(nn, gg::kThreads)));
+    Gq = std::max(1, div_up(div_up(nn, 4), gg::kThreads));  // one quad per thread
     state.alloc(1);
     // work: rs (k+1), c (k), sn (k), h1 (k+2), h2 (k+2), y (k), hh ((k+1) k)
     const size_t wsz = (size_t)(k + 1) + 2 * k + 2 * (k + 2) + k + (size_t)(k + 1) * k;
@@ -506,7 +719,21 @@ void GraphGmres::prepare(Solver &S) {
     std::vector<double *> vp, zp;
     for (int j = 0; j <= k; ++j) vp.push_back(g.p[j].get());
     own_z.clear();
-    if ((int)g.zf.size() >= k) {
+    fp32 = prm.krylov_fp32 != 0 ? 1 : 0;
+    basis32.release();
+    if (fp32) {
+        // FP32 basis: v_0..v_k then z_0..z_{k-1}, one allocation; each vector starts on a 256-byte
+        // boundary (the kernels move four entries per access)
+        const size_t stride = ((size_t)nn + 63) / 64 * 64;
+        basis32.alloc((size_t)(2 * k + 1) * stride);
+        std::vector<float *> v32, z32;
+        for (int j = 0; j <= k; ++j) v32.push_back(basis32.get() + (size_t)j * stride);
+        for (int j = 0; j < k; ++j) z32.push_back(basis32.get() + (size_t)(k + 1 + j) * stride);
+        vptr32.alloc(v32.size());
+        vptr32.upload(v32.data(), v32.size(), S.stream);
+        zptr32.alloc(z32.size());
+        zptr32.upload(z32.data(), z32.size(), S.stream);
+    } else if ((int)g.zf.size() >= k) {
         for (int j = 0; j < k; ++j) zp.push_back(g.zf[j].get());
     } else {
         for (int j = 0; j < k; ++j) {
@@ -529,6 +756,7 @@ void GraphGmres::prepare(Solver &S) {
     P.a_tol = prm.a_tol;
     P.convfac = prm.convfac_threshold;
     P.stall = prm.stall_ratio;
+    P.selective = prm.selective_reorth != 0 ? 1 : 0;
     JX_CUDA(cudaStreamSynchronize(s));
     reset_graph();
 }
@@ -536,7 +764,8 @@ void GraphGmres::prepare(Solver &S) {
 bool GraphGmres::matches(const SolverParams &prm) const {
     return prm.k_dim == P.k && prm.max_iter == P.max_iter && prm.min_iter == P.min_iter &&
            prm.is_check_restarted == P.check_restarted && prm.tol == P.tol && prm.a_tol == P.a_tol &&
-           prm.convfac_threshold == P.convfac && prm.stall_ratio == P.stall;
+           prm.convfac_threshold == P.convfac && prm.stall_ratio == P.stall && (prm.krylov_fp32 != 0) == (fp32 != 0) &&
+           (prm.selective_reorth != 0) == (P.selective != 0);
 }
 
 void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
@@ -548,6 +777,9 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
     double *b = S.b.get(), *x = S.x.get(), *r = S.gmres.r.get(), *w = S.gmres.w.get();
     double *const *V = vptr.get();
     double *const *Z = zptr.get();
+    float *const *V32 = vptr32.get();
+    float *const *Z32 = zptr32.get();
+    const bool f32 = fp32 != 0;
     GgState *st = state.get();
     double *pt = partials.get();
     const unsigned long long c0 = launch_count();
@@ -572,31 +804,52 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         JX_LAUNCH_CHECK();
         restart_kernel<<<1, kRedThreads, 0, s1>>>(st, pt, G, P, W, norms.get(), h_out, h_in);
         JX_LAUNCH_CHECK();
-        scale0_kernel<<<G1, kThreads, 0, s1>>>(nn, r, V, st);
+        if (f32)
+            scale0_kernel<float><<<G1, kThreads, 0, s1>>>(nn, r, V32, st);
+        else
+            scale0_kernel<double><<<G1, kThreads, 0, s1>>>(nn, r, V, st);
         JX_LAUNCH_CHECK();
         cudaGraph_t body_in = add_while(s1, h_in);
         c2 = launch_count();
         JX_CUDA(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        gather_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, cin.get());
+        if (f32)
+            gather_kernel<float><<<G1, kThreads, 0, s2>>>(nn, V32, st, cin.get());
+        else
+            gather_kernel<double><<<G1, kThreads, 0, s2>>>(nn, V, st, cin.get());
         JX_LAUNCH_CHECK();
         S.cpr.apply_enqueue(cin.get(), cout.get(), s2);
-        scatter_kernel<<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st);
+        if (f32)
+            scatter_kernel<float><<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z32, st, 1);
+        else
+            scatter_kernel<double><<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st, 0);
         JX_LAUNCH_CHECK();
         bsr_spmv<double, double>(A, 1.0, cout.get(), 0.0, w, kerr, s2, staged);
-        dots_kernel<<<G, kThreads, 0, s2>>>(nn, V, st, w, pt);
+        if (f32)
+            dots_kernel<float><<<G, kThreads, 0, s2>>>(nn, V32, st, w, pt);
+        else
+            dots_kernel<double><<<G, kThreads, 0, s2>>>(nn, V, st, w, pt);
         JX_LAUNCH_CHECK();
-        reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, W.h1);
+        reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, P, W);
         JX_LAUNCH_CHECK();
-        update_dots_kernel<<<G2, kThreads, 0, s2>>>(nn, V, st, W.h1, w, pt);
+        if (f32)
+            update_dots_kernel<float><<<G2, kThreads, 0, s2>>>(nn, V32, st, W.h1, w, pt);
+        else
+            update_dots_kernel<double><<<G2, kThreads, 0, s2>>>(nn, V, st, W.h1, w, pt);
         JX_LAUNCH_CHECK();
         arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G2, st, P, W, norms.get(), h_in);
         JX_LAUNCH_CHECK();
-        final_kernel<<<G1, kThreads, 0, s2>>>(nn, V, st, W.h2, w);
+        if (f32)
+            final_kernel<float><<<Gq, kThreads, 0, s2>>>(nn, V32, st, W.h2, w);
+        else
+            final_kernel<double><<<Gq, kThreads, 0, s2>>>(nn, V, st, W.h2, w);
         JX_LAUNCH_CHECK();
         cudaGraph_t gchk = nullptr;
         JX_CUDA(cudaStreamEndCapture(s2, &gchk));
         c3 = launch_count();
-        update_x_kernel<<<G1, kThreads, 0, s1>>>(nn, Z, st, W.y, x);
+        if (f32)
+            update_x_kernel<float><<<Gq, kThreads, 0, s1>>>(nn, Z32, st, W.y, x);
+        else
+            update_x_kernel<double><<<Gq, kThreads, 0, s1>>>(nn, Z, st, W.y, x);
         JX_LAUNCH_CHECK();
         JX_CUDA(cudaStreamEndCapture(s1, &gchk));
         c4 = launch_count();
@@ -636,6 +889,42 @@ void GraphGmres::build_single(Solver &S) {
         throw;
     }
     cudaStreamDestroy(cs);
+}
+
+void GraphGmres::orth_native(int m, int reps, const double *w, cudaStream_t s) {
+    using namespace gg;
+    if (!exec || m < 1 || m > k) {
+        set_error("krylov_native: needs a device-GMRES solve first and 1 <= m <= k_dim (%d)", k);
+        throw std::invalid_argument("krylov_native");
+    }
+    GgState h{};
+    h.i = m - 1;
+    h.m = m;
+    h.cont = 1;
+    h.scale = 1.0;
+    state.upload(&h, 1, s);
+    const long long nn = n;
+    GgState *st = state.get();
+    double *pt = partials.get(), *ww = const_cast<double *>(w);
+    for (int r = 0; r < reps; ++r) {
+        if (fp32)
+            dots_kernel<float><<<G, kThreads, 0, s>>>(nn, vptr32.get(), st, ww, pt);
+        else
+            dots_kernel<double><<<G, kThreads, 0, s>>>(nn, vptr.get(), st, ww, pt);
+        JX_LAUNCH_CHECK();
+        reduce_h_kernel<<<1, kRedThreads, 0, s>>>(pt, G, st, P, W);
+        JX_LAUNCH_CHECK();
+        if (fp32)
+            update_dots_kernel<float><<<G2, kThreads, 0, s>>>(nn, vptr32.get(), st, W.h1, ww, pt);
+        else
+            update_dots_kernel<double><<<G2, kThreads, 0, s>>>(nn, vptr.get(), st, W.h1, ww, pt);
+        JX_LAUNCH_CHECK();
+        if (fp32)
+            final_kernel<float><<<Gq, kThreads, 0, s>>>(nn, vptr32.get(), st, W.h2, ww);
+        else
+            final_kernel<double><<<Gq, kThreads, 0, s>>>(nn, vptr.get(), st, W.h2, ww);
+        JX_LAUNCH_CHECK();
+    }
 }
 
 unsigned long long GraphGmres::kernels_run(int iterations, int cycles) const {

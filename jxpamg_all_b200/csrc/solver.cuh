@@ -76,6 +76,10 @@ struct SolverParams {
     int orthog = 0;          // 0 modified Gram-Schmidt (the reference's), 1 classical Gram-Schmidt (one pass)
     int flexible = 0;        // 1: flexible GMRES (stores M^-1 v_j; for inexact / low-precision preconditioners)
     int graph_gmres = 0;     // 1: the whole GMRES solve on the device as one CUDA graph (fast path; flexible, CGS2)
+    int krylov_fp32 = 0;     // graph GMRES: basis and flexible directions stored in FP32 (products, norms,
+                             // Hessenberg, rotations, residuals and x in FP64)
+    int selective_reorth = 0;  // graph GMRES: the second Gram-Schmidt pass only when the first removed
+                               // more than half of ||w||^2 (0: always, classical Gram-Schmidt twice)
     double cheb_lower = 0.3; // Chebyshev interval [lower, upper] * lambda_max(D^-1 A)
     double cheb_upper = 1.1;
     int stage2_lanes = 4;
@@ -173,15 +177,18 @@ struct GgState {
     int i, m, iter, cycles;
     int converged, done, status, first;
     int est_conv, conv_fail, cont, stalled;
-    int iter0, pad;  // iterations at the current cycle's start
+    int iter0;       // iterations at the current cycle's start
+    int skip;        // this step keeps the first Gram-Schmidt pass (selective second pass)
     double b_norm, r_norm, r_norm0, epsilon, normdown, scale, rel;
     double r_cycle;  // true residual norm at the current cycle's start (stall rule)
+    double sig;      // ||w||^2 of a step that skips the second pass
     unsigned long long t_start, t_end;  // device global timer (ns) at the solve's start and end
 };
 struct GgParams {
     int k, max_iter, min_iter, check_restarted;
     double tol, a_tol, convfac;
     double stall;  // SolverParams::stall_ratio
+    int selective;  // SolverParams::selective_reorth
 };
 struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
     double *rs, *c, *sn, *h1, *h2, *y, *hh;
@@ -193,13 +200,16 @@ struct GgWork {  // device arrays: rotations, Hessenberg matrix, coefficients
 // replay a graph of their own; batches record many solvers into one graph.
 struct GraphGmres {
     long long n = 0;
-    int k = 0, max_iter = 0, G = 1, G1 = 1, G2 = 1;
+    int k = 0, max_iter = 0, G = 1, G1 = 1, G2 = 1, Gq = 1;
     GgParams P{};
     GgWork W{};
     DevBuf<GgState> state;
     DevBuf<double> work, partials, norms, summary, cin, cout;
     std::vector<DevBuf<double>> own_z;  // flexible directions when the host GMRES keeps none
     DevBuf<double *> vptr, zptr;
+    int fp32 = 0;              // krylov_fp32: v_0..v_k and z_0..z_{k-1} stored in FP32 (basis32)
+    DevBuf<float> basis32;
+    DevBuf<float *> vptr32, zptr32;
     cudaStream_t aux[2] = {nullptr, nullptr};  // capture streams of the loop bodies
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -214,6 +224,10 @@ struct GraphGmres {
     void record(Solver &S, cudaStream_t s, double *out);
     void build_single(Solver &S);
     unsigned long long kernels_run(int iterations, int cycles) const;
+    // `reps` times the orthogonalisation kernels of one Arnoldi step with m basis vectors (first
+    // products, fused update + second products, final update into v_m), outside the graph, on the
+    // basis the last solve left and the work vector w (profiling and roofline timing)
+    void orth_native(int m, int reps, const double *w, cudaStream_t s);
     // summary: iterations, converged, rel. residual, status, t_start, t_end, cycles, device error flags
     GmresResult result_from(const double *summary_host, cudaStream_t s, bool with_norms);
 };

@@ -76,6 +76,7 @@ def _declare_solver(lib):
     lib.jxcpr_solver_level_info.argtypes = [P, c_int, P, P, P, P]
     lib.jxcpr_solver_stage2_native.argtypes = [P, c_int]
     lib.jxcpr_solver_level_native.argtypes = [P, c_int, c_int, c_int]
+    lib.jxcpr_solver_krylov_native.argtypes = [P, c_int, c_int]
     lib.jxcpr_solver_level_stored_values.argtypes = [P, c_int, P]
     lib.jxcpr_solver_apply_bytes.argtypes = [P, P]
     lib.jxcpr_stage2_chunk_order.argtypes = [c_int, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int]

@@ -28,7 +28,8 @@ class CprGmres:
     pressure_index, stage1_maxit, stage2_maxit, stage1_solver_type,
     stage2_solver_type, decouple, consistent_rhs, smoother_order, coarse_exact,
     use_tma_spmv, precision, bf16_level, fast_smoother, stage2_lanes,
-    learned_fallback, record_features, flexible, graph_gmres.  Real options: tol, a_tol, threshold,
+    learned_fallback, record_features, flexible, graph_gmres, krylov_fp32,
+    selective_reorth.  Real options: tol, a_tol, threshold,
     convfac_threshold, stage2_relax_weight, stage2_omega, strong_threshold,
     cheb_lower, cheb_upper.
 
@@ -37,7 +38,9 @@ class CprGmres:
     2 FP32 + BF16 coarse levels) and fast_smoother (0 multicolour GS /
     l1-Jacobi, 1 Chebyshev-3, 2 learned) select the mixed and learned forms.
     graph_gmres 1 runs the whole GMRES solve on the device as one CUDA graph
-    (fast path only).
+    (fast path only); krylov_fp32 1 stores its basis in FP32 and
+    selective_reorth 1 takes the second Gram-Schmidt pass only where the first
+    cancelled more than half of the new vector's norm.
     """
 
     def __init__(self, **options):

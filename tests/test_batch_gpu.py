@@ -42,6 +42,11 @@ VARIANTS = [
     dict(precision=1, fast_smoother=2),
     dict(precision=2, fast_smoother=1),
     dict(k_dim=8),
+    dict(krylov_fp32=1),
+    dict(precision=0, fast_smoother=0, flexible=0, krylov_fp32=1),
+    dict(k_dim=8, krylov_fp32=1),
+    dict(selective_reorth=1),
+    dict(krylov_fp32=1, selective_reorth=1),
 ]
 
 
