@@ -586,11 +586,45 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if ws == 1 and args.config == "c1" and not args.no_extras:
+            line["details"]["other_workloads"] = other_workloads(args)
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def other_workloads(args):
+    """The three-phase system (config 4) and the uneven batch (config 3) measured by this same run, one
+    child process each after the config-1 measurement (their own JSON lines, summarised): the default
+    bench line then carries every workload's device-timed result."""
+    out = {}
+    for cfg in ("c4", "c3"):
+        cmd = [sys.executable, os.path.abspath(__file__), "--config", cfg, "--steps", str(min(args.steps, 3)),
+               "--warmup", "2", "--no-cpu-baseline", "--no-extras"]
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+        lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+        if p.returncode != 0 or not lines:
+            out[cfg] = {"error": f"exit {p.returncode}: {p.stderr.strip().splitlines()[-1:]}"}
+            continue
+        d = json.loads(lines[-1])
+        t = d.get("details", {})
+        c = d.get("config", {})
+        keep = {"workload": c.get("workload"), "metric": d["metric"], "value": d["value"], "unit": d["unit"],
+                "steps": d["steps"], "ms_per_step": d["ms_per_step"], "e2e": d.get("e2e", {}).get("value"),
+                "roofline_frac": (d.get("roofline") or {}).get("frac"), "clocks": d.get("clocks"),
+                "wall_s": time.perf_counter() - t0}
+        if cfg == "c4":
+            keep.update({"iterations": t.get("iterations"), "plain_fp64_s": t.get("plain_fp64_s"),
+                         "plain_fp64_iterations": t.get("plain_fp64_iterations"),
+                         "speedup_vs_plain_fp64": t.get("speedup_vs_plain_fp64"),
+                         "learned_used": (t.get("learned") or {}).get("learned_used")})
+        else:
+            keep.update({k: c.get(k) for k in ("latency_ms_p50", "latency_ms_p99", "last_finish_ms")})
+        out[cfg] = keep
+    return out
 
 
 # DRAM traffic of the roofline kernels per timed unit (a stage-2 sweep = its colour launches, a Chebyshev
@@ -1008,6 +1042,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="config 1 on one GPU: skip the config-4 and config-3 runs summarised in the line")
     ap.add_argument("--opt", action="append", default=[], metavar="KEY=VALUE",
                     help="override a solver option of the measured path (repeatable)")
     ap.add_argument("--path", default="mixed", choices=["mixed", "plain", "bilu"],
