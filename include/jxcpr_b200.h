@@ -152,7 +152,11 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         (4: CSR stage 2 without autotuning), stage2_chunk (4: stage 2 visits
  *         chunks of this many consecutive block rows in natural order, the
  *         chunks coloured for parallelism; 8 or 16 also accepted; 0: the
- *         level-0 colour order), learned_fallback (1: the probe
+ *         level-0 colour order), tail_rows (0: fast path, the V-cycle's
+ *         levels from the first with at most this many rows, the coarsest
+ *         included, run as one cooperative kernel; 0 one launch per pass),
+ *         tail_ctas (0: that kernel's grid, sized by its largest pass),
+ *         learned_fallback (1: the probe
  *         and the stall guard may replace the learned settings),
  *         record_features (0), thermal (0)
  *   real: tol (1e-6), a_tol (0), threshold (ignored, as in the reference),

@@ -61,6 +61,8 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"fast_smoother", &p.fast_smoother},
                {"stage2_lanes", &p.stage2_lanes},
                {"stage2_chunk", &p.stage2_chunk},
+               {"tail_rows", &p.tail_rows},
+               {"tail_ctas", &p.tail_ctas},
                {"learned_fallback", &p.learned_fallback},
                {"record_features", &p.record_features},
                {"flexible", &p.flexible},

@@ -102,6 +102,8 @@ struct FastOptions {
     double sell_max_mean = 40; // ... and at most this mean row length
     int graphs = 1;            // replay each preconditioner application as one captured CUDA graph
     int dep_launch = 1;        // kernels of an application launched as programmatic dependents (launch_dep)
+    int tail_rows = 0;         // levels from the first with at most this many rows run as one cooperative kernel (0: off)
+    int tail_ctas = 0;         // its grid (0: enough for the largest fused pass, at most the co-resident blocks)
     int autotune = 1;          // time the layouts (CSR with 1..32 lanes, sliced ELL) of every operator, keep the fastest;
                                // 2: share the choice among operators of one shape class (batches)
     // per-level Chebyshev interval overrides (learned); empty = use cheb_lower/upper

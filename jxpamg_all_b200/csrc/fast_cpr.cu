@@ -16,6 +16,7 @@
 
 #include "fast.cuh"
 #include "fast_kernels.cuh"
+#include "fast_tail.cuh"
 
 namespace jxcpr {
 
@@ -561,6 +562,12 @@ struct FastCpr final : FastCprBase {
     DevBuf<float> r32, z32, vt32;  // mixed path: stage-2 vectors in FP32
     CsrView<double> A0;  // FP64 level-0 operator (convergence-factor probe)
     DevBuf<double> pe, pr, pc, partials, nrm;
+    // levels tail_first.. (the coarsest included) run as one cooperative kernel (fast_tail.cuh);
+    // -1: every level launches its own passes
+    int tail_first = -1, tail_kind = VAL_F64, tail_grid = 0;
+    DevBuf<char> tail_desc;
+    DevBuf<GridBarrier> tail_bar;
+    int *amg_err = nullptr;  // the hierarchy's device error flag (a fused-kernel barrier time-out)
 
     int num_levels() const override { return (int)lv.size(); }
     void level_info(int l, int *smoother, int *kind, double *cheb) const override {
@@ -628,6 +635,158 @@ struct FastCpr final : FastCprBase {
         JX_LAUNCH_CHECK();
     }
 
+    // ---- the fused coarse levels (fast_tail.cuh) ---------------------------------------
+    template <typename TV>
+    static tail::Mat<TV> tail_mat(const LevelMat &M, const TV *a) {
+        tail::Mat<TV> m{};
+        m.sell = M.sell;
+        m.lanes = M.lanes;
+        m.nstored = M.nstored;
+        m.ia = M.ia.get();
+        m.ja = M.ja.get();
+        m.perm = M.perm;
+        m.sp = M.sp.get();
+        m.rows = M.rows.get();
+        m.a = a;
+        m.bscale = M.bscale.get();
+        return m;
+    }
+    template <typename TV>
+    void upload_tail(cudaStream_t s) {
+        std::unique_ptr<tail::Desc<TX, TV>> d(new tail::Desc<TX, TV>());
+        const int L = (int)lv.size();
+        d->nlev = L - tail_first;
+        d->nc = nc;
+        d->Ainv = Ainv;
+        for (int l = tail_first; l < L; ++l) {
+            const FastLevel<TX> &Lv = *lv[l];
+            tail::Level<TX, TV> &T = d->lv[l - tail_first];
+            T.n = Lv.n;
+            T.smoother = Lv.smoother;
+            T.f = Lv.f.get();
+            T.u = Lv.u.get();
+            if (l == L - 1) continue;  // the coarsest: f, u and the inverse only
+            const TV *av;
+            if constexpr (std::is_same<TV, double>::value) av = Lv.A.a64.get();
+            else if constexpr (std::is_same<TV, float>::value) av = Lv.A.a32.get();
+            else av = Lv.A.a16.get();
+            T.A = tail_mat<TV>(Lv.A, av);
+            // transfer operators are stored as TX (FP64 path: FP64, mixed path: FP32)
+            if constexpr (std::is_same<TX, double>::value) {
+                T.P = tail_mat<TX>(Lv.P, Lv.P.a64.get());
+                T.R = tail_mat<TX>(Lv.R, Lv.R.a64.get());
+            } else {
+                T.P = tail_mat<TX>(Lv.P, Lv.P.a32.get());
+                T.R = tail_mat<TX>(Lv.R, Lv.R.a32.get());
+            }
+            T.nseg = std::min((int)Lv.A.seg.size(), tail::kMaxSegs);
+            for (int c = 0; c < T.nseg; ++c) T.seg[c] = Lv.A.seg[c];
+            T.npass = 0;
+            if (Lv.smoother == FS_COLOR_GS) {  // FastCpr::smooth's sequence of colour passes
+                const int ncol = (int)Lv.A.seg.size() - 1;
+                int last = -1;
+                for (int rep = 0; rep < 4; ++rep)
+                    for (int g = 0; g < ncol; ++g) {
+                        const int c = (rep & 1) ? ncol - 1 - g : g;
+                        if (c == last) continue;
+                        last = c;
+                        T.pass[T.npass++] = (unsigned char)c;
+                    }
+            }
+            T.c0 = (TX)Lv.cheb[0];
+            T.c1 = (TX)Lv.cheb[1];
+            T.c2 = (TX)Lv.cheb[2];
+            T.dinv = Lv.dinv.get();
+            T.dinv_l1 = Lv.dinv_l1.get();
+            T.r = Lv.r.get();
+            T.z = Lv.z.get();
+            T.y1 = Lv.y1.get();
+            T.y2 = Lv.y2.get();
+        }
+        tail_desc.alloc(sizeof(tail::Desc<TX, TV>));
+        JX_CUDA(cudaMemcpyAsync(tail_desc.get(), d.get(), sizeof(tail::Desc<TX, TV>), cudaMemcpyHostToDevice, s));
+        JX_CUDA(cudaStreamSynchronize(s));
+    }
+    // (Re)writes the fused kernel's description after the smoothers are chosen or switched.
+    void refresh_tail(cudaStream_t s) {
+        if (tail_first <= 0) return;
+        if (tail_kind == VAL_F64) {
+            if constexpr (std::is_same<TX, double>::value) upload_tail<double>(s);
+        } else if (tail_kind == VAL_BF16) {
+            if constexpr (std::is_same<TX, float>::value) upload_tail<__nv_bfloat16>(s);
+        } else {
+            if constexpr (std::is_same<TX, float>::value) upload_tail<float>(s);
+        }
+    }
+    // Chooses the fused levels: every level from the first with at most `rows` rows (the coarsest
+    // included), all stored in one precision, at least one of them smoothed; sizes the grid.
+    void setup_tail(int rows, int ctas, cudaStream_t s) {
+        tail_first = -1;
+        const int L = (int)lv.size();
+        if (rows <= 0 || L < 3) return;
+        int first = -1;
+        for (int l = 1; l < L; ++l)
+            if (lv[l]->n <= rows) {
+                first = l;
+                break;
+            }
+        if (first < 0 || first > L - 2) return;
+        for (int l = first; l < L - 1; ++l) {
+            const LevelMat &A = lv[l]->A;
+            if ((int)A.seg.size() - 1 > tail::kMaxSegs - 1 || lv[l]->n == 0) return;
+        }
+        if (L - first > tail::kMaxLevels) first = L - tail::kMaxLevels;
+        // one storage type over the fused levels (precision 2 changes it at bf16_level)
+        while (first < L - 1 && lv[first]->A.kind != lv[L - 2]->A.kind) ++first;
+        if (first > L - 2) return;
+        tail_first = first;
+        tail_kind = lv[L - 2]->A.kind;
+        void *fn = nullptr;
+        if constexpr (std::is_same<TX, double>::value)
+            fn = (void *)tail::tail_vcycle_kernel<double, double>;
+        else
+            fn = tail_kind == VAL_BF16 ? (void *)tail::tail_vcycle_kernel<float, __nv_bfloat16>
+                                       : (void *)tail::tail_vcycle_kernel<float, float>;
+        int per_sm = 0;
+        JX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
+        long long want = 1;
+        for (int l = first; l < L - 1; ++l) {
+            const LevelMat &A = lv[l]->A;
+            want = std::max(want, (long long)A.nstored * (A.sell ? 1 : A.lanes));
+        }
+        want = std::max(want, (long long)nc * 32);
+        int grid = std::max(1, std::min(std::max(per_sm, 1) * sm_count(), div_up(want, kThreads)));
+        if (ctas > 0) grid = std::min(grid, ctas);
+        tail_grid = grid;
+        tail_bar.alloc(1);
+        refresh_tail(s);
+    }
+    void launch_tail(cudaStream_t s) {
+        JX_CUDA(cudaMemsetAsync(tail_bar.get(), 0, sizeof(GridBarrier), s));
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3(tail_grid);
+        lc.blockDim = dim3(kThreads);
+        lc.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        GridBarrier *bar = tail_bar.get();
+        int *err = amg_err;
+        if constexpr (std::is_same<TX, double>::value) {
+            const auto *d = reinterpret_cast<const tail::Desc<double, double> *>(tail_desc.get());
+            JX_CUDA(cudaLaunchKernelEx(&lc, tail::tail_vcycle_kernel<double, double>, d, bar, err));
+        } else if (tail_kind == VAL_BF16) {
+            const auto *d = reinterpret_cast<const tail::Desc<float, __nv_bfloat16> *>(tail_desc.get());
+            JX_CUDA(cudaLaunchKernelEx(&lc, tail::tail_vcycle_kernel<float, __nv_bfloat16>, d, bar, err));
+        } else {
+            const auto *d = reinterpret_cast<const tail::Desc<float, float> *>(tail_desc.get());
+            JX_CUDA(cudaLaunchKernelEx(&lc, tail::tail_vcycle_kernel<float, float>, d, bar, err));
+        }
+        JX_LAUNCH_CHECK();
+    }
+
     // u0 = V-cycle(f0) from a zero initial guess
     void vcycle_tx(const TX *f0, TX *u0, cudaStream_t s) {
         const int L = (int)lv.size();
@@ -637,15 +796,19 @@ struct FastCpr final : FastCprBase {
             coarse(f0, u0, s);
             return;
         }
-        for (int l = 0; l < L - 1; ++l) {
+        const int top = tail_first > 0 ? tail_first : L - 1;  // levels above the fused ones
+        for (int l = 0; l < top; ++l) {
             FastLevel<TX> &Lv = *lv[l];
             if (Lv.smoother == FS_COLOR_GS && Lv.n) JX_CUDA(cudaMemsetAsync(U(l), 0, sizeof(TX) * Lv.n, s));
             smooth(Lv, F(l), U(l), true, s);
             residual(Lv, F(l), U(l), Lv.r.get(), s);
             spmv(Lv.R, Lv.r.get(), false, lv[l + 1]->f.get(), s);
         }
-        coarse(F(L - 1), U(L - 1), s);
-        for (int l = L - 2; l >= 0; --l) {
+        if (tail_first > 0)
+            launch_tail(s);
+        else
+            coarse(F(L - 1), U(L - 1), s);
+        for (int l = top - 1; l >= 0; --l) {
             FastLevel<TX> &Lv = *lv[l];
             spmv(Lv.P, U(l + 1), true, U(l), s);
             smooth(Lv, F(l), U(l), false, s);
@@ -867,6 +1030,7 @@ struct FastCpr final : FastCprBase {
 
     void set_plain_mode(bool plain) override {
         for (auto &lp : lv) lp->smoother = plain ? lp->smoother_plain : lp->smoother_cfg;
+        refresh_tail(nullptr);
         if (graph_exec) {  // the captured sequence depends on the smoothers
             cudaGraphExecDestroy(graph_exec);
             graph_exec = nullptr;
@@ -1190,6 +1354,8 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
         }
     }
     H.log.mark("fast_stage2", s);
+    F->amg_err = H.err.get();
+    F->setup_tail(opt.tail_rows, opt.tail_ctas, s);
     JX_CUDA(cudaStreamSynchronize(s));
     return F.release();
 }

@@ -74,6 +74,8 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         opt.cheb_upper = prm.cheb_upper;
         opt.stage2_lanes = prm.stage2_lanes;
         opt.stage2_chunk = prm.stage2_chunk;
+        opt.tail_rows = prm.tail_rows;
+        opt.tail_ctas = prm.tail_ctas;
         opt.autotune = prm.autotune;
         opt.graphs = prm.graphs;
         opt.dep_launch = prm.dep_launch;

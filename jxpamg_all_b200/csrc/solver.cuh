@@ -84,6 +84,9 @@ struct SolverParams {
     double cheb_upper = 1.1;
     int stage2_lanes = 4;
     int stage2_chunk = 4;      // fast path: stage 2 in chunk order (4, 8 or 16 consecutive block rows; 0 colour order)
+    int tail_rows = 0;         // fast path: the V-cycle's levels from the first with at most this many rows
+                               // (the coarsest included) run as one cooperative kernel (0: one launch per pass)
+    int tail_ctas = 0;         // its grid (0: sized by the largest fused pass, at most the co-resident blocks)
     int learned_fallback = 1;  // learned mode: keep the plain smoothers when their V-cycle factor is lower
     int record_features = 0;   // fast path: record the per-level features (training data)
 };
