@@ -523,28 +523,51 @@ void chebyshev3_coefficients(double lo, double hi, double c[3]) {
     c[2] = -n3 / n0;
 }
 
+// One power step's scalars on the device: lam = sqrt(<y,y> / <x,x>) and the scale 1 / ||y|| of the
+// next iterate (the correctly rounded FP64 operations the host would do), or the stop flag once a
+// norm is not positive (lam keeps its last value).  st = {lam, scale, stop}.
+__global__ void power_scalars_kernel(const double *__restrict__ nrm, double *st) {
+    if (st[2] != 0.0) return;
+    const double yy = nrm[0], xx = nrm[1];
+    if (!(yy > 0.0) || !(xx > 0.0)) {
+        st[2] = 1.0;
+        return;
+    }
+    st[0] = sqrt(yy / xx);
+    st[1] = 1.0 / sqrt(yy);
+}
+__global__ void power_scale_kernel(int n, const double *__restrict__ st, double *__restrict__ y) {
+    if (st[2] != 0.0) return;
+    const double a = st[1];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = a * y[i];
+}
+
+// lambda_max(D^-1 A) by `iters` power steps from x = 1, with the host reading the result once.
 double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s) {
     const int n = A.nrows;
     if (n == 0) return 1.0;
-    DevBuf<double> dinv(n), x(n), y(n), partials(reduce_partials() + 8), nrm(2);
+    DevBuf<double> dinv(n), x(n), y(n), partials(reduce_partials() + 8), nrm(2), st(3);
     fk::dinv_diag<double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get());
     JX_LAUNCH_CHECK();
     fill_dev(n, 1.0, x.get(), s);
-    double lam = 1.0;
+    const double init[3] = {1.0, 1.0, 0.0};
+    JX_CUDA(cudaMemcpyAsync(st.get(), init, sizeof(init), cudaMemcpyHostToDevice, s));
     for (int it = 0; it < iters; ++it) {
         fk::dinv_a_x<<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get(), x.get(), y.get());
         JX_LAUNCH_CHECK();
         dot_dev(n, y.get(), y.get(), partials.get(), nrm.get(), s);
         dot_dev(n, x.get(), x.get(), partials.get(), nrm.get() + 1, s);
-        double h[2];
-        JX_CUDA(cudaMemcpyAsync(h, nrm.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
-        JX_CUDA(cudaStreamSynchronize(s));
-        if (!(h[0] > 0.0) || !(h[1] > 0.0)) break;
-        lam = sqrt(h[0] / h[1]);
-        scale_dev(n, 1.0 / sqrt(h[0]), y.get(), s);
+        power_scalars_kernel<<<1, 1, 0, s>>>(nrm.get(), st.get());
+        JX_LAUNCH_CHECK();
+        power_scale_kernel<<<div_up(n, kThreads), kThreads, 0, s>>>(n, st.get(), y.get());
+        JX_LAUNCH_CHECK();
         std::swap(x.p, y.p);
     }
-    return lam;
+    double h[3];
+    JX_CUDA(cudaMemcpyAsync(h, st.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    JX_CUDA(cudaStreamSynchronize(s));
+    return h[0];
 }
 
 template <typename TX>

@@ -230,3 +230,22 @@ def test_parallel_setup_reports_failure():
     assert e.value.status == 4 and "system 2" in str(e.value)
     for G in solvers:
         G.close()
+
+
+def test_krylov_native_after_a_solve(systems):
+    """The orthogonalisation kernels queued outside the graph (the profiling / roofline entry point)
+    need a device-GMRES solve first, run on the basis it left, and the next solve starts afresh."""
+    from jxpamg_all_b200 import lib
+
+    s = systems("c0")
+    G = make(s, graph_gmres=1, krylov_fp32=1, k_dim=10)
+    so = lib.load()
+    assert so.jxcpr_solver_krylov_native(G.h, 3, 1) == 4  # no device-GMRES solve yet
+    x0, it0, rel0, conv0 = G.solve(s.b)
+    assert so.jxcpr_solver_krylov_native(G.h, 11, 1) == 4  # m > k_dim
+    lib.check(so.jxcpr_solver_krylov_native(G.h, 5, 3))
+    x1, it1, rel1, conv1 = G.solve(s.b)
+    assert conv0 and conv1 and it0 == it1
+    assert np.array_equal(x0, x1)
+    G.close()
+
