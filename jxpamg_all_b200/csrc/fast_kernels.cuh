@@ -34,7 +34,8 @@ __device__ __forceinline__ TA group_sum(TA v) {
 }
 
 // sum_{k in [kb, ke)} a_k x_{ja_k}, reduced over the V lanes of the group.
-// Two entries per lane per trip keep more loads in flight.
+// Two entries per lane per trip keep more loads in flight; each product is added with one fused
+// multiply-add (the fast path has no bit-exactness contract; the exact path's kernels do not use it).
 template <int V, typename TA, typename TV, typename TX>
 __device__ __forceinline__ TA row_sum(const int *__restrict__ ja, const TV *__restrict__ a, const float *bsc, int kb,
                                       int ke, const TX *x, int lane) {
@@ -43,10 +44,10 @@ __device__ __forceinline__ TA row_sum(const int *__restrict__ ja, const TV *__re
     for (; k + V < ke; k += 2 * V) {
         const int j0 = __ldg(ja + k), j1 = __ldg(ja + k + V);
         const TA a0 = (TA)ldvs(a, bsc, k), a1 = (TA)ldvs(a, bsc, k + V);
-        s0 += a0 * (TA)x[j0];
-        s1 += a1 * (TA)x[j1];
+        s0 = fma(a0, (TA)x[j0], s0);
+        s1 = fma(a1, (TA)x[j1], s1);
     }
-    if (k < ke) s0 += (TA)ldvs(a, bsc, k) * (TA)x[__ldg(ja + k)];
+    if (k < ke) s0 = fma((TA)ldvs(a, bsc, k), (TA)x[__ldg(ja + k)], s0);
     return group_sum<V, TA>(s0 + s1);
 }
 
@@ -97,14 +98,14 @@ struct SellFmt {
                       j3 = __ldg(col + p + 96);
             const TA a0 = (TA)ldvs(a, bscale, p), a1 = (TA)ldvs(a, bscale, p + 32), a2 = (TA)ldvs(a, bscale, p + 64),
                      a3 = (TA)ldvs(a, bscale, p + 96);
-            s0 += a0 * (TA)x[j0];
-            s1 += a1 * (TA)x[j1];
-            s2 += a2 * (TA)x[j2];
-            s3 += a3 * (TA)x[j3];
+            s0 = fma(a0, (TA)x[j0], s0);
+            s1 = fma(a1, (TA)x[j1], s1);
+            s2 = fma(a2, (TA)x[j2], s2);
+            s3 = fma(a3, (TA)x[j3], s3);
         }
         for (; k < w; ++k) {
             const long long p = o + (long long)k * 32;
-            s0 += (TA)ldvs(a, bscale, p) * (TA)x[__ldg(col + p)];
+            s0 = fma((TA)ldvs(a, bscale, p), (TA)x[__ldg(col + p)], s0);
         }
         return (s0 + s1) + (s2 + s3);
     }
