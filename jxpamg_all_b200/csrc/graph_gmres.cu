@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) scale0_kernel(long long n, const dou
 template <typename TB>
 __global__ void __launch_bounds__(kThreads) gather_kernel(long long n, const TB *const *__restrict__ V,
                                                           const GgState *st, double *__restrict__ dst) {
+    grid_dep_wait();
     const TB *src = V[st->i];
     for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads)
         dst[e] = (double)src[e];
@@ -185,6 +186,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(long long n, const TB 
 template <typename TB>
 __global__ void __launch_bounds__(kThreads) scatter_kernel(long long n, double *__restrict__ src,
                                                            TB *const *__restrict__ Z, const GgState *st, int round_src) {
+    grid_dep_wait();
     TB *dst = Z[st->i];
     for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
         const TB v = (TB)src[e];
@@ -260,6 +262,7 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const TB *c
                                                         double *__restrict__ partials) {
     static_assert(kSlice == kThreads * 8, "two quads per thread");
     __shared__ double part[kGgMaxK + 2][kThreads / 32];
+    grid_dep_wait();
     const long long q0 = (long long)blockIdx.x * (kSlice / 4) + threadIdx.x, q1 = q0 + kThreads;
     double w0[4], w1[4];
     ld4n(w, q0, n, w0);
@@ -329,6 +332,7 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(long long n, const TB *c
 __global__ void __launch_bounds__(kRedThreads) reduce_h_kernel(const double *__restrict__ partials, int G,
                                                                GgState *st, GgParams P, GgWork W) {
     __shared__ double ww;
+    grid_dep_wait();
     const int m = st->i + 1, lane = threadIdx.x & 31;
     for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
         const double v = warp_row_sum(partials + (long long)k * G, G, lane);
@@ -371,6 +375,7 @@ __global__ void __launch_bounds__(kThreads) update_dots_kernel(long long n, cons
     __shared__ const TB *vs[kGgMaxK + 2];
     __shared__ double hs[kGgMaxK + 2];
     __shared__ double part[kGgMaxK + 2][kThreads / 32];
+    grid_dep_wait();
     if (st->skip) return;  // the selective rule kept the first pass
     const int m = st->i + 1;
     for (int k = threadIdx.x; k < m; k += kThreads) {
@@ -447,6 +452,7 @@ __global__ void __launch_bounds__(kRedThreads) arnoldi_kernel(const double *__re
                                                               GgParams P, GgWork W, double *__restrict__ norms,
                                                               cudaGraphConditionalHandle h_in) {
     __shared__ double sig;
+    grid_dep_wait();
     const int i0 = st->i, m = i0 + 1, lane = threadIdx.x & 31;
     if (st->skip) {  // no second pass: h2 and ||w||^2 come from the first (reduce_h_kernel)
         if (threadIdx.x == 0) sig = st->sig;
@@ -531,6 +537,7 @@ __global__ void __launch_bounds__(kThreads) final_kernel(long long n, TB *const 
                                                          const double *__restrict__ w) {
     __shared__ const TB *vs[kGgMaxK + 2];
     __shared__ double hs[kGgMaxK + 2];
+    grid_dep_wait();
     if (!st->cont) return;
     const int m = st->m;
     const double sc = st->scale;
@@ -812,36 +819,37 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         cudaGraph_t body_in = add_while(s1, h_in);
         c2 = launch_count();
         JX_CUDA(cudaStreamBeginCaptureToGraph(s2, body_in, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        DepLaunchScope dep(S.prm.dep_launch);  // programmatic edges between the step's kernels
         if (f32)
-            gather_kernel<float><<<G1, kThreads, 0, s2>>>(nn, V32, st, cin.get());
+            launch_dep(gather_kernel<float>, dim3(G1), dim3(kThreads), s2, nn, V32, st, cin.get());
         else
-            gather_kernel<double><<<G1, kThreads, 0, s2>>>(nn, V, st, cin.get());
+            launch_dep(gather_kernel<double>, dim3(G1), dim3(kThreads), s2, nn, V, st, cin.get());
         JX_LAUNCH_CHECK();
         S.cpr.apply_enqueue(cin.get(), cout.get(), s2);
         if (f32)
-            scatter_kernel<float><<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z32, st, 1);
+            launch_dep(scatter_kernel<float>, dim3(G1), dim3(kThreads), s2, nn, cout.get(), Z32, st, 1);
         else
-            scatter_kernel<double><<<G1, kThreads, 0, s2>>>(nn, cout.get(), Z, st, 0);
+            launch_dep(scatter_kernel<double>, dim3(G1), dim3(kThreads), s2, nn, cout.get(), Z, st, 0);
         JX_LAUNCH_CHECK();
         bsr_spmv<double, double>(A, 1.0, cout.get(), 0.0, w, kerr, s2, staged);
         if (f32)
-            dots_kernel<float><<<G, kThreads, 0, s2>>>(nn, V32, st, w, pt);
+            launch_dep(dots_kernel<float>, dim3(G), dim3(kThreads), s2, nn, V32, st, w, pt);
         else
-            dots_kernel<double><<<G, kThreads, 0, s2>>>(nn, V, st, w, pt);
+            launch_dep(dots_kernel<double>, dim3(G), dim3(kThreads), s2, nn, V, st, w, pt);
         JX_LAUNCH_CHECK();
-        reduce_h_kernel<<<1, kRedThreads, 0, s2>>>(pt, G, st, P, W);
+        launch_dep(reduce_h_kernel, dim3(1), dim3(kRedThreads), s2, pt, G, st, P, W);
         JX_LAUNCH_CHECK();
         if (f32)
-            update_dots_kernel<float><<<G2, kThreads, 0, s2>>>(nn, V32, st, W.h1, w, pt);
+            launch_dep(update_dots_kernel<float>, dim3(G2), dim3(kThreads), s2, nn, V32, st, W.h1, w, pt);
         else
-            update_dots_kernel<double><<<G2, kThreads, 0, s2>>>(nn, V, st, W.h1, w, pt);
+            launch_dep(update_dots_kernel<double>, dim3(G2), dim3(kThreads), s2, nn, V, st, W.h1, w, pt);
         JX_LAUNCH_CHECK();
-        arnoldi_kernel<<<1, kRedThreads, 0, s2>>>(pt, G2, st, P, W, norms.get(), h_in);
+        launch_dep(arnoldi_kernel, dim3(1), dim3(kRedThreads), s2, pt, G2, st, P, W, norms.get(), h_in);
         JX_LAUNCH_CHECK();
         if (f32)
-            final_kernel<float><<<Gq, kThreads, 0, s2>>>(nn, V32, st, W.h2, w);
+            launch_dep(final_kernel<float>, dim3(Gq), dim3(kThreads), s2, nn, V32, st, W.h2, w);
         else
-            final_kernel<double><<<Gq, kThreads, 0, s2>>>(nn, V, st, W.h2, w);
+            launch_dep(final_kernel<double>, dim3(Gq), dim3(kThreads), s2, nn, V, st, W.h2, w);
         JX_LAUNCH_CHECK();
         cudaGraph_t gchk = nullptr;
         JX_CUDA(cudaStreamEndCapture(s2, &gchk));
