@@ -108,6 +108,8 @@ struct FastOptions {
                                // 2: share the choice among operators of one shape class (batches)
     // per-level Chebyshev interval overrides (learned); empty = use cheb_lower/upper
     std::vector<double> level_lower, level_upper;
+    // per-level lambda_max(D^-1 A) after 12 power steps, from the learned-features pass (0: compute)
+    std::vector<double> level_lambda;
 };
 
 // Precision-independent interface.
@@ -158,7 +160,8 @@ FastCprBase *make_fast_cpr(Amg &H, const BsrView<double> &A, const CprConfig &cf
                            cudaStream_t s);
 
 // Largest eigenvalue estimate of D^-1 A (D = diag), FP64 power iteration.
-double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s);
+double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s, int iters2 = 0,
+                           double *lam2 = nullptr);
 // Coefficients of the degree-2 polynomial p with 1 - t p(t) = the degree-3
 // Chebyshev polynomial of [lo, hi] normalised to 1 at t = 0.
 void chebyshev3_coefficients(double lo, double hi, double c[3]);

@@ -544,16 +544,25 @@ __global__ void power_scale_kernel(int n, const double *__restrict__ st, double 
 }
 
 // lambda_max(D^-1 A) by `iters` power steps from x = 1, with the host reading the result once.
-double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s) {
+// iters2 > iters: the power steps go on to iters2 and *lam2 receives that estimate too (the same
+// sequence of iterates, so each value equals a separate run of that many steps).
+double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s, int iters2, double *lam2) {
     const int n = A.nrows;
-    if (n == 0) return 1.0;
+    if (n == 0) {
+        if (lam2) *lam2 = 1.0;
+        return 1.0;
+    }
     DevBuf<double> dinv(n), x(n), y(n), partials(reduce_partials() + 8), nrm(2), st(3);
     fk::dinv_diag<double><<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get());
     JX_LAUNCH_CHECK();
     fill_dev(n, 1.0, x.get(), s);
     const double init[3] = {1.0, 1.0, 0.0};
     JX_CUDA(cudaMemcpyAsync(st.get(), init, sizeof(init), cudaMemcpyHostToDevice, s));
-    for (int it = 0; it < iters; ++it) {
+    DevBuf<double> at_iters(1);
+    const int total = (lam2 && iters2 > iters) ? iters2 : iters;
+    for (int it = 0; it < total; ++it) {
+        if (it == iters)
+            JX_CUDA(cudaMemcpyAsync(at_iters.get(), st.get(), sizeof(double), cudaMemcpyDeviceToDevice, s));
         fk::dinv_a_x<<<div_up(n, kThreads), kThreads, 0, s>>>(n, A.ia, A.ja, A.a, dinv.get(), x.get(), y.get());
         JX_LAUNCH_CHECK();
         dot_dev(n, y.get(), y.get(), partials.get(), nrm.get(), s);
@@ -564,9 +573,15 @@ double estimate_lambda_max(const CsrView<double> &A, int iters, cudaStream_t s) 
         JX_LAUNCH_CHECK();
         std::swap(x.p, y.p);
     }
-    double h[3];
+    double h[3], first = 0.0;
     JX_CUDA(cudaMemcpyAsync(h, st.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    if (total > iters) JX_CUDA(cudaMemcpyAsync(&first, at_iters.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
     JX_CUDA(cudaStreamSynchronize(s));
+    if (total > iters) {
+        *lam2 = h[0];
+        return first;
+    }
+    if (lam2) *lam2 = h[0];
     return h[0];
 }
 
@@ -1232,7 +1247,9 @@ static FastCprBase *build_fast(Amg &H, const BsrView<double> &A, const CprConfig
                 }
             }
             if (sm == FS_CHEB) {
-                Lv.lambda_max = estimate_lambda_max(Av, 12, s);
+                // the learned-features pass ran the same power steps on this operator already
+                const bool known = (size_t)l < opt.level_lambda.size() && opt.level_lambda[l] > 0.0;
+                Lv.lambda_max = known ? opt.level_lambda[l] : estimate_lambda_max(Av, 12, s);
                 const double lo = (size_t)l < opt.level_lower.size() ? opt.level_lower[l] : opt.cheb_lower;
                 const double hi = (size_t)l < opt.level_upper.size() ? opt.level_upper[l] : opt.cheb_upper;
                 Lv.cheb_lo = lo * Lv.lambda_max;

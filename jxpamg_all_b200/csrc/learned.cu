@@ -228,7 +228,8 @@ void mlp_forward_host(const float *w, const float *x, float *y) {
     }
 }
 
-void level_features(const CsrView<double> &A, int level, int prev_n, float *out, cudaStream_t s) {
+void level_features(const CsrView<double> &A, int level, int prev_n, float *out, cudaStream_t s,
+                    double *lambda12) {
     const int n = A.nrows;
     for (int k = 0; k < kMlpIn; ++k) out[k] = 0.0f;
     if (n == 0) return;
@@ -245,7 +246,8 @@ void level_features(const CsrView<double> &A, int level, int prev_n, float *out,
             const double v = h[(size_t)b * kFeatStats + k];
             t[k] = (k == 1 || k == 3) ? std::max(t[k], v) : t[k] + v;
         }
-    const double lam = estimate_lambda_max(A, 8, s);
+    // 8 power steps for the feature; on to 12 for the Chebyshev estimate of the fast path
+    const double lam = estimate_lambda_max(A, 8, s, lambda12 ? 12 : 0, lambda12);
     const double nd = (double)n, noff = std::max(t[6], 1.0), ndiag = std::max(t[13], 1.0);
     const double mean_nnz = t[0] / nd;
     const double lmean = t[11] / ndiag, lvar = std::max(0.0, t[12] / ndiag - lmean * lmean);
@@ -270,8 +272,11 @@ void level_features(const CsrView<double> &A, int level, int prev_n, float *out,
 double learned_predict_level(LearnedPlan &plan, int level, const CsrView<double> &A, double default_theta,
                              cudaStream_t s) {
     std::vector<float> f(kMlpIn);
-    level_features(A, level, plan.prev_n, f.data(), s);
+    double lam12 = 0.0;
+    level_features(A, level, plan.prev_n, f.data(), s, &lam12);
     plan.prev_n = A.nrows;
+    if ((int)plan.lambda12.size() <= level) plan.lambda12.resize(level + 1, 0.0);
+    plan.lambda12[level] = lam12;
     if ((int)plan.features.size() <= level) plan.features.resize(level + 1);
     plan.features[level] = f;
     if (!plan.active) return default_theta;

@@ -27,12 +27,14 @@ struct LearnedPlan {
     bool active = false;
     bool record = false;     // record features only (no prediction)
     std::vector<double> theta, lower, upper;
+    std::vector<double> lambda12;  // lambda_max(D^-1 A) after 12 power steps, per level (the Chebyshev estimate)
     std::vector<std::vector<float>> features;
     int prev_n = 0;
 };
 
 // Features of level `level` (kMlpIn floats; prev_n = rows of the previous level, 0 at level 0).
-void level_features(const CsrView<double> &A, int level, int prev_n, float *out, cudaStream_t s);
+void level_features(const CsrView<double> &A, int level, int prev_n, float *out, cudaStream_t s,
+                    double *lambda12 = nullptr);
 // Called by the AMG setup before coarsening `level`: records the level's
 // features, runs the MLP (when plan.active) and returns the strength threshold.
 double learned_predict_level(LearnedPlan &plan, int level, const CsrView<double> &A, double default_theta,

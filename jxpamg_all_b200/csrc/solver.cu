@@ -82,6 +82,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         if (plan.active) {
             opt.level_lower = plan.lower;
             opt.level_upper = plan.upper;
+            opt.level_lambda = plan.lambda12;
         }
         fast.reset(make_fast_cpr(amg, A, cfg, opt, s));
         amg.log.mark("fast_build", s);
