@@ -134,6 +134,8 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         rs_range_rows (131072; order 1: the coarsening's first pass on row
  *         ranges of this size, as each process of a distributed run does it,
  *         par_coarsen_ruge.c:37-44; 0 one pass over the level),
+ *         rs_range_rows_coarse (0: as rs_range_rows; the range size on the
+ *         levels below the finest),
  *         coarse_exact (1 substitution in the reference's order, 0 inverse),
  *         dep_launch (1; order 1: the preconditioner's kernels launched as
  *         programmatic dependents inside its CUDA graphs),

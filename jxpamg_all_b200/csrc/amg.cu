@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <future>
+#include <memory>
 #include <vector>
 
 #include "amg.cuh"
@@ -164,22 +165,35 @@ struct ScheduleJob {
     std::vector<int> chunk_order, chunk_seg;
 };
 
-// chunk > 0: also the stage-2 chunk order of the pattern (level 0 of the fast path)
+// chunk > 0: also the stage-2 chunk order of the pattern (level 0 of the fast path), on a host thread
+// of its own beside the Gauss-Seidel schedule
 static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, int chunk, cudaStream_t s) {
     const int n = L.A.nrows;
-    std::vector<int> ia(n + 1), ja(L.A.nnz > 0 ? L.A.nnz : 1);
-    L.A.ia.download(ia.data(), n + 1, s);
-    L.A.ja.download(ja.data(), L.A.nnz, s);
+    auto ia = std::make_shared<std::vector<int>>(n + 1), ja = std::make_shared<std::vector<int>>(L.A.nnz > 0 ? L.A.nnz : 1);
+    L.A.ia.download(ia->data(), n + 1, s);
+    L.A.ja.download(ja->data(), L.A.nnz, s);
     JX_CUDA(cudaStreamSynchronize(s));
-    return std::async(std::launch::async, [n, order, chunk, ia = std::move(ia), ja = std::move(ja)]() {
+    using Chunks = std::pair<std::vector<int>, std::vector<int>>;
+    std::shared_future<Chunks> chunks;
+    if (chunk > 0)
+        chunks = std::async(std::launch::async, [n, chunk, ia, ja]() {
+                     Chunks c;
+                     build_chunk_order_host(n, ia->data(), ja->data(), chunk, c.first, c.second);
+                     return c;
+                 }).share();
+    return std::async(std::launch::async, [n, order, ia, ja, chunks]() {
         ScheduleJob J;
-        build_schedule_host(n, ia.data(), ja.data(), order, true, J.perm[0], J.gptr[0], J.rank[0]);
+        build_schedule_host(n, ia->data(), ja->data(), order, true, J.perm[0], J.gptr[0], J.rank[0]);
         if (order == ORDER_EXACT) {
             J.both = true;
-            build_schedule_host(n, ia.data(), ja.data(), order, false, J.perm[1], J.gptr[1], J.rank[1]);
+            build_schedule_host(n, ia->data(), ja->data(), order, false, J.perm[1], J.gptr[1], J.rank[1]);
         }
         // multicolour: the backward sweep visits the same classes in reverse order (fwd schedule, reversed)
-        if (chunk > 0) build_chunk_order_host(n, ia.data(), ja.data(), chunk, J.chunk_order, J.chunk_seg);
+        if (chunks.valid()) {
+            Chunks c = chunks.get();
+            J.chunk_order = std::move(c.first);
+            J.chunk_seg = std::move(c.second);
+        }
         return J;
     });
 }
@@ -242,12 +256,13 @@ void amg_setup(Amg &H, DeviceCsr &&A0, cudaStream_t s) {
         amg_strength(L.A.view(), L.theta, H.prm.max_row_sum, S, s);
         H.log.mark("strength", s);
         L.cf.assign(n, 0);
-        if (H.prm.rs_range_rows > 0 && n >= 2 * H.prm.rs_range_rows) {
+        const int range_rows = level == 0 ? H.prm.rs_range_rows : H.prm.rs_range_rows_coarse;
+        if (range_rows > 0 && n >= 2 * range_rows) {
             std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1);
             S.ia.download(sia.data(), n + 1, s);
             S.ja.download(sja.data(), S.nnz, s);
             JX_CUDA(cudaStreamSynchronize(s));
-            rs_first_pass_ranges(n, sia.data(), sja.data(), H.prm.rs_range_rows, L.cf.data());
+            rs_first_pass_ranges(n, sia.data(), sja.data(), range_rows, L.cf.data());
         } else {
             // the pattern and its transpose (stable: rows ascending in each column) go to the host
             std::vector<int> sia(n + 1), sja(S.nnz > 0 ? S.nnz : 1), stia(n + 1), stja(S.nnz > 0 ? S.nnz : 1);

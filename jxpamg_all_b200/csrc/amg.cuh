@@ -67,6 +67,7 @@ struct AmgParams {
     int max_colors = 8;    // multicolour mode: levels needing more colours use l1-Jacobi
     double jacobi_mean_row = 12.0;  // multicolour mode: levels with longer mean rows go straight to l1-Jacobi
     int rs_range_rows = 0;  // > 0: the coarsening's first pass runs on row ranges of this size (host threads)
+    int rs_range_rows_coarse = 0;  // the same on the levels below the finest
     int stage2_chunk = 0;   // > 0 (fast path): level 0 also gets the stage-2 chunk order (build_chunk_order_host)
     // Optional per-level strength thresholds: called before level l is
     // coarsened with its operator; returns the threshold to use (learned model).

@@ -54,6 +54,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"coarse_exact", &p.coarse_exact},
                {"max_colors", &p.max_colors},
                {"rs_range_rows", &p.rs_range_rows},
+               {"rs_range_rows_coarse", &p.rs_range_rows_coarse},
                {"dep_launch", &p.dep_launch},
                {"use_tma_spmv", &p.use_tma_spmv},
                {"precision", &p.precision},

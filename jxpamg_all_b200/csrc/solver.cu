@@ -36,6 +36,8 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
     amg.prm.jacobi_mean_row = prm.jacobi_mean_row;
     amg.prm.stage2_chunk = fast_path ? prm.stage2_chunk : 0;
     amg.prm.rs_range_rows = fast_path ? prm.rs_range_rows : 0;
+    amg.prm.rs_range_rows_coarse = fast_path ? (prm.rs_range_rows_coarse > 0 ? prm.rs_range_rows_coarse
+                                                                              : prm.rs_range_rows) : 0;
     amg.prm.strong_threshold = prm.strong_threshold;
     amg.prm.theta_for_level = nullptr;
     fast.reset();

@@ -63,6 +63,7 @@ struct SolverParams {
     // fast path: the coarsening's first pass on row ranges of this many rows, one host thread per
     // range (levels with fewer than twice as many rows, and the exact order always, take one pass)
     int rs_range_rows = 131072;
+    int rs_range_rows_coarse = 0;  // the levels below the finest (0: rs_range_rows)
     int dep_launch = 1;  // fast path: programmatic dependent launches inside each CPR application
     int use_tma_spmv = 0;
     // fast path (smoother_order 1)
