@@ -664,18 +664,24 @@ __global__ void __launch_bounds__(32 * kRapWarps)
                     }
                     next += __popc(fresh_mask);
                     if (FILL) {
+                        // each leader adds its group's products in lane order (the discovery order);
+                        // the warp takes as many shuffle steps as the largest group has members
                         double acc = 0.0;
                         bool first = fresh;
                         if (is_leader && !fresh) acc = vals[h];
-                        for (int src = 0; src < 32; ++src) {
+                        unsigned rem = is_leader ? grp : 0u;
+                        const unsigned steps = __reduce_max_sync(FULL, (unsigned)__popc(rem));
+                        for (unsigned it = 0; it < steps; ++it) {
+                            const int src = rem ? __ffs(rem) - 1 : lane;
                             const double v = __shfl_sync(FULL, prod, src);
-                            if (is_leader && ((grp >> src) & 1u)) {
+                            if (rem) {
                                 if (first) {
                                     acc = v;
                                     first = false;
                                 } else {
                                     acc += v;
                                 }
+                                rem &= rem - 1u;
                             }
                         }
                         if (is_leader) vals[h] = acc;
