@@ -552,53 +552,61 @@ __device__ __forceinline__ int table_slot(int *keys, int *vals, long long tsz, i
 // coarse column are grouped (__match_any_sync) and the group's lowest lane adds
 // the members' products to the column's sum one by one in lane order, so
 // every column's sum is formed in traversal order.  New columns get slots in
-// order of first occurrence.  The row's column table lives in shared memory;
-// a row with more than kRapWarpMaxCols columns sets its overflow flag and is
-// redone by rap_fallback_kernel (one thread, table in global memory).
-static constexpr int kRapTable = 2048;        // shared-memory table entries per warp
-static constexpr int kRapWarpMaxCols = 1024;  // columns a warp row may hold
-static constexpr int kRapWarps = 2;           // warps per block
+// order of first occurrence.  The row's column table lives in shared memory,
+// in two sizes: every row is first tried with a 256-entry table (8 warps per
+// block, many blocks per SM: the rows of the fine levels are short), a row
+// with more than 128 columns again with a 2,048-entry table (2 warps per
+// block), and a row with more than 1,024 columns is redone by
+// rap_fallback_kernel (one thread, table in global memory).  The table only
+// indexes the columns: a row's result does not depend on which size held it.
+// overflow[I]: 0 small table, 1 large table, 2 fallback.
+static constexpr int kRapTableS = 256, kRapWarpsS = 8;   // small tier: entries per warp, warps per block
+static constexpr int kRapTableL = 2048, kRapWarpsL = 2;  // large tier
 
+template <int TBL>
 __device__ __forceinline__ int rap_find(const int *keys, int J) {
-    unsigned h = hash_col(J) & (kRapTable - 1);
+    unsigned h = hash_col(J) & (TBL - 1);
     while (true) {
         const int k = keys[h];
         if (k == J) return (int)h;
         if (k < 0) return -1;
-        h = (h + 1) & (kRapTable - 1);
+        h = (h + 1) & (TBL - 1);
     }
 }
 
+template <int TBL>
 __device__ __forceinline__ int rap_insert(int *keys, int J) {
-    unsigned h = hash_col(J) & (kRapTable - 1);
+    unsigned h = hash_col(J) & (TBL - 1);
     while (true) {
         const int prev = atomicCAS(keys + h, -1, J);
         if (prev == -1 || prev == J) return (int)h;
-        h = (h + 1) & (kRapTable - 1);
+        h = (h + 1) & (TBL - 1);
     }
 }
 
-template <bool FILL>
-__global__ void __launch_bounds__(32 * kRapWarps)
+template <bool FILL, int TBL, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS)
     rap_warp_kernel(int nrows, const int *__restrict__ ria, const int *__restrict__ rja,
                     const double *__restrict__ ra, const int *__restrict__ aia, const int *__restrict__ aja,
                     const double *__restrict__ aa, const int *__restrict__ pia, const int *__restrict__ pja,
                     const double *__restrict__ pa, int *__restrict__ cnt, unsigned char *__restrict__ overflow,
                     const int *__restrict__ cia, int *__restrict__ cja, double *__restrict__ ca) {
+    constexpr int kMaxCols = TBL / 2;  // columns a warp row may hold
+    constexpr unsigned char kTier = TBL == kRapTableS ? 0 : 1;
     extern __shared__ __align__(16) unsigned char rap_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int *keys = reinterpret_cast<int *>(rap_smem) + warp * kRapTable;
-    int *slots = reinterpret_cast<int *>(rap_smem) + kRapWarps * kRapTable + warp * kRapTable;
-    double *vals = reinterpret_cast<double *>(rap_smem + (size_t)2 * kRapWarps * kRapTable * sizeof(int)) +
-                   warp * kRapTable;
+    int *keys = reinterpret_cast<int *>(rap_smem) + warp * TBL;
+    int *slots = reinterpret_cast<int *>(rap_smem) + WARPS * TBL + warp * TBL;
+    double *vals = reinterpret_cast<double *>(rap_smem + (size_t)2 * WARPS * TBL * sizeof(int)) + warp * TBL;
     const unsigned FULL = 0xffffffffu;
-    for (int I = blockIdx.x * kRapWarps + warp; I < nrows; I += gridDim.x * kRapWarps) {
-        if (FILL && overflow[I]) continue;
-        for (int t = lane; t < kRapTable; t += 32) keys[t] = -1;
+    for (int I = blockIdx.x * WARPS + warp; I < nrows; I += gridDim.x * WARPS) {
+        // the small tier counts every row; every other pass takes the rows of its own tier
+        if ((FILL || kTier == 1) && overflow[I] != kTier) continue;
+        for (int t = lane; t < TBL; t += 32) keys[t] = -1;
         __syncwarp();
         int next = 1;
         if (lane == 0) {
-            const int h = rap_insert(keys, I);  // diagonal first, starting from zero
+            const int h = rap_insert<TBL>(keys, I);  // diagonal first, starting from zero
             slots[h] = 0;
             if (FILL) vals[h] = 0.0;
         }
@@ -651,15 +659,15 @@ __global__ void __launch_bounds__(32 * kRapWarps)
                     const int leader = __ffs(grp) - 1;
                     const bool is_leader = valid && lane == leader;
                     int h = -1;
-                    if (is_leader) h = rap_find(keys, J);
+                    if (is_leader) h = rap_find<TBL>(keys, J);
                     const bool fresh = is_leader && h < 0;
                     const unsigned fresh_mask = __ballot_sync(FULL, fresh);
-                    if (next + __popc(fresh_mask) > kRapWarpMaxCols) {
+                    if (next + __popc(fresh_mask) > kMaxCols) {
                         over = true;  // warp-uniform
                         break;
                     }
                     if (fresh) {
-                        h = rap_insert(keys, J);
+                        h = rap_insert<TBL>(keys, J);
                         slots[h] = next + __popc(fresh_mask & ((1u << lane) - 1u));
                     }
                     next += __popc(fresh_mask);
@@ -691,7 +699,7 @@ __global__ void __launch_bounds__(32 * kRapWarps)
             }
         }
         if (over) {
-            if (!FILL && lane == 0) overflow[I] = 1;
+            if (!FILL && lane == 0) overflow[I] = kTier + 1;  // to the next tier
             __syncwarp();
             continue;
         }
@@ -699,7 +707,7 @@ __global__ void __launch_bounds__(32 * kRapWarps)
             if (lane == 0) cnt[I] = next;
         } else {
             const int base = cia[I];
-            for (int t = lane; t < kRapTable; t += 32) {
+            for (int t = lane; t < TBL; t += 32) {
                 const int key = keys[t];
                 if (key >= 0) {
                     cja[base + slots[t]] = key;
@@ -763,24 +771,32 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
              long long table_budget_entries) {
     (void)table_budget_entries;
     const int nc = P.ncols;
-    const size_t smem = (size_t)kRapWarps * kRapTable * (2 * sizeof(int) + sizeof(double));
+    const size_t smemS = (size_t)kRapWarpsS * kRapTableS * (2 * sizeof(int) + sizeof(double));
+    const size_t smemL = (size_t)kRapWarpsL * kRapTableL * (2 * sizeof(int) + sizeof(double));
     static bool attr[64] = {};
     int dev = 0;
     JX_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64 || !attr[dev]) {
-        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<false, kRapTableL, kRapWarpsL>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemL));
+        JX_CUDA(cudaFuncSetAttribute(rap_warp_kernel<true, kRapTableL, kRapWarpsL>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemL));
         if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     DevBuf<int> cnt(nc + 1);
     DevBuf<unsigned char> over(nc + 1);
     cnt.zero(s);
     over.zero(s);
-    const int grid = std::max(1, std::min(div_up(nc, kRapWarps), 64 * sm_count()));
+    const int gridS = std::max(1, std::min(div_up(nc, kRapWarpsS), 64 * sm_count()));
+    const int gridL = std::max(1, std::min(div_up(nc, kRapWarpsL), 64 * sm_count()));
     if (nc > 0) {
-        rap_warp_kernel<false><<<grid, 32 * kRapWarps, smem, s>>>(nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja,
-                                                                 A.a, P.ia.get(), P.ja.get(), P.a.get(), cnt.get(),
-                                                                 over.get(), nullptr, nullptr, nullptr);
+        rap_warp_kernel<false, kRapTableS, kRapWarpsS><<<gridS, 32 * kRapWarpsS, smemS, s>>>(
+            nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(), cnt.get(),
+            over.get(), nullptr, nullptr, nullptr);
+        JX_LAUNCH_CHECK();
+        rap_warp_kernel<false, kRapTableL, kRapWarpsL><<<gridL, 32 * kRapWarpsL, smemL, s>>>(
+            nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(), cnt.get(),
+            over.get(), nullptr, nullptr, nullptr);
         JX_LAUNCH_CHECK();
     }
     // rows that overflowed the shared table: thread-per-row with a global table
@@ -789,7 +805,7 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
     JX_CUDA(cudaStreamSynchronize(s));
     std::vector<int> list;
     for (int I = 0; I < nc; ++I)
-        if (h_over[I]) list.push_back(I);
+        if (h_over[I] == 2) list.push_back(I);
     const int nl = (int)list.size();
     DevBuf<int> d_list(nl > 0 ? nl : 1);
     DevBuf<long long> toff(nl + 1);
@@ -821,9 +837,13 @@ void amg_rap(const CsrView<double> &A, const DeviceCsr &P, const DeviceCsr &R, D
     Ac.ja.alloc(nnz > 0 ? nnz : 1);
     Ac.a.alloc(nnz > 0 ? nnz : 1);
     if (nc > 0) {
-        rap_warp_kernel<true><<<grid, 32 * kRapWarps, smem, s>>>(nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja,
-                                                                A.a, P.ia.get(), P.ja.get(), P.a.get(), nullptr,
-                                                                over.get(), Ac.ia.get(), Ac.ja.get(), Ac.a.get());
+        rap_warp_kernel<true, kRapTableS, kRapWarpsS><<<gridS, 32 * kRapWarpsS, smemS, s>>>(
+            nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(), nullptr,
+            over.get(), Ac.ia.get(), Ac.ja.get(), Ac.a.get());
+        JX_LAUNCH_CHECK();
+        rap_warp_kernel<true, kRapTableL, kRapWarpsL><<<gridL, 32 * kRapWarpsL, smemL, s>>>(
+            nc, R.ia.get(), R.ja.get(), R.a.get(), A.ia, A.ja, A.a, P.ia.get(), P.ja.get(), P.a.get(), nullptr,
+            over.get(), Ac.ia.get(), Ac.ja.get(), Ac.a.get());
         JX_LAUNCH_CHECK();
     }
     if (nl > 0) {
