@@ -59,6 +59,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "CPR-GMRES time to 1e-6 FP64 rel-res, mixed+learned vs plain FP64, 1xB200"
 UNIT = "s"
+# the reference arm's timed complete runs stop after this many seconds (at least one run)
+REF_BUDGET_S = 120.0
 # GMRES iterations the reference library needs (tol 1e-6), measured by running
 # it to convergence: config 1 with ABF decoupling and GMRES(30), one thread (the
 # device path in exact-order mode reproduces the same count); config 4 with
@@ -284,7 +286,9 @@ def run_reference(args):
     into oracle/_ref; the oracle restatement where it is absent) on all host threads.  Each timed step is
     one complete run to convergence; value = the GMRES solve phase (setup excluded, as in our arm's
     value), e2e = decoupling + CPR setup + solve (as our arm's e2e, which also includes the uploads).
-    Warm-up steps are short runs (two GMRES iterations) that page the library and the system in."""
+    Warm-up steps are short runs (two GMRES iterations) that page the library and the system in.  A
+    complete run takes about 35 s on C1 and 250 s on C4, so the timed runs stop once REF_BUDGET_S
+    has passed (at least one): the line's `steps` is the number of runs made."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
@@ -306,18 +310,21 @@ def run_reference(args):
         t, it, kind = reference_full_solve(s, threads, args.config)
         phases.append(t)
         iters.append(it)
+        if time.perf_counter() - w0 > REF_BUDGET_S:
+            break
     wall = time.perf_counter() - w0
     ph = np.array(phases)
     value = float(ph[:, 2].mean())
     total = float(ph.sum(axis=1).mean())
     what = ("reference JXFPAMG built from source (FP64)" if kind == "reference"
             else "oracle C restatement (FP64, the reference library was not built)")
-    desc = (f"{what}, {threads} OpenMP threads, {args.steps} complete runs to FP64 rel-res 1e-6 "
+    desc = (f"{what}, {threads} OpenMP threads, {len(phases)} complete runs to FP64 rel-res 1e-6 "
             f"({iters[0]} GMRES iterations; decoupling {ph[:, 0].mean():.2f} s, CPR setup {ph[:, 1].mean():.2f} s, "
             f"solve {value:.2f} s per run; {wall:.0f} s in all)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3, "higher_is_better": False,
+        "steps": len(phases), "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3,
+        "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": common_config(args.config, plain_opts(args)),
         "parallelism": f"1 host process, {threads} OpenMP threads",
