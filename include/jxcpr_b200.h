@@ -102,6 +102,24 @@ JXCPR_API int jxcpr_dot_dev(long long n, const double *x, const double *y, doubl
 JXCPR_API int jxcpr_dot_dev_noalloc(long long n, const double *x, const double *y, double *out_host,
                                     void *stream);
 
+/* ---- BSR files into device memory -------------------------------------------
+ * Reads a BSR matrix file in the text (binary = 0) or binary (1) format of jxf_BSRMatrixRead /
+ * jxf_BSRMatrixRead_Binary (jxfpamg-0220/csrc/mat_vec_data/seq_bsr_matrix.c:1735-2120) straight into
+ * device arrays: the file is read in 64 MB chunks into pinned host memory and each chunk is copied
+ * to the device while the next is read; a text file is tokenised and its numbers converted on the
+ * device (values to the nearest FP64, as the host reader's fscanf gives: bit-identical arrays).
+ * As the host readers: 1-based indices become 0-based, the largest column must be cols - 1, and
+ * column-major blocks (storage 1) become row-major.  *ia (rows + 1), *ja (nnzb) and *a (nnzb*bs*bs)
+ * are device allocations the caller releases with jxcpr_bsr_free_device.  Returns 4 (message in
+ * jxcpr_last_error) for a file that cannot be opened or is malformed, 512 for a CUDA failure. */
+JXCPR_API int jxcpr_bsr_read_device(const char *file, int binary, int *rows, int *cols, int *bs, long long *nnzb,
+                                    int **ia, int **ja, double **a, void *stream);
+JXCPR_API int jxcpr_bsr_free_device(int *ia, int *ja, double *a);
+/* The device reader's conversion of one number token (no white space) on the host: 0 converted
+ * (*out = the nearest FP64), 1 a form it leaves to strtod (more than 19 significant digits, inf,
+ * nan), 2 not a number. */
+JXCPR_API int jxcpr_parse_double_host(const char *token, int len, double *out);
+
 /* ---- dense inverse (coarsest AMG level) ------------------------------------
  * ainv = a^-1 for a dense n x n row-major FP64 matrix (n <= 8192; device pointers, may not alias) by
  * blocked Gauss-Jordan elimination without pivoting, as the reference eliminates its coarsest level
