@@ -292,6 +292,37 @@ __device__ __forceinline__ void load_block<2, float, float>(const float *__restr
     out[3] = v.w;
 }
 
+// The same with the cache-streaming hint (ld.global.cs): the chunk-ordered stage-2 sweep streams its
+// matrix once per sweep, and marking those lines evict-first keeps the gathered vectors (x, the
+// start values) in L1 / L2 (measured 56 -> 47 us per sweep on C1; the CSR level passes, whose lanes
+// share sectors across trips, measured slower with it and keep the default loads).
+__device__ __forceinline__ double ldv_cs(const double *p, long long k) { return __ldcs(p + k); }
+__device__ __forceinline__ float ldv_cs(const float *p, long long k) { return __ldcs(p + k); }
+template <int BS, typename TV, typename TA>
+__device__ __forceinline__ void load_block_cs(const TV *__restrict__ a, long long k, TA out[BS * BS]) {
+#pragma unroll
+    for (int q = 0; q < BS * BS; ++q) out[q] = (TA)ldv_cs(a, k * BS * BS + q);
+}
+template <>
+__device__ __forceinline__ void load_block_cs<2, double, double>(const double *__restrict__ a, long long k,
+                                                                 double out[4]) {
+    const double2 *p = reinterpret_cast<const double2 *>(a + k * 4);
+    const double2 v0 = __ldcs(p), v1 = __ldcs(p + 1);
+    out[0] = v0.x;
+    out[1] = v0.y;
+    out[2] = v1.x;
+    out[3] = v1.y;
+}
+template <>
+__device__ __forceinline__ void load_block_cs<2, float, float>(const float *__restrict__ a, long long k,
+                                                               float out[4]) {
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(a + k * 4));
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+    out[3] = v.w;
+}
+
 template <int BS, typename TA>
 __device__ __forceinline__ void block_solve(const TA D[BS * BS], const TA rhs[BS], TA out[BS]) {
     if (BS == 2) {
@@ -538,7 +569,7 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
         }
 #pragma unroll
         for (int q = 0; q < BS * BS; ++q) K[q] = 0;
-        load_block<BS, TV, TA>(a, o, D);
+        load_block_cs<BS, TV, TA>(a, o, D);
         // one off-diagonal entry: its contribution c (A_ij c added to acc) and the in-chunk bookkeeping
         // one off-diagonal entry: its contribution c (A_ij c added to acc) and the in-chunk bookkeeping
         auto entry = [&](unsigned cw, const TA B[BS * BS]) {
@@ -610,8 +641,8 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
             TA B[4][BS * BS];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                cw[e] = __ldg(col + p0 + 32 * e);
-                load_block<BS, TV, TA>(a, p0 + 32 * e, B[e]);
+                cw[e] = __ldcs(col + p0 + 32 * e);
+                load_block_cs<BS, TV, TA>(a, p0 + 32 * e, B[e]);
             }
 #pragma unroll
             for (int e = 0; e < 4; ++e) entry(cw[e], B[e]);
@@ -619,8 +650,8 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
         for (; k < wd; ++k) {
             const long long p0 = o + (long long)k * 32;
             TA B0[BS * BS];
-            load_block<BS, TV, TA>(a, p0, B0);
-            entry(__ldg(col + p0), B0);
+            load_block_cs<BS, TV, TA>(a, p0, B0);
+            entry(__ldcs(col + p0), B0);
         }
         block_inverse<BS, TA>(D, Di);
         TA r2[BS];
