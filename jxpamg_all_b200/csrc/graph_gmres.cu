@@ -360,6 +360,23 @@ __global__ void __launch_bounds__(kRedThreads) reduce_h_kernel(const double *__r
     st->skip = skip;
 }
 
+// h1[k] = sum of partials row k (k <= i), one block per row: the rows are summed side by side
+// (without the selective second pass, which reduce_h_kernel decides on from all of them).
+__global__ void __launch_bounds__(kThreads) reduce_rows_kernel(const double *__restrict__ partials, int G,
+                                                              GgState *st, GgWork W) {
+    __shared__ double sh[32];
+    grid_dep_wait();
+    const int m = st->i + 1, k = blockIdx.x;
+    if (k > m) return;
+    double v = 0.0;
+    for (int j = threadIdx.x; j < G; j += kThreads) v += partials[(long long)k * G + j];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        if (k < m) W.h1[k] = v;
+        if (k == 0) st->skip = 0;
+    }
+}
+
 // The first update and the second Gram products in one pass over the basis:
 // w -= sum_{k <= i} h[k] V[k], then partial <V[k], w> (k <= i) and <w, w> of
 // the updated w over the block's slice of kSlice2 elements (one quad per thread).
@@ -837,7 +854,10 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         else
             launch_dep(dots_kernel<double>, dim3(G), dim3(kThreads), s2, nn, V, st, w, pt);
         JX_LAUNCH_CHECK();
-        launch_dep(reduce_h_kernel, dim3(1), dim3(kRedThreads), s2, pt, G, st, P, W);
+        if (P.selective)
+            launch_dep(reduce_h_kernel, dim3(1), dim3(kRedThreads), s2, pt, G, st, P, W);
+        else
+            launch_dep(reduce_rows_kernel, dim3(kGgMaxK + 1), dim3(kThreads), s2, pt, G, st, W);
         JX_LAUNCH_CHECK();
         if (f32)
             launch_dep(update_dots_kernel<float>, dim3(G2), dim3(kThreads), s2, nn, V32, st, W.h1, w, pt);
@@ -920,7 +940,10 @@ void GraphGmres::orth_native(int m, int reps, const double *w, cudaStream_t s) {
         else
             dots_kernel<double><<<G, kThreads, 0, s>>>(nn, vptr.get(), st, ww, pt);
         JX_LAUNCH_CHECK();
-        reduce_h_kernel<<<1, kRedThreads, 0, s>>>(pt, G, st, P, W);
+        if (P.selective)
+            reduce_h_kernel<<<1, kRedThreads, 0, s>>>(pt, G, st, P, W);
+        else
+            reduce_rows_kernel<<<kGgMaxK + 1, kThreads, 0, s>>>(pt, G, st, W);
         JX_LAUNCH_CHECK();
         if (fp32)
             update_dots_kernel<float><<<G2, kThreads, 0, s>>>(nn, vptr32.get(), st, W.h1, ww, pt);
