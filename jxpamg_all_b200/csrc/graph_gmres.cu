@@ -463,28 +463,33 @@ __global__ void __launch_bounds__(kThreads) update_dots_kernel(long long n, cons
     }
 }
 
+// The second-pass coefficients h2[k] (k <= i) and ||w||^2 (into st->sig) from the fused update's
+// partials, one block per row; nothing when the selective rule kept the first pass (reduce_h_kernel
+// set them then).
+__global__ void __launch_bounds__(kThreads) reduce_rows2_kernel(const double *__restrict__ partials, int G,
+                                                               GgState *st, GgWork W) {
+    __shared__ double sh[32];
+    grid_dep_wait();
+    if (st->skip) return;
+    const int m = st->i + 1, k = blockIdx.x;
+    if (k > m) return;
+    double v = 0.0;
+    for (int j = threadIdx.x; j < G; j += kThreads) v += partials[(long long)k * G + j];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        if (k < m) W.h2[k] = v;
+        else st->sig = v;
+    }
+}
+
 // One thread: the Hessenberg column of this step, its Givens rotation, the
 // residual estimate, the cycle-end rules and, at a cycle end, y = H^-1 rs.
-__global__ void __launch_bounds__(kRedThreads) arnoldi_kernel(const double *__restrict__ partials, int G, GgState *st,
-                                                              GgParams P, GgWork W, double *__restrict__ norms,
-                                                              cudaGraphConditionalHandle h_in) {
-    __shared__ double sig;
+__global__ void arnoldi_kernel(GgState *st, GgParams P, GgWork W, double *__restrict__ norms,
+                               cudaGraphConditionalHandle h_in) {
     grid_dep_wait();
-    const int i0 = st->i, m = i0 + 1, lane = threadIdx.x & 31;
-    if (st->skip) {  // no second pass: h2 and ||w||^2 come from the first (reduce_h_kernel)
-        if (threadIdx.x == 0) sig = st->sig;
-    } else {
-        // second-pass coefficients h2[k], k < m, and ||w||^2 (row m)
-        for (int k = threadIdx.x >> 5; k <= m; k += kRedThreads / 32) {
-            const double v = warp_row_sum(partials + (long long)k * G, G, lane);
-            if (lane == 0) {
-                if (k < m) W.h2[k] = v;
-                else sig = v;
-            }
-        }
-    }
-    __syncthreads();
     if (threadIdx.x != 0) return;
+    const int i0 = st->i, m = i0 + 1;
+    const double sig = st->sig;  // ||w||^2 after the step's last Gram-Schmidt pass
     GgState &s = *st;
     const int K = P.k;
     double *hh = W.hh, *rs = W.rs, *c = W.c, *sn = W.sn;
@@ -864,7 +869,9 @@ void GraphGmres::record(Solver &S, cudaStream_t s, double *out) {
         else
             launch_dep(update_dots_kernel<double>, dim3(G2), dim3(kThreads), s2, nn, V, st, W.h1, w, pt);
         JX_LAUNCH_CHECK();
-        launch_dep(arnoldi_kernel, dim3(1), dim3(kRedThreads), s2, pt, G2, st, P, W, norms.get(), h_in);
+        launch_dep(reduce_rows2_kernel, dim3(kGgMaxK + 1), dim3(kThreads), s2, pt, G2, st, W);
+        JX_LAUNCH_CHECK();
+        launch_dep(arnoldi_kernel, dim3(1), dim3(32), s2, st, P, W, norms.get(), h_in);
         JX_LAUNCH_CHECK();
         if (f32)
             launch_dep(final_kernel<float>, dim3(Gq), dim3(kThreads), s2, nn, V32, st, W.h2, w);
