@@ -26,6 +26,9 @@
 // instead of MGS (i + 1 passes).  The norm of the new vector comes from Pythagoras,
 // ||w - V h2||^2 = ||w||^2 - ||h2||^2, as in delayed CGS2 (Swirydowicz et al.,
 // 2020).  Flexible: the preconditioned directions z_i are kept and x += Z y.
+// Each pass writes per-block partial sums, which one block per row adds up
+// (reduce_rows_kernel, reduce_rows2_kernel) before the one-thread Arnoldi
+// kernel; the kernels of a step are launched as programmatic dependents.
 // Options: the basis and the z_i stored in FP32 (krylov_fp32; every product,
 // norm and update still in FP64), and the second pass taken only where the
 // first cancelled more than half of ||w||^2 (selective_reorth, the Daniel-
