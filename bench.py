@@ -64,7 +64,7 @@ REF_BUDGET_S = 120.0
 # GMRES iterations the reference library needs (tol 1e-6), measured by running
 # it to convergence: config 1 with ABF decoupling and GMRES(30), one thread (the
 # device path in exact-order mode reproduces the same count); config 4 with
-# True-IMPES decoupling and GMRES(60), 16 threads (253 s on the GPU box's host).
+# True-IMPES decoupling and GMRES(60), 16 threads (253 s on a 16-core host of a B200 machine).
 REF_ITERS = {"c1": 51, "c0": 23, "c4": 233}
 WORKLOADS = {
     "c1": "config-1 system: 60x220x85 channelised two-phase Jacobian, 1,122,000 cells, 2x2 BSR, 7,780,000 blocks, seed 1",

@@ -8,7 +8,7 @@ ctypes front end to
                           the reference tree was available at build time.
 
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this package, and only as the checker / baseline.
+``bench.py`` may import this package, and only as the test oracle / baseline.
 """
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_LIB = os.path.join(HERE, "liborc.so")
 REF_LIB = os.path.join(HERE, "_ref", "libjxf_ref64.so")
-# the reference source tree the checker library is compiled from (build step only)
+# the reference source tree the test oracle's library is compiled from (build step only)
 REF_TREE = os.environ.get("JXF_REFERENCE_TREE", "")
 
 _orc = None

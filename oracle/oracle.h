@@ -1,7 +1,7 @@
 /*
  * ORACLE (test infrastructure only): declarations of the plain-C restatement
  * of the reference CPR-GMRES path.  Used by tests/, the smoke check and the
- * CPU-baseline leg of bench.py as the checker; never linked by the product.
+ * CPU-baseline leg of bench.py as the test oracle; never linked by the product.
  */
 #ifndef JXCPR_ORACLE_H
 #define JXCPR_ORACLE_H

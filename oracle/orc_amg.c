@@ -7,7 +7,7 @@
  * hybrid symmetric Gauss-Seidel (two full SGS sweeps per pre/post step at
  * one rank and one thread) and Gaussian elimination on the coarsest level.
  *
- * Used only by tests/ and bench.py's CPU-baseline leg as the checker; the
+ * Used only by tests/ and bench.py's CPU-baseline leg as the test oracle; the
  * product library never links it.  Sequential C, -ffp-contract=off.
  */
 #include <math.h>

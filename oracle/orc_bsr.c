@@ -1,7 +1,7 @@
 /*
  * ORACLE (test infrastructure only): plain-C restatement of the reference's
  * BSR kernels on the CPR-GMRES path.  Only tests/, the package's smoke check
- * and bench.py's CPU-baseline leg call this code, and only as a checker or
+ * and bench.py's CPU-baseline leg call this code, and only as a test oracle or
  * baseline; the product library never links it.
  *
  * Each function cites the reference lines it restates (paths relative to the

@@ -1,5 +1,5 @@
 # Builds the reference JXFPAMG library from its own C sources into oracle/_ref/
-# as a CPU checker (FP64: no JXF_SINGLE, as the reference's headers select
+# as a CPU test oracle (FP64: no JXF_SINGLE, as the reference's headers select
 # double when it is undefined).  Object files and the shared library go only
 # under oracle/_ref/, which is git-ignored.  The reference's own build system
 # is not used; this recipe compiles its sources directly with a single-rank
