@@ -14,7 +14,8 @@ true residual b - A x in FP64 before it reports convergence).
   value : device-resident solve with the measured path (FP32 preconditioner,
           learned per-level strength thresholds and Chebyshev intervals, the
           stage-2 weights of the reference's mixed-precision driver, flexible
-          FP64 GMRES run on the device as one CUDA graph), seconds;
+          FP64 GMRES run on the device as one CUDA graph with its Krylov basis
+          stored in FP32), seconds;
           details.plain_fp64_s is the same measurement for the plain FP64 path
           (the reference's CPR weights, host-driven MGS GMRES) and
           details.speedup_vs_plain_fp64 their ratio; details.*same_driver* is
@@ -29,10 +30,14 @@ true residual b - A x in FP64 before it reports convergence).
 The matrix, AMG hierarchy and Krylov basis (~2 GB) exceed L2 (126 MB), so no
 explicit flush is needed between steps.
 
+On one GPU the default run also measures the three-phase system (--config c4)
+and the uneven batch (--config c3) in child processes and summarises their
+lines in details.other_workloads.
+
 --impl reference times the reference library (compiled from its own sources
 into oracle/_ref) on the host cores: every timed step is one complete run to
-FP64 rel-res 1e-6; value = its GMRES solve phase (setup excluded, as our
-value), e2e = decoupling + setup + solve.  Our arm's cpu_baseline is a
+FP64 rel-res 1e-6 (until REF_BUDGET_S has passed); value = its GMRES solve
+phase (setup excluded, as our value), e2e = decoupling + setup + solve.  Our arm's cpu_baseline is a
 bounded sample of the same library (decoupling + setup + GMRES runs of 2 and
 4 iterations, scaled to the reference's iteration count) so that the default
 run stays short.
