@@ -157,31 +157,56 @@ void coarse_solve(Amg &H, const double *f, double *u, cudaStream_t s) {
 // hierarchy
 // ---------------------------------------------------------------------------
 // Gauss-Seidel schedules of a level, built on the host from its pattern.  The
-// host work runs on a worker thread while the setup carries on with the next
-// levels (the pattern is copied here, on the setup's stream, first).
+// pattern's copy to the host and the host work run on a worker thread while the
+// setup carries on with the strength, coarsening and the next levels: the copy
+// waits for the pattern on a stream of its own (an event recorded on the
+// setup's stream), so the setup's stream is not stalled by it.
 struct ScheduleJob {
     std::vector<int> perm[2], gptr[2], rank[2];
     bool both = false;
     std::vector<int> chunk_order, chunk_seg;
 };
 
+namespace {
+// A stream and an event owned by the worker thread's copy, released on every exit path.
+struct CopyStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ready = nullptr;
+    ~CopyStream() {
+        if (stream) cudaStreamDestroy(stream);
+        if (ready) cudaEventDestroy(ready);
+    }
+};
+}  // namespace
+
 // chunk > 0: also the stage-2 chunk order of the pattern (level 0 of the fast path), on a host thread
 // of its own beside the Gauss-Seidel schedule
 static std::future<ScheduleJob> start_level_schedules(AmgLevel &L, int order, int chunk, cudaStream_t s) {
     const int n = L.A.nrows;
-    auto ia = std::make_shared<std::vector<int>>(n + 1), ja = std::make_shared<std::vector<int>>(L.A.nnz > 0 ? L.A.nnz : 1);
-    L.A.ia.download(ia->data(), n + 1, s);
-    L.A.ja.download(ja->data(), L.A.nnz, s);
-    JX_CUDA(cudaStreamSynchronize(s));
+    const long long nnz = L.A.nnz;
+    const int *dia = L.A.ia.get(), *dja = L.A.ja.get();
+    int dev = 0;
+    JX_CUDA(cudaGetDevice(&dev));
+    auto cs = std::make_shared<CopyStream>();
+    JX_CUDA(cudaEventCreateWithFlags(&cs->ready, cudaEventDisableTiming));
+    JX_CUDA(cudaEventRecord(cs->ready, s));
     using Chunks = std::pair<std::vector<int>, std::vector<int>>;
-    std::shared_future<Chunks> chunks;
-    if (chunk > 0)
-        chunks = std::async(std::launch::async, [n, chunk, ia, ja]() {
-                     Chunks c;
-                     build_chunk_order_host(n, ia->data(), ja->data(), chunk, c.first, c.second);
-                     return c;
-                 }).share();
-    return std::async(std::launch::async, [n, order, ia, ja, chunks]() {
+    return std::async(std::launch::async, [n, nnz, dia, dja, dev, cs, order, chunk]() {
+        JX_CUDA(cudaSetDevice(dev));
+        JX_CUDA(cudaStreamCreateWithFlags(&cs->stream, cudaStreamNonBlocking));
+        JX_CUDA(cudaStreamWaitEvent(cs->stream, cs->ready, 0));
+        auto ia = std::make_shared<std::vector<int>>(n + 1), ja = std::make_shared<std::vector<int>>(nnz > 0 ? nnz : 1);
+        JX_CUDA(cudaMemcpyAsync(ia->data(), dia, sizeof(int) * (size_t)(n + 1), cudaMemcpyDeviceToHost, cs->stream));
+        if (nnz > 0)
+            JX_CUDA(cudaMemcpyAsync(ja->data(), dja, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, cs->stream));
+        JX_CUDA(cudaStreamSynchronize(cs->stream));
+        std::future<Chunks> chunks;
+        if (chunk > 0)
+            chunks = std::async(std::launch::async, [n, chunk, ia, ja]() {
+                Chunks c;
+                build_chunk_order_host(n, ia->data(), ja->data(), chunk, c.first, c.second);
+                return c;
+            });
         ScheduleJob J;
         build_schedule_host(n, ia->data(), ja->data(), order, true, J.perm[0], J.gptr[0], J.rank[0]);
         if (order == ORDER_EXACT) {

@@ -930,6 +930,11 @@ struct FastCpr final : FastCprBase {
     void launch_stage2(const LevelMat &M, const TV *a, int r0, int r1, const TXV *r, TXV *z, TXV *vtp, TAC w,
                        TAC om, int plain, fk::SweepOrder so, cudaStream_t s) {
         if (M.chunk) {
+            // the 2x2 sweep gathers x and the start values as pairs (one 8-byte load in FP32)
+            if (bs == 2 && ((reinterpret_cast<uintptr_t>(z) | reinterpret_cast<uintptr_t>(vtp)) % 8) != 0) {
+                set_error("stage 2: the iterate and start-value vectors must be 8-byte aligned");
+                throw CudaError{cudaErrorInvalidValue, "stage 2 alignment"};
+            }
             const int grid = div_up(r1 - r0, kThreads);
 #define JX_HGS_CHUNK(BSV, CHV)                                                                              \
     launch_dep(fk::hgs_chunk<BSV, CHV, TV, TAC, TXV>, dim3(grid), dim3(kThreads), s, r0, r1, M.sp.get(),     \

@@ -526,19 +526,40 @@ __device__ __forceinline__ void block_matvec(const TA M[BS * BS], const TA v[BS]
     }
 }
 
+// The two values of a 2-vector entry j of x (FP32: one 8-byte load; x's base is 8-byte aligned, which
+// the stage-2 launcher checks).  NC: through the read-only path, valid where no thread of the launch
+// writes the entry before it is read.
+template <typename TXV, typename TA, bool NC>
+__device__ __forceinline__ void ld_pair(const TXV *p, int j, TA out[2]) {
+    if constexpr (sizeof(TXV) == 4) {
+        const float2 v = NC ? __ldg(reinterpret_cast<const float2 *>(p) + j) : reinterpret_cast<const float2 *>(p)[j];
+        out[0] = (TA)v.x;
+        out[1] = (TA)v.y;
+    } else {
+        out[0] = (TA)(NC ? __ldg(p + 2LL * j) : p[2LL * j]);
+        out[1] = (TA)(NC ? __ldg(p + 2LL * j + 1) : p[2LL * j + 1]);
+    }
+}
+
 // Column words of the chunk-ordered stage-2 matrix: the column in the low 30 bits, bit 30 set when the
 // neighbour's colour comes earlier in the sweep (its start value is in vt), bit 31 when it lies in the
 // row's own chunk.  The sweep order is fixed at setup, so the relation is stored, not looked up.
 constexpr unsigned kChunkColMask = 0x3fffffffu, kChunkEarlier = 1u << 30, kChunkSame = 1u << 31;
 
-// FP32 arithmetic: at least 5 blocks of 256 threads per SM (<= 51 registers), so that enough rows'
-// loads are in flight; FP64: 3 (<= 85 registers)
+// FP32 arithmetic: 5 blocks of 256 threads per SM for 2x2 blocks (<= 51 registers), so that enough rows'
+// loads are in flight, 4 for 3x3 (<= 64 registers: the row state of 3x3 blocks spills below that);
+// FP64: 3 (<= 85 registers).  To keep the state small, the diagonal block, b and the row's own x are
+// loaded after the entry loop, and for 2x2 blocks the kept in-chunk block is re-read by its slot
+// rather than held (measured on C1: 46.9 -> 41.1 us per sweep with the paired x gathers; C4: 103 ->
+// 79 us).
 template <int BS, int CH, typename TV, typename TA, typename TXV>
-__global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0, int r1, const long long *__restrict__ sp,
+__global__ void __launch_bounds__(256, sizeof(TA) == 4 ? (BS == 2 ? 5 : 4) : 3) hgs_chunk(int r0, int r1, const long long *__restrict__ sp,
                                                  const unsigned *__restrict__ col, const TV *__restrict__ a,
                                                  const int *__restrict__ rows, const TXV *__restrict__ b,
                                                  TXV *x, TXV *vt, TA w, TA omega, int plain, int save) {
     static_assert(32 % CH == 0, "chunks tile the 32-row slices");
+    constexpr bool kKeepSlot = BS == 2;  // hold the kept in-chunk block's slot, not its values
+    constexpr int NB = BS == 2 ? 4 : 2;  // entries loaded per batch
     grid_dep_wait();
     const int t = r0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -560,19 +581,15 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
         const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
         wd = (int)((b1 - b0) >> 5);
         o = b0 + (t & 31);
-        TA rhs[BS], acc[BS], D[BS * BS], K[BS * BS];
+        TA acc[BS], K[kKeepSlot ? 1 : BS * BS];
+        int kslot = 0;  // slot of the kept in-chunk block (kKeepSlot)
 #pragma unroll
-        for (int q = 0; q < BS; ++q) {
-            rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
-            xv[q] = (TA)x[(long long)i * BS + q];
-            acc[q] = 0;
-        }
+        for (int q = 0; q < BS; ++q) acc[q] = 0;
 #pragma unroll
-        for (int q = 0; q < BS * BS; ++q) K[q] = 0;
-        load_block_cs<BS, TV, TA>(a, o, D);
-        // one off-diagonal entry: its contribution c (A_ij c added to acc) and the in-chunk bookkeeping
-        // one off-diagonal entry: its contribution c (A_ij c added to acc) and the in-chunk bookkeeping
-        auto entry = [&](unsigned cw, const TA B[BS * BS]) {
+        for (int q = 0; q < (kKeepSlot ? 1 : BS * BS); ++q) K[q] = 0;
+        // one off-diagonal entry in slot kk: its contribution c (A_ij c added to acc) and the in-chunk
+        // bookkeeping
+        auto entry = [&](unsigned cw, const TA B[BS * BS], int kk) {
             TA c[BS];
             if constexpr (BS == 2) {
                 // 2x2 blocks: the three cases (later in the chunk, earlier in the chunk, outside it) as
@@ -586,17 +603,20 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
                     lowmask |= 1u << dq;
                     if (kq < 0) {
                         kq = dq;
-#pragma unroll
-                        for (int q = 0; q < BS * BS; ++q) K[q] = B[q];
+                        kslot = kk;
                     }
                 }
+                // x is read-only within the launch where it is gathered: the chunks of one colour are
+                // not coupled, and the row's own chunk writes only after every lane's phase 1
+                TA xp[2], vp[2];
+                ld_pair<TXV, TA, true>(x, j, xp);
+                vp[0] = xp[0];
+                vp[1] = xp[1];
+                if (earlier_col) ld_pair<TXV, TA, true>(vt, j, vp);
 #pragma unroll
                 for (int m = 0; m < BS; ++m) {
-                    const long long oj = (long long)j * BS + m;
-                    const TA xj = (TA)x[oj];
-                    const TA vj = earlier_col ? (TA)__ldg(vt + oj) : xj;
-                    const TA base = same_earlier ? (TA)0 : xj;  // earlier in the chunk: -(1 - omega) A vt_j now
-                    const TA sub = same_earlier ? xj : vj;
+                    const TA base = same_earlier ? (TA)0 : xp[m];  // earlier in the chunk: -(1 - omega) A vt_j now
+                    const TA sub = same_earlier ? xp[m] : vp[m];
                     c[m] = plain ? base : base - omo * sub;
                 }
             } else {
@@ -613,8 +633,10 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
                         lowmask |= 1u << dq;
                         if (kq < 0) {
                             kq = dq;
+                            if constexpr (!kKeepSlot) {
 #pragma unroll
-                            for (int q = 0; q < BS * BS; ++q) K[q] = B[q];
+                                for (int q = 0; q < BS * BS; ++q) K[q] = B[q];
+                            }
                         }
 #pragma unroll
                         for (int m = 0; m < BS; ++m) c[m] = plain ? (TA)0 : -omo * (TA)x[(long long)j * BS + m];
@@ -635,37 +657,51 @@ __global__ void __launch_bounds__(256, sizeof(TA) == 4 ? 5 : 3) hgs_chunk(int r0
                 for (int m = 0; m < BS; ++m) acc[q] += B[q * BS + m] * c[m];
         };
         int k = 1;
-        for (; k + 3 < wd; k += 4) {
+        for (; k + NB - 1 < wd; k += NB) {
             const long long p0 = o + (long long)k * 32;
-            unsigned cw[4];
-            TA B[4][BS * BS];
+            unsigned cw[NB];
+            TA B[NB][BS * BS];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+            for (int e = 0; e < NB; ++e) {
                 cw[e] = __ldcs(col + p0 + 32 * e);
                 load_block_cs<BS, TV, TA>(a, p0 + 32 * e, B[e]);
             }
 #pragma unroll
-            for (int e = 0; e < 4; ++e) entry(cw[e], B[e]);
+            for (int e = 0; e < NB; ++e) entry(cw[e], B[e], k + e);
         }
         for (; k < wd; ++k) {
             const long long p0 = o + (long long)k * 32;
             TA B0[BS * BS];
             load_block_cs<BS, TV, TA>(a, p0, B0);
-            entry(__ldcs(col + p0), B0);
+            entry(__ldcs(col + p0), B0, k);
         }
+        TA rhs[BS], D[BS * BS];
+#pragma unroll
+        for (int q = 0; q < BS; ++q) {
+            rhs[q] = (TA)__ldg(b + (long long)i * BS + q);
+            xv[q] = (TA)x[(long long)i * BS + q];
+        }
+        load_block_cs<BS, TV, TA>(a, o, D);
         block_inverse<BS, TA>(D, Di);
         TA r2[BS];
 #pragma unroll
         for (int q = 0; q < BS; ++q) r2[q] = (plain ? (TA)1 : omega) * rhs[q] - acc[q];
         block_matvec<BS, TA>(Di, r2, u);
         if (kq >= 0) {
+            TA Kb[BS * BS];
+            if constexpr (kKeepSlot) {
+                load_block<BS, TV, TA>(a, o + (long long)kslot * 32, Kb);
+            } else {
+#pragma unroll
+                for (int q = 0; q < BS * BS; ++q) Kb[q] = K[q];
+            }
 #pragma unroll
             for (int q = 0; q < BS; ++q)
 #pragma unroll
                 for (int m = 0; m < BS; ++m) {
                     TA g = 0;
 #pragma unroll
-                    for (int l = 0; l < BS; ++l) g += Di[q * BS + l] * K[l * BS + m];
+                    for (int l = 0; l < BS; ++l) g += Di[q * BS + l] * Kb[l * BS + m];
                     G[q * BS + m] = g;
                 }
         }
