@@ -103,7 +103,7 @@ BATCH_OPTS = dict(PLAIN_OPTS, precision=1, fast_smoother=1, flexible=1, stage2_r
 
 # the kernel the `roofline` object reports for each workload: the one with the largest share of the
 # measured solve in its launch list (profiles/launches_*): "cheb_level1" or "stage2"
-DOMINANT = {"c1": "stage2", "c4": "stage2"}
+DOMINANT = {"c1": "cheb_level1", "c4": "stage2"}
 
 # per-workload method choices: the three-phase system is decoupled by True-IMPES and solved with
 # GMRES(60) (with ABF, or with GMRES(30), the reference itself is still short of 1e-6 after 300
