@@ -646,7 +646,7 @@ def other_workloads(args):
 TRAFFIC_BYTES = {
     ("c1", "stage2/4/chunk4"): 209_080_576,    # hgs_chunk<2,4,float>: 99,779,584 + 109,300,992 (2 colours)
     ("c1", "cheb/A1/4/csr/4"): 103_513_600,    # row_kernel<CsrFmt<4,float>, OpCheb>: mean of 2 launches
-    ("c1", "cheb/A1/4/sell"): 108_209_792,     # row_kernel<SellFmt<float>, OpCheb>: mean of 2 launches
+    ("c1", "cheb/A1/4/sell"): 108_742_144,     # row_kernel<SellFmt<float>, OpCheb>: mean of 2 launches
     ("c1", "bsr_spmv/8"): 318_746_624,         # bsr_spmv_direct_kernel<2, double>
 }
 

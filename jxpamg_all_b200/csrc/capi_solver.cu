@@ -453,6 +453,7 @@ int jxcpr_solver_level_stored_values(jxcpr_solver *h, int level, double *values)
         }
         const long long nnz = S.cpr.amg.levels[level]->A.nnz;
         DevBuf<double> out(nnz > 0 ? nnz : 1);
+        JX_CUDA(cudaMemsetAsync(out.get(), 0, sizeof(double) * (nnz > 0 ? nnz : 1), S.stream));
         if (!S.cpr.fast->stored_values(level, out.get(), S.stream)) {
             set_error("level_stored_values: level %d has no smoothed operator", level);
             return JXCPR_ERROR_ARG;

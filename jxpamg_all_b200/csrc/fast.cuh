@@ -79,7 +79,7 @@ struct FastLevel {
     int smoother = FS_L1_JACOBI;  // in use
     int smoother_cfg = FS_L1_JACOBI, smoother_plain = FS_L1_JACOBI;  // configured / plain settings
     LevelMat A;          // colour classes as segments (FS_COLOR_GS) or one segment
-    const int *src_ia = nullptr;  // row pointer of the hierarchy's CSR operator (not owned)
+    const int *src_ia = nullptr, *src_ja = nullptr;  // the hierarchy's CSR operator's pattern (not owned)
     int last_color = -1;
     LevelMat P, R;       // interpolation from level+1 / restriction to it
     DevBuf<TX> dinv;     // 1/a_ii (GS, Chebyshev); 0 skips the row

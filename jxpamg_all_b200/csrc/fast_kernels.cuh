@@ -811,11 +811,13 @@ __device__ __forceinline__ double warp_max(double v) {
 // Stored row t receives the entries of CSR/BSR row rows[t] (E values per entry, E = 1 or bs*bs) in
 // slot-major order.  A warp covers one 32-row slice, so each slot of the slice is one block of 32
 // stored values; bscale != nullptr (BF16, E = 1): that block's power-of-two scale goes to
-// bscale[p / 32] and the values are stored divided by it.
+// bscale[p / 32] and the values are stored divided by it.  sorted (E = 1, no bscale): each row's
+// entries after the first go to the slots in ascending column order (the first, the diagonal of a
+// square operator, stays first), so that the rows of a slice gather nearby columns in each slot.
 template <typename TV>
 __global__ void sell_fill(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
                           const int *__restrict__ ia, const int *__restrict__ ja, const double *__restrict__ a,
-                          int E, int *__restrict__ col, TV *__restrict__ val, float *__restrict__ bscale) {
+                          int E, int *__restrict__ col, TV *__restrict__ val, float *__restrict__ bscale, int sorted) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ((nstored + 31) & ~31)) return;  // whole slices: every lane of a slice's warp stays
     const bool in = t < nstored;
@@ -833,13 +835,46 @@ __global__ void sell_fill(int nstored, const int *__restrict__ rows, const long 
             if ((t & 31) == 0) bscale[p >> 5] = (float)sc;
         }
         if (!in) continue;
-        if (k < len) {
+        if (k < len && sorted) {
+            // entry k goes to slot 1 + (entries 1.. before it in column order, ties by position)
+            const int jk = ja[d + k];
+            int pos = 0;
+            if (k > 0) {
+                pos = 1;
+                for (int e = 1; e < len; ++e) pos += ja[d + e] < jk || (ja[d + e] == jk && e < k);
+            }
+            const long long pp = o + (long long)pos * 32;
+            col[pp] = jk;
+            val[pp] = cvt_val<TV>(a[d + k], sc);
+        } else if (k < len) {
             col[p] = ja[d + k];
             for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(a[(long long)(d + k) * E + q], sc);
         } else {
             col[p] = 0;
             for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(0.0, 1.0);
         }
+    }
+}
+
+// The CSR counterpart of sell_fill's `sorted`: each row's entries after the first in ascending column
+// order (the first, the diagonal of a square operator, stays first), by an insertion sort of one
+// thread per row.
+template <typename TV>
+__global__ void sort_row_entries(int n, const int *__restrict__ ia, int *__restrict__ ja, TV *__restrict__ a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int b = ia[i] + 1, e = ia[i + 1];
+    for (int k = b + 1; k < e; ++k) {
+        const int jk = ja[k];
+        const TV ak = a[k];
+        int q = k - 1;
+        while (q >= b && ja[q] > jk) {
+            ja[q + 1] = ja[q];
+            a[q + 1] = a[q];
+            --q;
+        }
+        ja[q + 1] = jk;
+        a[q + 1] = ak;
     }
 }
 
