@@ -721,9 +721,14 @@ def roofline_level(G, stream, level, op, value_bytes, vec_bytes, cfg="c1"):
     sec = _event_time(stream, lambda r: lib.check(so.jxcpr_solver_level_native(G.h, level, op, r)), 20)
     alg = nnz * (value_bytes + 4) + (n + 1) * 4 + 4 * n * vec_bytes
     layout = _layout(G, f"A{level}")
-    fmt = "SellFmt" if layout == "sell" else f"CsrFmt<{layout.split('/')[-1]}>"
     ty = {8: "double", 4: "float", 2: "bf16"}[value_bytes]
-    return _roof(f"AMG level {level} Chebyshev step (row_kernel<{fmt}<{ty}>, OpCheb>, {n} rows, {nnz} entries)",
+    if layout == "sell":
+        fmt = f"SellFmt<{ty}>"
+    elif layout == "sell/2":
+        fmt = f"SellFmt<{ty}, 2>"  # two lanes per row
+    else:
+        fmt = f"CsrFmt<{layout.split('/')[-1]}, {ty}>"
+    return _roof(f"AMG level {level} Chebyshev step (row_kernel<{fmt}, OpCheb>, {n} rows, {nnz} entries)",
                  alg, sec, cfg, f"cheb/A{level}/{value_bytes}/{layout}", {"level": level})
 
 

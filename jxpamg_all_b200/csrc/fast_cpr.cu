@@ -55,6 +55,12 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
     if (r1 <= r0) return;
     with_values<TX>(M, [&](auto a) {
         using TV = typename std::remove_cv<typename std::remove_pointer<decltype(a)>::type>::type;
+        if (M.sell == 2) {
+            fk::SellFmt<TV, 2> f{M.sp.get(), M.ja.get(), a, M.bscale.get(), M.rows.get()};
+            launch_dep(fk::row_kernel<fk::SellFmt<TV, 2>, Op, TX>, dim3(div_up((long long)(r1 - r0) * 2, kThreads)),
+                       dim3(kThreads), s, f, op, r0, r1);
+            return;
+        }
         if (M.sell) {
             fk::SellFmt<TV> f{M.sp.get(), M.ja.get(), a, M.bscale.get(), M.rows.get()};
             launch_dep(fk::row_kernel<fk::SellFmt<TV>, Op, TX>, dim3(div_up(r1 - r0, kThreads)), dim3(kThreads), s,
@@ -78,9 +84,11 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
 // sorted by decreasing length inside windows (a stable counting sort: equal
 // lengths keep their order), each segment padded to whole slices.  Windows
 // are independent (each starts on a slice boundary), so large layouts sort
-// them on host threads.
+// them on host threads.  P lanes per row (SellFmt<TV, P>): a slice holds 32 / P
+// stored rows, and its width is the slots of its longest row's lane 0.
 void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, const std::vector<int> &seg_in,
-                 std::vector<int> &rows, std::vector<long long> &sp, std::vector<int> &seg_out) {
+                 std::vector<int> &rows, std::vector<long long> &sp, std::vector<int> &seg_out, int P = 1) {
+    const int SR = 32 / P;  // stored rows per slice
     struct Win {
         int w0, w1;
         size_t pos;
@@ -94,10 +102,10 @@ void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, cons
             wins.push_back({w0, w1, pos});
             pos += w1 - w0;
         }
-        pos = (pos + 31) / 32 * 32;
+        pos = (pos + SR - 1) / SR * SR;
         seg_out.push_back((int)pos);
     }
-    const size_t total = pos, ns = total / 32;
+    const size_t total = pos, ns = total / SR;
     rows.assign(total, -1);
     std::vector<int> width(ns, 0);
     auto sort_windows = [&](size_t b, size_t e) {
@@ -123,7 +131,7 @@ void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, cons
             }
             // a window starts on a slice boundary and its slices hold its rows alone (the
             // padding of a segment's last slice follows its last window), longest first
-            for (int q = 0; q < nw; q += 32) width[W.pos / 32 + q / 32] = slen[q];
+            for (int q = 0; q < nw; q += SR) width[W.pos / SR + q / SR] = (slen[q] + P - 1) / P;
         }
     };
     const size_t nwin = wins.size();
@@ -160,14 +168,16 @@ void sell_fill_launch(LevelMat &M, const int *ia, const int *ja, const double *a
 //  level 2 12.6 -> 11.9 us; C4 level 1 20.2 -> 19.0 us).  The row sums' order changes with it; the
 //  fast path's contract is the FP64 true residual, not a fixed summation order.
 void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const int *ja, const double *a, int kind,
-                     bool sell, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
+                     int sell, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
                      LevelMat &M, cudaStream_t s) {
+    // sell: 0 CSR, 1 sliced ELL, 2 sliced ELL with two lanes per row (E = 1, FP32 / FP64 values)
+    if (sell == 2 && (E != 1 || kind == VAL_BF16)) sell = 1;
     M.n = n;
     M.m = m;
     M.nnz = nnz;
     M.E = E;
     M.kind = kind;
-    M.sell = sell ? 1 : 0;
+    M.sell = sell;
     const bool natural = order.empty();
     if (sell) {
         std::vector<int> ia_h(n + 1);
@@ -181,7 +191,7 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
         }
         std::vector<int> rows;
         std::vector<long long> sp;
-        sell_layout(ia_h, natural ? ord : order, natural ? sg : seg, rows, sp, M.seg);
+        sell_layout(ia_h, natural ? ord : order, natural ? sg : seg, rows, sp, M.seg, sell);
         M.nstored = (int)rows.size();
         const long long slots = sp.back();
         M.rows.alloc(rows.size() + 1);
@@ -190,7 +200,21 @@ void build_level_mat(int n, int m, long long nnz, int E, const int *ia, const in
         M.sp.upload(sp.data(), sp.size(), s);
         M.ja.alloc(slots > 0 ? slots : 1);
         const long long nv = (slots > 0 ? slots : 1) * E;
-        if (kind == VAL_F64) {
+        if (sell == 2) {
+            const long long lanes = (long long)M.nstored * 2;
+            if (kind == VAL_F64) {
+                M.a64.alloc(nv);
+                if (lanes)
+                    fk::sell_fill_lanes<double><<<div_up(lanes, kThreads), kThreads, 0, s>>>(
+                        M.nstored, 2, M.rows.get(), M.sp.get(), ia, ja, a, M.ja.get(), M.a64.get(), 0);
+            } else {
+                M.a32.alloc(nv);
+                if (lanes)
+                    fk::sell_fill_lanes<float><<<div_up(lanes, kThreads), kThreads, 0, s>>>(
+                        M.nstored, 2, M.rows.get(), M.sp.get(), ia, ja, a, M.ja.get(), M.a32.get(), 1);
+            }
+            JX_LAUNCH_CHECK();
+        } else if (kind == VAL_F64) {
             M.a64.alloc(nv);
             sell_fill_launch<double>(M, ia, ja, a, M.a64.get(), nullptr, s);
         } else if (kind == VAL_F32) {
@@ -345,7 +369,7 @@ double time_pass(const LevelMat &M, const TX *x, TX *y, cudaStream_t s) {
 }
 
 std::string layout_name(const LevelMat &M) {
-    return M.sell ? std::string("sell") : ("csr/" + std::to_string(M.lanes));
+    return M.sell == 2 ? std::string("sell/2") : M.sell ? std::string("sell") : ("csr/" + std::to_string(M.lanes));
 }
 
 // Layout choices of earlier setups, keyed by operator role, shape and storage:
@@ -421,7 +445,7 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
         }
     }
     if (cached) {
-        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, best.sell != 0, order, seg, order_dev, M, s);
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, best.sell, order, seg, order_dev, M, s);
         if (!best.sell) M.lanes = best.lanes;
     } else {
         build_level_mat(n, m, nnz, 1, ia, ja, a, kind, false, order, seg, order_dev, M, s);
@@ -441,13 +465,16 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
         }
         M.lanes = best.lanes;
         if (n >= 2048) {
-            LevelMat S;
-            build_level_mat(n, m, nnz, 1, ia, ja, a, kind, true, order, seg, order_dev, S, s);
-            const double t = time_pass<TX>(S, x.get(), y.get(), s);
-            if (t < best.us) {
-                best.us = t;
-                best.sell = 1;
-                M = std::move(S);
+            // sliced ELL with one lane per row, and (FP32 / FP64 values) with two
+            for (int P = 1; P <= (kind == VAL_BF16 ? 1 : 2); ++P) {
+                LevelMat S;
+                build_level_mat(n, m, nnz, 1, ia, ja, a, kind, P, order, seg, order_dev, S, s);
+                const double t = time_pass<TX>(S, x.get(), y.get(), s);
+                if (t < best.us) {
+                    best.us = t;
+                    best.sell = P;
+                    M = std::move(S);
+                }
             }
         }
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -478,9 +505,14 @@ __device__ __forceinline__ int source_slot(const int *__restrict__ src_ja, int d
     return -1;
 }
 
-// sliced ELL: stored row t = row rows[t], entry k at sp[t / 32] + 32 k + t % 32
+// sliced ELL with P lanes per row: stored row t = row rows[t]; its entry at stored position q sits in
+// virtual row v = P t + q % P, slot q / P: at sp[v / 32] + 32 (q / P) + v % 32
+__device__ __forceinline__ long long sell_slot(const long long *__restrict__ sp, int P, int t, int q) {
+    const long long v = (long long)t * P + q % P;
+    return sp[v >> 5] + (v & 31) + 32LL * (q / P);
+}
 template <typename TV>
-__global__ void unpack_sell_kernel(int nstored, const int *__restrict__ rows, const long long *__restrict__ sp,
+__global__ void unpack_sell_kernel(int nstored, int P, const int *__restrict__ rows, const long long *__restrict__ sp,
                                    const int *__restrict__ col, const int *__restrict__ src_ia,
                                    const int *__restrict__ src_ja, const TV *__restrict__ val,
                                    const float *__restrict__ bsc, double *__restrict__ out) {
@@ -488,14 +520,14 @@ __global__ void unpack_sell_kernel(int nstored, const int *__restrict__ rows, co
     if (t >= nstored) return;
     const int i = rows[t];
     if (i < 0) return;
-    const long long o = sp[t >> 5] + (t & 31);
     const int d = src_ia[i], len = src_ia[i + 1] - d;
     for (int k = 0; k < len; ++k) {
-        const int cj = col[o + (long long)k * 32];
+        const long long pk = sell_slot(sp, P, t, k);
+        const int cj = col[pk];
         int r = 0;
-        for (int q = 0; q < k; ++q) r += col[o + (long long)q * 32] == cj;
+        for (int q = 0; q < k; ++q) r += col[sell_slot(sp, P, t, q)] == cj;
         const int pos = source_slot(src_ja, d, len, cj, r);
-        if (pos >= 0) out[d + pos] = (double)fk::ldvs(val, bsc, o + (long long)k * 32);
+        if (pos >= 0) out[d + pos] = (double)fk::ldvs(val, bsc, pk);
     }
 }
 
@@ -822,7 +854,7 @@ struct FastCpr final : FastCprBase {
         long long want = 1;
         for (int l = first; l < L - 1; ++l) {
             const LevelMat &A = lv[l]->A;
-            want = std::max(want, (long long)A.nstored * (A.sell ? 1 : A.lanes));
+            want = std::max(want, (long long)A.nstored * (A.sell ? A.sell : A.lanes));
         }
         want = std::max(want, (long long)nc * 32);
         int grid = std::max(1, std::min(std::max(per_sm, 1) * sm_count(), div_up(want, kThreads)));
@@ -1173,7 +1205,7 @@ struct FastCpr final : FastCprBase {
         with_values<TX>(M, [&](auto a) {
             if (M.sell)
                 unpack_sell_kernel<<<div_up(M.nstored, kThreads), kThreads, 0, s>>>(
-                    M.nstored, M.rows.get(), M.sp.get(), M.ja.get(), L.src_ia, L.src_ja, a, M.bscale.get(), out);
+                    M.nstored, M.sell, M.rows.get(), M.sp.get(), M.ja.get(), L.src_ia, L.src_ja, a, M.bscale.get(), out);
             else
                 unpack_csr_kernel<<<div_up(M.n, kThreads), kThreads, 0, s>>>(
                     M.n, M.perm, M.ia.get(), M.ja.get(), L.src_ia, L.src_ja, a, M.bscale.get(), out);

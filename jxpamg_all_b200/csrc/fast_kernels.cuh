@@ -75,9 +75,12 @@ struct CsrFmt {
 // sp[t/32] + 32 k + t%32 (padding: value 0, column 0).  rows[t] is the vector
 // row of stored row t (-1: padding row).  One thread per row: the 32 rows of a
 // warp read each slot with one coalesced access.
-template <typename TV>
+// P = 2: two lanes per row.  Stored row t is split into the virtual rows 2t and 2t + 1, holding its
+// entries of even and odd position; the virtual rows form the 32-row slices (16 stored rows each),
+// and the pair's sums are added with one shuffle.
+template <typename TV, int P = 1>
 struct SellFmt {
-    static constexpr int V = 1;
+    static constexpr int V = P;
     const long long *sp;
     const int *col;
     const TV *a;
@@ -85,11 +88,23 @@ struct SellFmt {
     const int *rows;
     __device__ __forceinline__ int row(int t) const { return __ldg(rows + t); }
     template <typename TA, typename TX>
-    __device__ __forceinline__ TA sum(int t, bool live, int, const TX *x, int kstart) const {
-        if (!live) return 0;
-        const long long b0 = __ldg(sp + (t >> 5)), b1 = __ldg(sp + (t >> 5) + 1);
+    __device__ __forceinline__ TA sum(int t, bool live, int lane, const TX *x, int kstart) const {
+        if constexpr (P == 1) {
+            if (!live) return 0;
+            return slots<TA>((long long)t, x, kstart);
+        } else {
+            // every lane takes part in the shuffle, live or not; lane h holds positions h, h + P, ...
+            const TA s = live ? slots<TA>((long long)t * P + lane, x, kstart > lane ? (kstart - lane + P - 1) / P : 0)
+                              : (TA)0;
+            return group_sum<P, TA>(s);
+        }
+    }
+    // slots [kstart, width) of virtual row vt
+    template <typename TA, typename TX>
+    __device__ __forceinline__ TA slots(long long vt, const TX *x, int kstart) const {
+        const long long b0 = __ldg(sp + (vt >> 5)), b1 = __ldg(sp + (vt >> 5) + 1);
         const int w = (int)((b1 - b0) >> 5);
-        const long long o = b0 + (t & 31);
+        const long long o = b0 + (vt & 31);
         TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
         int k = kstart;
         for (; k + 3 < w; k += 4) {
@@ -853,6 +868,40 @@ __global__ void sell_fill(int nstored, const int *__restrict__ rows, const long 
             col[p] = 0;
             for (int q = 0; q < E; ++q) val[p * E + q] = cvt_val<TV>(0.0, 1.0);
         }
+    }
+}
+
+// The sliced ELL with P lanes per stored row (SellFmt<TV, P>, P > 1; FP32 / FP64 values, no block
+// scales): thread u is virtual row u (stored row u / P, lane u % P); the entry at (sorted) position
+// q of the row goes to lane q % P, slot q / P.  Unfilled slots are padding (value 0, column 0).
+template <typename TV>
+__global__ void sell_fill_lanes(int nstored, int P, const int *__restrict__ rows, const long long *__restrict__ sp,
+                                const int *__restrict__ ia, const int *__restrict__ ja, const double *__restrict__ a,
+                                int *__restrict__ col, TV *__restrict__ val, int sorted) {
+    const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (long long)nstored * P) return;
+    const int t = (int)(u / P), h = (int)(u % P);
+    const int i = rows[t];
+    const long long b0 = sp[u >> 5], b1 = sp[(u >> 5) + 1];
+    const int w = (int)((b1 - b0) >> 5);
+    const long long o = b0 + (u & 31);
+    const int d = i >= 0 ? ia[i] : 0, len = i >= 0 ? ia[i + 1] - d : 0;
+    for (int k = 0; k < w; ++k)
+        if (h + (long long)P * k >= len) {
+            col[o + (long long)k * 32] = 0;
+            val[o + (long long)k * 32] = cvt_val<TV>(0.0, 1.0);
+        }
+    for (int e = 0; e < len; ++e) {
+        int q = e;
+        if (sorted && e > 0) {
+            const int je = ja[d + e];
+            q = 1;
+            for (int f = 1; f < len; ++f) q += ja[d + f] < je || (ja[d + f] == je && f < e);
+        }
+        if (q % P != h) continue;
+        const long long pp = o + (long long)(q / P) * 32;
+        col[pp] = ja[d + e];
+        val[pp] = cvt_val<TV>(a[d + e], 1.0);
     }
 }
 

@@ -21,7 +21,8 @@ constexpr int kMaxLevels = 12;   // fused levels, the coarsest included
 constexpr int kMaxSegs = 10;     // colour classes of a multicolour GS level (max_colors <= 8)
 constexpr int kMaxPasses = 40;   // colour passes of one GS smoothing (4 sweeps x classes)
 
-// One operator in its fast-path layout (CSR with `lanes` lanes per row, or sliced ELL).
+// One operator in its fast-path layout (CSR with `lanes` lanes per row, or sliced ELL with `sell` lanes
+// per row).
 template <typename TV>
 struct Mat {
     int sell, lanes, nstored;
@@ -76,6 +77,11 @@ __device__ __forceinline__ void rows_pass(const Fmt &fmt, const Op &op, int r0, 
 template <typename TX, typename TV, class Op>
 __device__ __noinline__ void mat_pass(const Mat<TV> &M, const Op &op, int r0, int r1) {
     if (r1 <= r0) return;
+    if (M.sell == 2) {
+        fk::SellFmt<TV, 2> f{M.sp, M.ja, M.a, M.bscale, M.rows};
+        rows_pass<fk::SellFmt<TV, 2>, Op, TX>(f, op, r0, r1);
+        return;
+    }
     if (M.sell) {
         fk::SellFmt<TV> f{M.sp, M.ja, M.a, M.bscale, M.rows};
         rows_pass<fk::SellFmt<TV>, Op, TX>(f, op, r0, r1);
