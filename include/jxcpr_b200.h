@@ -176,6 +176,9 @@ JXCPR_API int jxcpr_dense_inverse_dev(int n, const double *a, double *ainv, void
  *         levels from the first with at most this many rows, the coarsest
  *         included, run as one cooperative kernel; 0 one launch per pass),
  *         tail_ctas (0: that kernel's grid, sized by its largest pass),
+ *         sell_lanes (1: with autotune 0, lanes per row of the sliced-ELL
+ *         level operators; 2 splits each row into its even- and
+ *         odd-position entries),
  *         learned_fallback (1: the probe
  *         and the stall guard may replace the learned settings),
  *         record_features (0), thermal (0)

@@ -63,6 +63,7 @@ int set_int_param(SolverParams &p, const char *key, int v) {
                {"stage2_lanes", &p.stage2_lanes},
                {"stage2_chunk", &p.stage2_chunk},
                {"tail_rows", &p.tail_rows},
+               {"sell_lanes", &p.sell_lanes},
                {"tail_ctas", &p.tail_ctas},
                {"learned_fallback", &p.learned_fallback},
                {"record_features", &p.record_features},

@@ -100,6 +100,7 @@ struct FastOptions {
                                // level-0 colour order)
     int sell_min_rows = 16384; // without autotuning: sliced ELL for operators with at least this many rows ...
     double sell_max_mean = 40; // ... and at most this mean row length
+    int sell_lanes = 1;        // ... with this many lanes per row (1 or 2; FP32 / FP64 values)
     int graphs = 1;            // replay each preconditioner application as one captured CUDA graph
     int dep_launch = 1;        // kernels of an application launched as programmatic dependents (launch_dep)
     int tail_rows = 0;         // levels from the first with at most this many rows run as one cooperative kernel (0: off)

@@ -430,7 +430,14 @@ void build_tuned(const char *name, int n, int m, long long nnz, const int *ia, c
                  int kind, const std::vector<int> &order, const std::vector<int> &seg, const int *order_dev,
                  const FastOptions &opt, LevelMat &M, std::vector<std::string> &log, cudaStream_t s) {
     if (!opt.autotune || n == 0) {
-        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, use_sell(opt, n, nnz), order, seg, order_dev, M, s);
+        build_level_mat(n, m, nnz, 1, ia, ja, a, kind, use_sell(opt, n, nnz) ? (opt.sell_lanes == 2 ? 2 : 1) : 0,
+                        order, seg, order_dev, M, s);
+        if (n) {
+            char line[200];
+            snprintf(line, sizeof line, "%s rows %d mean %.1f layout %s (heuristic)", name, n, (double)nnz / n,
+                     layout_name(M).c_str());
+            log.emplace_back(line);
+        }
         return;
     }
     const std::string key = tune_key(name, n, nnz, kind, 1, opt.autotune);

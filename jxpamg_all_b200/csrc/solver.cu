@@ -78,6 +78,7 @@ void CprPrecond::setup(const BsrView<double> &A_, cudaStream_t s) {
         opt.stage2_chunk = prm.stage2_chunk;
         opt.tail_rows = prm.tail_rows;
         opt.tail_ctas = prm.tail_ctas;
+        opt.sell_lanes = prm.sell_lanes;
         opt.autotune = prm.autotune;
         opt.graphs = prm.graphs;
         opt.dep_launch = prm.dep_launch;

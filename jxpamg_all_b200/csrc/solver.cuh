@@ -88,6 +88,7 @@ struct SolverParams {
     int tail_rows = 0;         // fast path: the V-cycle's levels from the first with at most this many rows
                                // (the coarsest included) run as one cooperative kernel (0: one launch per pass)
     int tail_ctas = 0;         // its grid (0: sized by the largest fused pass, at most the co-resident blocks)
+    int sell_lanes = 1;        // fast path without autotuning: lanes per row of the sliced-ELL operators (1 or 2)
     int learned_fallback = 1;  // learned mode: keep the plain smoothers when their V-cycle factor is lower
     int record_features = 0;   // fast path: record the per-level features (training data)
 };

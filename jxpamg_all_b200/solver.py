@@ -27,7 +27,7 @@ class CprGmres:
     Integer options: k_dim, max_iter, min_iter, is_check_restarted,
     pressure_index, stage1_maxit, stage2_maxit, stage1_solver_type,
     stage2_solver_type, decouple, consistent_rhs, smoother_order, coarse_exact,
-    use_tma_spmv, precision, bf16_level, fast_smoother, stage2_lanes, stage2_chunk, tail_rows, tail_ctas,
+    use_tma_spmv, precision, bf16_level, fast_smoother, stage2_lanes, stage2_chunk, tail_rows, tail_ctas, sell_lanes,
     learned_fallback, record_features, flexible, graph_gmres, krylov_fp32,
     selective_reorth.  Real options: tol, a_tol, threshold,
     convfac_threshold, stage2_relax_weight, stage2_omega, strong_threshold,

@@ -40,7 +40,7 @@ def test_version_and_error_without_gpu():
 INT_KEYS = ["k_dim", "max_iter", "min_iter", "is_check_restarted", "print_level", "logging", "pressure_index",
             "stage1_maxit", "stage2_maxit", "stage1_solver_type", "stage2_solver_type", "decouple", "thermal",
             "consistent_rhs", "smoother_order", "coarse_exact", "max_colors", "rs_range_rows", "rs_range_rows_coarse", "dep_launch",
-            "use_tma_spmv", "precision", "bf16_level", "fast_smoother", "stage2_lanes", "stage2_chunk", "tail_rows", "tail_ctas", "learned_fallback",
+            "use_tma_spmv", "precision", "bf16_level", "fast_smoother", "stage2_lanes", "stage2_chunk", "tail_rows", "tail_ctas", "sell_lanes", "learned_fallback",
             "record_features", "flexible", "autotune", "graphs", "orthog", "graph_gmres", "krylov_fp32", "selective_reorth", "bilu_sweeps",
             "bilu_ir_iters", "bilu_lower_iters", "bilu_upper_iters", "bilu_exact"]
 REAL_KEYS = ["tol", "a_tol", "threshold", "convfac_threshold", "stage2_relax_weight", "stage2_omega",

@@ -281,3 +281,28 @@ def test_stored_level_values_against_fp64(systems, name, precision):
             m, _ = np.frexp(got[got != 0])
             assert np.all(np.abs(m * 256 - np.round(m * 256)) == 0)
     G.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_two_lane_sliced_ell(precision):
+    """The sliced ELL with two lanes per row (sell_lanes 2, without autotuning): every operator that
+    takes the sliced ELL uses it, the stored values are the hierarchy's (FP64) or their FP32 rounding,
+    and the solve reaches the FP64 true residual in about as many iterations as with one lane per row
+    (the pair's shuffle changes the order of the row sums)."""
+    s = synth.reservoir_system(30, 110, 12, seed=21, phases=2, channelised_layers=7)
+    its = {}
+    for lanes in (1, 2):
+        G = CprGmres(**dict(BASE, precision=precision, fast_smoother=1, flexible=1, autotune=0,
+                            sell_lanes=lanes)).setup(s.ia, s.ja, s.a, s.block_size)
+        sell = [l for l in G.setup_report().splitlines() if "layout sell" in l]
+        assert sell, G.setup_report()
+        assert all(("layout sell/2" in l) == (lanes == 2) for l in sell), sell
+        for lev in range(G.num_levels() - 1):
+            ia, ja, a, _ = G.level_matrix(lev, 0)
+            got = G.level_stored_values(lev)
+            assert np.array_equal(got, a if precision == 0 else a.astype(np.float32).astype(np.float64)), lev
+        x, it, rel, conv = G.solve(s.b)
+        G.close()
+        assert conv and true_rel(s, x) <= 1.05e-6, (lanes, it, rel)
+        its[lanes] = it
+    assert abs(its[2] - its[1]) <= 2, its
