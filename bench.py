@@ -648,6 +648,7 @@ TRAFFIC_BYTES = {
     ("c1", "cheb/A1/4/csr/4"): 103_513_600,    # row_kernel<CsrFmt<4,float>, OpCheb>: mean of 2 launches
     ("c1", "cheb/A1/4/sell"): 108_742_144,     # row_kernel<SellFmt<float>, OpCheb>: mean of 2 launches
     ("c1", "bsr_spmv/8"): 318_746_624,         # bsr_spmv_direct_kernel<2, double>
+    ("c4", "stage2/4/chunk4"): 389_580_032,    # hgs_chunk<3,4,float>: 189,072,128 + 200,507,904 (2 colours)
 }
 
 
