@@ -82,7 +82,8 @@ void launch_rows(const LevelMat &M, const Op &op, int r0, int r1, cudaStream_t s
 // ---- construction -----------------------------------------------------------------
 // Sliced-ELL layout on the host: segments of `order` (offsets seg_in), rows
 // sorted by decreasing length inside windows (a stable counting sort: equal
-// lengths keep their order), each segment padded to whole slices.  Windows
+// lengths keep their order), a segment's windows heaviest first, each segment
+// padded to whole slices.  Windows
 // are independent (each starts on a slice boundary), so large layouts sort
 // them on host threads.  P lanes per row (SellFmt<TV, P>): a slice holds 32 / P
 // stored rows, and its width is the slots of its longest row's lane 0.
@@ -97,10 +98,30 @@ void sell_layout(const std::vector<int> &ia, const std::vector<int> &order, cons
     seg_out.assign(1, 0);
     size_t pos = 0;
     for (size_t c = 0; c + 1 < seg_in.size(); ++c) {
+        // a segment's full windows heaviest first (most entries; stable), its short last window last:
+        // the blocks launched last, which run with the grid's tail, then hold the lightest rows
+        std::vector<std::pair<long long, int>> full;
+        int tail0 = seg_in[c + 1];
         for (int w0 = seg_in[c]; w0 < seg_in[c + 1]; w0 += kSellWindow) {
-            const int w1 = std::min(seg_in[c + 1], w0 + kSellWindow);
-            wins.push_back({w0, w1, pos});
-            pos += w1 - w0;
+            if (w0 + kSellWindow > seg_in[c + 1]) {
+                tail0 = w0;
+                break;
+            }
+            long long work = 0;
+            for (int t = w0; t < w0 + kSellWindow; ++t) work += ia[order[t] + 1] - ia[order[t]];
+            full.push_back({work, w0});
+        }
+        std::stable_sort(full.begin(), full.end(),
+                         [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
+                             return x.first > y.first;
+                         });
+        for (const auto &f : full) {
+            wins.push_back({f.second, f.second + kSellWindow, pos});
+            pos += kSellWindow;
+        }
+        if (tail0 < seg_in[c + 1]) {
+            wins.push_back({tail0, seg_in[c + 1], pos});
+            pos += seg_in[c + 1] - tail0;
         }
         pos = (pos + SR - 1) / SR * SR;
         seg_out.push_back((int)pos);
